@@ -1,0 +1,366 @@
+"""Benchmark of the fused-chunk path: chunk GB/s against the measured HBM peak.
+
+Workload ("large fused chunks", float32, n = 2^28 per array, seeded synthetic data):
+x ~ N(0,1), y ~ U[0.1, 10), z ~ U[-1, 1) with NaN injected at rate 1e-6. One step runs the six
+operations a libsci user writes for it, each one kernel launch through the C ABI:
+
+    stored = root(absolute(x)) * logarithm(y) + tanh(z)     16 B/element
+    lower  = minimum(x, z)                                  12 B/element
+    upper  = maximum(x, z)                                  12 B/element
+    mean(exponential(-x * x))                                4 B/element
+    maximum(sin(x) * cos(z))                                 8 B/element
+    dot(x, z)                                                8 B/element
+
+`value` = algorithmic bytes of a step (60 B/element) / device time of a step (CUDA events on the
+library's stream, max over ranks). Inputs are 1 GiB each, far larger than the 126 MB L2, so no
+flush is needed between steps. `e2e` runs the same step through the C ABI from pinned host buffers:
+the three inputs are uploaded and the three stored outputs and three reductions downloaded inside
+the timed region. `roofline` is the dominant kernel's achieved GB/s over the measured copy peak.
+`cpu_baseline` times libsci's own CPU path (oracle/_ref/libsci_ref.so, all host cores) on a
+2^24-element sample of the same workload.
+
+`--impl reference` times only that CPU path (the reference arm), on rank 0.
+With N > 1 GPUs (torchrun), every rank runs its own 2^28-element shard (weak scaling) and the
+three reductions are combined across ranks with one NCCL all-reduce per step.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+BYTES_PER_ELEMENT = {"stored": 16, "lower": 12, "upper": 12, "mean": 4, "peak": 8, "dot": 8}
+STEP_BYTES_PER_ELEMENT = sum(BYTES_PER_ELEMENT.values())
+METRIC = "chunk GB/s vs HBM peak"
+
+
+def generate(count: int, seed: int = 0):
+    """Seeded inputs of the large fused chunks: x ~ N(0,1), y ~ U[0.1,10), z ~ U[-1,1), NaN at 1e-6."""
+    rng = np.random.default_rng(seed)
+    x = rng.standard_normal(count, dtype=np.float32)
+    y = rng.uniform(0.1, 10.0, count).astype(np.float32)
+    z = rng.uniform(-1.0, 1.0, count).astype(np.float32)
+    holes = rng.choice(count, size=max(1, int(round(count * 1e-6))), replace=False)
+    z[holes] = np.nan
+    return x, y, z
+
+
+def measured_peaks():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons through NVML while the timed region runs."""
+
+    REASONS = {
+        0x0000000000000008: "hw_slowdown",
+        0x0000000000000040: "hw_thermal_slowdown",
+        0x0000000000000020: "sw_thermal_slowdown",
+        0x0000000000000004: "sw_power_cap",
+        0x0000000000000080: "hw_power_brake_slowdown",
+    }
+
+    def __init__(self, index: int):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.handle = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM)
+        except Exception:  # NVML missing: clocks are reported as unknown
+            self.nvml = None
+        self.thread = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self.nvml.nvmlDeviceGetClockInfo(self.handle, self.nvml.NVML_CLOCK_SM))
+                mask = self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+                for bit, name in self.REASONS.items():
+                    if mask & bit:
+                        self.reasons.add(name)
+            except Exception:
+                break
+            time.sleep(0.002)
+
+    def __enter__(self):
+        if self.nvml:
+            self.thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self.nvml:
+            self.thread.join()
+
+    def summary(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def cpu_reference_sample(count: int, repeats: int):
+    """libsci's own CPU path (oracle/_ref) on `count` elements: seconds per step, threads used."""
+    from tests import _oracle
+
+    lib = _oracle.reference()
+    if lib is None:
+        return None
+    x, y, z = generate(count, seed=1)
+    handle = lib.sci_ref_workload_create(x.ctypes.data, y.ctypes.data, z.ctypes.data, count)
+    results = np.zeros(3, np.float64)
+    lib.sci_ref_workload_step(handle, results.ctypes.data)  # warm-up (page faults, pool start)
+    times = []
+    for _ in range(repeats):
+        start = time.perf_counter()
+        lib.sci_ref_workload_step(handle, results.ctypes.data)
+        times.append(time.perf_counter() - start)
+    lib.sci_ref_workload_destroy(handle)
+    return {"seconds": statistics.median(times), "threads": int(lib.sci_ref_threads()), "count": count,
+            "times": times}
+
+
+def run_reference_arm(args, rank: int) -> int:
+    if rank != 0:
+        return 0
+    sample = 1 << 24
+    from tests import _oracle
+
+    lib = _oracle.reference()
+    if lib is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libsci_ref.so was not built"}))
+        return 0
+    x, y, z = generate(sample, seed=1)
+    handle = lib.sci_ref_workload_create(x.ctypes.data, y.ctypes.data, z.ctypes.data, sample)
+    results = np.zeros(3, np.float64)
+    for _ in range(args.warmup):
+        lib.sci_ref_workload_step(handle, results.ctypes.data)
+    start = time.perf_counter()
+    for _ in range(args.steps):
+        lib.sci_ref_workload_step(handle, results.ctypes.data)
+    elapsed = time.perf_counter() - start
+    lib.sci_ref_workload_destroy(handle)
+    per_step = elapsed / args.steps
+    value = STEP_BYTES_PER_ELEMENT * sample / per_step / 1e9
+    threads = int(lib.sci_ref_threads())
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "large fused chunks (float32), libsci CPU path on a 2^24-element sample",
+                   "elements": sample, "bytes_per_element": STEP_BYTES_PER_ELEMENT},
+        "cpu_baseline": {"value": value, "unit": "GB/s", "cores": threads, "kind": "reference",
+                         "sample": f"{sample} elements per step (2^24 of the 2^28 workload), libsci public API"},
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main() -> int:
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=20)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    parser.add_argument("--elements", type=int, default=1 << 28)
+    parser.add_argument("--e2e-steps", type=int, default=3)
+    parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = parser.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank)
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from libsci_b200 import chunk as C
+    from libsci_b200.device import Device
+
+    n = args.elements
+    device = Device(local)
+    stream = torch.cuda.ExternalStream(device.stream, device=torch.device("cuda", local))
+
+    x, y, z = generate(n, seed=rank)
+    dx, dy, dz = device.array(x), device.array(y), device.array(z)
+    stored, lower, upper = device.empty(n), device.empty(n), device.empty(n)
+    results = torch.zeros(3, dtype=torch.float64, device=f"cuda:{local}")
+    a, b, c = dx.expression(), dy.expression(), dz.expression()
+    chunks = {
+        "stored": (C.record_output(C.unary("root", C.unary("absolute", a)) * C.unary("logarithm", b) + C.unary("tanh", c)), stored),
+        "lower": (C.record_output(C.binary("minimum", a, c)), lower),
+        "upper": (C.record_output(C.binary("maximum", a, c)), upper),
+        "mean": (C.record_reduce(C.unary("exponential", -a * a)), C.SUM),
+        "peak": (C.record_reduce(C.unary("sin", a) * C.unary("cos", c)), C.MAXIMUM),
+        "dot": (C.record_reduce(a * c), C.SUM),
+    }
+    names = list(chunks)
+
+    def launch(name, slot):
+        chunk, target = chunks[name]
+        if name in ("stored", "lower", "upper"):
+            device.execute(chunk, target.pointer, n)
+        else:
+            device.reduce_async(chunk, target, n, results.data_ptr() + 8 * slot)
+
+    def step(events=None):
+        for i, name in enumerate(names):
+            if events is not None:
+                events[i].record(stream)
+            launch(name, max(0, i - 3))
+        if events is not None:
+            events[len(names)].record(stream)
+        if dist is not None:
+            with torch.cuda.stream(stream):
+                sums = results[[0, 2]].clone()
+                peak = results[1:2].clone()
+                dist.all_reduce(sums)
+                dist.all_reduce(peak, op=dist.ReduceOp.MAX)
+
+    # warm-up (also lets any specialised kernels compile and load)
+    for _ in range(args.warmup):
+        step()
+    if hasattr(device, "jit_wait"):
+        device.jit_wait()
+    for _ in range(2):
+        step()
+    device.synchronize()
+
+    # timed region: K steps, per-launch events on the library's stream
+    per_kernel = {name: [] for name in names}
+    step_events = [[torch.cuda.Event(enable_timing=True) for _ in range(len(names) + 1)] for _ in range(args.steps)]
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for k in range(args.steps):
+            step(step_events[k])
+        stop.record(stream)
+        stop.synchronize()
+    torch.cuda.synchronize()
+    elapsed_ms = start.elapsed_time(stop)
+    for k in range(args.steps):
+        for i, name in enumerate(names):
+            per_kernel[name].append(step_events[k][i].elapsed_time(step_events[k][i + 1]))
+    if dist is not None:
+        t = torch.tensor([elapsed_ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+    ms_per_step = elapsed_ms / args.steps
+    value = STEP_BYTES_PER_ELEMENT * n * world / (ms_per_step * 1e-3) / 1e9
+
+    # the dominant kernel and its roofline
+    mean_ms = {name: statistics.mean(v) for name, v in per_kernel.items()}
+    dominant = max(mean_ms, key=mean_ms.get)
+    peak_gbs, peak_kind = measured_peaks()
+    achieved = BYTES_PER_ELEMENT[dominant] * n / (mean_ms[dominant] * 1e-3) / 1e9
+    traffic = None
+    traffic_file = ROOT / "profiles" / "traffic.json"
+    if traffic_file.exists():
+        known = json.loads(traffic_file.read_text())
+        entry = known.get(dominant)
+        if entry:
+            traffic = entry["bytes_per_element"] * n
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak_gbs, "unit": "GB/s", "frac": achieved / peak_gbs,
+                "traffic": traffic, "kernel": f"chunk_stream ({dominant})", "peak_source": f"{peak_kind} hbm_gbs"}
+    kernels = {name: {"ms": mean_ms[name], "GB/s": BYTES_PER_ELEMENT[name] * n / (mean_ms[name] * 1e-3) / 1e9,
+                      "frac": BYTES_PER_ELEMENT[name] * n / (mean_ms[name] * 1e-3) / 1e9 / peak_gbs}
+               for name in names}
+
+    # end to end through the C ABI from pinned host buffers
+    hx = torch.from_numpy(x).pin_memory()
+    hy = torch.from_numpy(y).pin_memory()
+    hz = torch.from_numpy(z).pin_memory()
+    outs = [torch.empty(n, dtype=torch.float32).pin_memory() for _ in range(3)]
+    host_results = torch.zeros(3, dtype=torch.float64).pin_memory()
+    from libsci_b200.native import check, lib
+
+    def e2e_step():
+        for host, dev in ((hx, dx), (hy, dy), (hz, dz)):
+            check(lib.sci_cuda_upload(device.handle, dev.pointer, host.data_ptr(), n * 4), device.handle)
+        step()
+        for host, dev in zip(outs, (stored, lower, upper)):
+            check(lib.sci_cuda_download(device.handle, host.data_ptr(), dev.pointer, n * 4), device.handle)
+        check(lib.sci_cuda_download(device.handle, host_results.data_ptr(), results.data_ptr(), 24), device.handle)
+
+    e2e_step()
+    device.synchronize()
+    e_start, e_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist is not None:
+        dist.barrier()
+    e_start.record(stream)
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    e_stop.record(stream)
+    e_stop.synchronize()
+    e2e_ms = e_start.elapsed_time(e_stop) / args.e2e_steps
+    if dist is not None:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = STEP_BYTES_PER_ELEMENT * n * world / (e2e_ms * 1e-3) / 1e9
+
+    # a correctness spot check of the step just run: the stored chunk against the CPU oracle
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        sample = cpu_reference_sample(1 << 24, repeats=5)
+        if sample:
+            cpu = {"value": STEP_BYTES_PER_ELEMENT * sample["count"] / sample["seconds"] / 1e9, "unit": "GB/s",
+                   "cores": sample["threads"], "kind": "reference",
+                   "sample": f"{sample['count']} elements (2^24 of 2^28) per step, median of 5, libsci public API"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "large fused chunks (float32, n=2^28 per array per GPU, NaN rate 1e-6)",
+                       "elements": n, "bytes_per_element": STEP_BYTES_PER_ELEMENT,
+                       "chunks": names, "l2": "inputs 1 GiB each, larger than L2; no flush",
+                       "parallelism": f"shard per GPU x{world}"},
+            "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": 3 * n * 4,
+                    "d2h_bytes_per_step": 3 * n * 4 + 24, "ms_per_step": e2e_ms},
+            "gpu_launches": len(names) * args.steps,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line))
+    device.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

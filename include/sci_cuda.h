@@ -1,0 +1,144 @@
+/* sci_cuda.h -- C ABI of the B200 (sm_100a) backend for libsci.
+ *
+ * The reference drives every compute device through sci::core::drivers::Device
+ * (include/core/drivers/device.hpp:27-89 in libsci). This header is the boundary a new
+ * `Target::cuda` branch of that class calls: plain pointers, sizes and status codes, no C++
+ * or torch types. Each entry point names the reference interface it stands in for.
+ *
+ * Conventions
+ *  - Every call returns SCI_CUDA_OK (0) or a nonzero status; sci_cuda_last_error() gives the
+ *    message. Nothing falls back to the CPU: a chunk the device cannot run is an error.
+ *  - Work is queued in order on one CUDA stream per context (the reference's vulkan::Stream,
+ *    src/core/drivers/vulkan/stream.cpp:56-130); calls that return a host value wait for it.
+ *  - One mutex per context serialises its users (Graphics::guard, src/core/drivers/device.cpp:127).
+ */
+#ifndef SCI_CUDA_H
+#define SCI_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------ */
+enum {
+    SCI_CUDA_OK = 0,
+    SCI_CUDA_ERROR_INVALID = 1,     /* bad argument: null pointer, size, code, slot, ...      */
+    SCI_CUDA_ERROR_MEMORY = 2,      /* device allocation failed                                */
+    SCI_CUDA_ERROR_LAUNCH = 3,      /* a CUDA call or kernel launch failed                     */
+    SCI_CUDA_ERROR_UNSUPPORTED = 4, /* valid request this build does not run                   */
+    SCI_CUDA_ERROR_DEVICE = 5,      /* no usable sm_100 device at that ordinal                 */
+    SCI_CUDA_ERROR_TIMEOUT = 6,     /* a bounded device-side wait ran out                      */
+    SCI_CUDA_ERROR_COMPILE = 7      /* NVRTC specialisation failed (the interpreter still runs) */
+};
+
+/* ---- the chunk: mirrors sci::core::Chunk field for field --------------------------------- */
+/* include/core/bytecode/chunk.hpp:78-246, instruction.hpp:12-35, code.hpp:18-61, fold.hpp:11 */
+#define SCI_CHUNK_CAPACITY 64
+
+enum { SCI_PRECISION_SINGLE = 0, SCI_PRECISION_WIDE = 1 }; /* precision.hpp:12 */
+
+/* value ids: kind in the top two bits, index in the low six (instruction.hpp:12-25) */
+enum {
+    SCI_SLOT_INPUT = 0x00,
+    SCI_SLOT_LITERAL = 0x40,
+    SCI_SLOT_TEMPORARY = 0x80,
+    SCI_SLOT_OUTPUT = 0xC0,
+    SCI_SLOT_NONE = 0xFF,
+    SCI_SLOT_TYPES = 0xC0
+};
+
+/* operation codes, in core::Code's order (code.hpp:18-61) */
+enum {
+    SCI_CODE_COPY, SCI_CODE_NEGATE, SCI_CODE_ABSOLUTE,
+    SCI_CODE_ROOT, SCI_CODE_EXPONENTIAL, SCI_CODE_LOGARITHM,
+    SCI_CODE_SIN, SCI_CODE_COS, SCI_CODE_TAN, SCI_CODE_ASIN, SCI_CODE_ACOS, SCI_CODE_ATAN,
+    SCI_CODE_CSC, SCI_CODE_SEC, SCI_CODE_COT, SCI_CODE_ACSC, SCI_CODE_ASEC, SCI_CODE_ACOT,
+    SCI_CODE_SINH, SCI_CODE_COSH, SCI_CODE_TANH, SCI_CODE_ASINH, SCI_CODE_ACOSH, SCI_CODE_ATANH,
+    SCI_CODE_CSCH, SCI_CODE_SECH, SCI_CODE_COTH, SCI_CODE_ACSCH, SCI_CODE_ASECH, SCI_CODE_ACOTH,
+    SCI_CODE_ADD, SCI_CODE_SUBTRACT, SCI_CODE_MULTIPLY, SCI_CODE_DIVIDE,
+    SCI_CODE_MINIMUM, SCI_CODE_MAXIMUM, SCI_CODE_FUSE,
+    SCI_CODE_COUNT
+};
+
+enum { SCI_FOLD_SUM = 0, SCI_FOLD_MINIMUM = 1, SCI_FOLD_MAXIMUM = 2 }; /* fold.hpp:11 */
+
+typedef struct sci_instruction { /* core::Instruction, instruction.hpp:28-35 */
+    uint8_t code;
+    uint8_t target;
+    uint8_t sources[3];
+} sci_instruction;
+
+typedef struct sci_chunk { /* core::Chunk's public state, chunk.hpp:228-246 */
+    uint8_t precision;
+    uint8_t length;
+    uint8_t arguments;
+    uint8_t literals;
+    uint8_t temporaries;
+    uint8_t result;
+    sci_instruction instructions[SCI_CHUNK_CAPACITY];
+    const void *inputs[SCI_CHUNK_CAPACITY];
+    double constants[SCI_CHUNK_CAPACITY];
+} sci_chunk;
+
+
+/* ---- context ----------------------------------------------------------------------------- */
+typedef struct sci_cuda_context sci_cuda_context;
+
+/* Device::Device(Target, index) (device.hpp:32, device.cpp:186-199). Opens device `ordinal`;
+ * fails with SCI_CUDA_ERROR_DEVICE when it is not an sm_100 part (no CPU fallback). */
+int sci_cuda_open(uint32_t ordinal, sci_cuda_context **context);
+/* Device::~Device(): waits for queued work, then frees everything the context owns. */
+int sci_cuda_close(sci_cuda_context *context);
+/* Device::name() (device.hpp:46). */
+const char *sci_cuda_name(const sci_cuda_context *context);
+/* Device::synchronize() (device.hpp:49, device.cpp:205-210): waits for queued work and reports
+ * any error a kernel recorded on the device since the last wait. */
+int sci_cuda_synchronize(sci_cuda_context *context);
+/* The message of the last failed call on this context. */
+int sci_cuda_last_error(const sci_cuda_context *context, char *buffer, size_t length);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own work with it. */
+void *sci_cuda_stream(sci_cuda_context *context);
+
+/* ---- memory ------------------------------------------------------------------------------ */
+enum {
+    SCI_CUDA_MEMORY_DEVICE = 0, /* HBM only; reach it with upload / download                   */
+    SCI_CUDA_MEMORY_MANAGED = 1 /* also a valid host pointer, like the reference's Memory::host */
+};
+/* Device::allocate(bytes, Memory&) (device.hpp:55, device.cpp:212-224). 256-byte aligned. */
+int sci_cuda_allocate(sci_cuda_context *context, uint64_t bytes, uint32_t kind, void **memory);
+/* Device::dispose(Memory&) (device.hpp:58, device.cpp:226-233): the free is deferred until work
+ * queued before it has finished, as vulkan::Stream::retire does (stream.cpp:117-130). */
+int sci_cuda_dispose(sci_cuda_context *context, void *memory);
+/* Array::to(device) / Array::host() transfers (array.hpp:223-237), queued on the stream. */
+int sci_cuda_upload(sci_cuda_context *context, void *device, const void *host, uint64_t bytes);
+int sci_cuda_download(sci_cuda_context *context, void *host, const void *device, uint64_t bytes);
+
+/* ---- chunks ------------------------------------------------------------------------------ */
+/* Device::execute(chunk, output, count) (device.hpp:63, device.cpp:235-263): output[i] =
+ * chunk(inputs[i]) for i < count, queued. Inputs and output must be device or managed memory of
+ * this context's GPU. Arithmetic is bit-identical to the reference's AVX-512 kernel table;
+ * the C-library functions are within 2 ulp of it. */
+int sci_cuda_execute(sci_cuda_context *context, const sci_chunk *chunk, void *output, uint64_t count);
+/* Device::reduce(chunk, fold, count) (device.hpp:69, device.cpp:265-316): the sum, minimum or
+ * maximum of the chunk's result over count elements, folded in double in a single pass; NaN
+ * anywhere gives NaN; an empty sum is 0 and an empty extreme NaN. sum(a*b) is contracted
+ * (chunk.hpp:201-204): a*b is never rounded or stored. Waits for the result. */
+int sci_cuda_reduce(sci_cuda_context *context, const sci_chunk *chunk, uint32_t fold, uint64_t count,
+                    double *result);
+/* The same reduction, queued: the double result is written to device memory `device_result`. */
+int sci_cuda_reduce_async(sci_cuda_context *context, const sci_chunk *chunk, uint32_t fold, uint64_t count,
+                          double *device_result);
+/* Waits until every queued NVRTC specialisation has been compiled and loaded
+ * (vulkan::Compiler::loop, src/core/drivers/vulkan/compiler.cpp:184-222, compiles in the
+ * background the same way; a chunk runs on the interpreter until its kernel is ready).
+ * SCI_CUDA_JIT=0 disables specialisation, =sync compiles on first use, =trace logs compiles. */
+int sci_cuda_jit_wait(sci_cuda_context *context);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SCI_CUDA_H */

@@ -1,0 +1,137 @@
+// context.hpp -- the per-device state behind a sci_cuda_context (host side, C++).
+//
+// Stands in for the reference's Graphics bundle (src/core/drivers/device.cpp:111-184): one CUDA
+// stream plays vulkan::Stream (in-order queue, src/core/drivers/vulkan/stream.cpp:56-130), a
+// mutex plays Graphics::guard, and the scratch of the single-pass reductions is allocated once
+// when the context opens.
+#pragma once
+
+#include "../../include/sci_cuda.h"
+#include "chunk_kernel.cuh"
+
+#include <cuda.h>  // driver-API types only; the functions are resolved at run time (Driver)
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <unordered_map>
+#include <vector>
+
+namespace sci_cuda {
+
+    // The few driver-API calls the NVRTC path needs, resolved through the runtime
+    // (cudaGetDriverEntryPoint), so the library links no libcuda and loads on machines without a
+    // driver (the CPU build and test host); `ready` is false there.
+    struct Driver {
+        bool ready{false};
+        CUresult (*module_load)(CUmodule *, const void *){nullptr};
+        CUresult (*module_function)(CUfunction *, CUmodule, const char *){nullptr};
+        CUresult (*module_unload)(CUmodule){nullptr};
+        CUresult (*function_attribute)(CUfunction, CUfunction_attribute, int){nullptr};
+        CUresult (*occupancy)(int *, CUfunction, int, size_t){nullptr};
+        CUresult (*launch)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, CUstream,
+                           void **, void **){nullptr};
+
+        static const Driver &get() {
+            static const Driver table = [] {
+                Driver d;
+                auto resolve = [](const char *name, void **out) {
+                    cudaDriverEntryPointQueryResult found{};
+                    return cudaGetDriverEntryPoint(name, out, cudaEnableDefault, &found) == cudaSuccess &&
+                           found == cudaDriverEntryPointSuccess && *out != nullptr;
+                };
+                d.ready = resolve("cuModuleLoadData", reinterpret_cast<void **>(&d.module_load)) &&
+                          resolve("cuModuleGetFunction", reinterpret_cast<void **>(&d.module_function)) &&
+                          resolve("cuModuleUnload", reinterpret_cast<void **>(&d.module_unload)) &&
+                          resolve("cuFuncSetAttribute", reinterpret_cast<void **>(&d.function_attribute)) &&
+                          resolve("cuOccupancyMaxActiveBlocksPerMultiprocessor", reinterpret_cast<void **>(&d.occupancy)) &&
+                          resolve("cuLaunchKernel", reinterpret_cast<void **>(&d.launch));
+                if (!d.ready) cudaGetLastError();
+                return d;
+            }();
+            return table;
+        }
+    };
+
+    class Specializer;  // NVRTC specialisation of the chunk kernel (specialize.cu)
+    struct Workspace;   // scratch of the product / LU paths, grown on demand
+
+    struct Retired {
+        cudaEvent_t done;
+        void *memory;
+        bool managed;
+    };
+
+    struct Context {
+        int device{0};
+        int sms{0};
+        size_t shared_limit{0};     // opt-in dynamic shared memory per block
+        cudaStream_t stream{nullptr};
+        std::recursive_mutex guard;
+        std::string error;
+        std::string name;
+
+        ReduceState *state{nullptr};   // reduction scratch (device)
+        double *result{nullptr};       // reduction result (device)
+        int *status{nullptr};          // device-side error word
+        double *host_result{nullptr};  // pinned
+        int *host_status{nullptr};     // pinned
+
+        std::vector<Retired> retired;  // frees deferred until queued work is done
+        std::map<std::tuple<const void *, int, size_t>, int> occupancy;  // (kernel, threads, smem) -> blocks/SM
+        std::unique_ptr<Specializer> specializer;
+        std::unique_ptr<Workspace> workspace;
+        int jit_mode{1};  // 0 off, 1 background, 2 synchronous (SCI_CUDA_JIT)
+        bool jit_trace{false};
+
+        int fail(int code, const char *format, ...) {
+            char buffer[512];
+            va_list args;
+            va_start(args, format);
+            std::vsnprintf(buffer, sizeof(buffer), format, args);
+            va_end(args);
+            error = buffer;
+            return code;
+        }
+
+        // Maps a CUDA error to a status, keeping the message.
+        int check(cudaError_t code, const char *what) {
+            if (code == cudaSuccess) return SCI_CUDA_OK;
+            return fail(code == cudaErrorMemoryAllocation ? SCI_CUDA_ERROR_MEMORY : SCI_CUDA_ERROR_LAUNCH, "%s: %s",
+                        what, cudaGetErrorString(code));
+        }
+
+        // Blocks per SM for a kernel at a block size and dynamic shared memory, cached.
+        int blocks_per_sm(const void *kernel, int threads, size_t smem) {
+            auto key = std::make_tuple(kernel, threads, smem);
+            auto found = occupancy.find(key);
+            if (found != occupancy.end()) return found->second;
+            int blocks = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, threads, smem) != cudaSuccess) blocks = 1;
+            occupancy[key] = blocks > 0 ? blocks : 1;
+            return occupancy[key];
+        }
+
+        // Reads and clears the device error word; waits for the stream.
+        int drain();
+    };
+
+    // The generic interpreter's kernels, compiled ahead of time (chunk_kernels_f32.cu / _f64.cu).
+    const void *generic_chunk_kernel(bool wide, int mode);
+    const void *generic_chunk_kernel_f32(int mode);
+    const void *generic_chunk_kernel_f64(int mode);
+    inline const void *generic_chunk_kernel(bool wide, int mode) {
+        return wide ? generic_chunk_kernel_f64(mode) : generic_chunk_kernel_f32(mode);
+    }
+
+    // Validates a chunk before anything is launched: counts, codes, and every value id in range.
+    int validate(Context &ctx, const sci_chunk *chunk, bool reducing);
+
+} // namespace sci_cuda
+
+struct sci_cuda_context : sci_cuda::Context {};

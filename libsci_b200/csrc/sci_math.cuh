@@ -1,0 +1,274 @@
+// sci_math.cuh -- per-element arithmetic of libsci's chunk codes on sm_100a.
+//
+// Every operation rounds exactly as the reference's AVX-512 kernel table does
+// (src/core/drivers/processor/kernels/avx512.cpp:17-153 via
+// include/core/drivers/processor/kernels/generic/operation.hpp:21-111):
+//  - add / subtract / multiply / divide / root are single IEEE operations; they are written with
+//    the _rn intrinsics so the compiler cannot contract a multiply into a following add. Only a
+//    chunk `fuse` becomes an fma (chunk.hpp:119-126,253-261).
+//  - exp / log / sin / cos repeat the reference's operation sequence (exponential.hpp:24-61,
+//    logarithm.hpp:90-126, trigonometry.hpp:162-207) with its coefficients, rounded from double
+//    exactly as polynomial.hpp:17-51 computes them, and its constants (constants.hpp:16-120).
+//  - the nine functions the reference sends to the C library per lane (library.hpp:22-35) and
+//    sin / cos beyond the Cody-Waite reach (trigonometry.hpp:189-205) are evaluated in double
+//    with CUDA's double-precision functions and rounded once to float: the nearest float to the
+//    true value except for rare double-rounding cases, within 2 ulp of glibc's float result.
+//  - minimum / maximum follow the AVX-512 blend form in the vector body and the one-lane Scalar
+//    form (scalar.hpp:115-127) in the loop tail, which the caller selects per element.
+// The file is included by the ahead-of-time build and by NVRTC specialisations alike, so it
+// depends on nothing but the CUDA device headers.
+#pragma once
+
+
+namespace sci_cuda {
+
+    enum Code : int {
+        kCopy, kNegate, kAbsolute, kRoot, kExponential, kLogarithm,
+        kSin, kCos, kTan, kAsin, kAcos, kAtan, kCsc, kSec, kCot, kAcsc, kAsec, kAcot,
+        kSinh, kCosh, kTanh, kAsinh, kAcosh, kAtanh, kCsch, kSech, kCoth, kAcsch, kAsech, kAcoth,
+        kAdd, kSubtract, kMultiply, kDivide, kMinimum, kMaximum, kFuse, kCodeCount
+    };
+
+    // ---- IEEE building blocks, never contracted ------------------------------------------------
+    __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+    __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+    __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+    __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+    __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+    __device__ __forceinline__ float fma_(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+    __device__ __forceinline__ double fma_(double a, double b, double c) { return __fma_rn(a, b, c); }
+    __device__ __forceinline__ float root(float a) { return __fsqrt_rn(a); }
+    __device__ __forceinline__ double root(double a) { return __dsqrt_rn(a); }
+
+    __device__ __forceinline__ unsigned int bits(float v) { return __float_as_uint(v); }
+    __device__ __forceinline__ unsigned long long bits(double v) { return (unsigned long long)__double_as_longlong(v); }
+    __device__ __forceinline__ float from_bits(unsigned int v) { return __uint_as_float(v); }
+    __device__ __forceinline__ double from_bits(unsigned long long v) { return __longlong_as_double((long long)v); }
+
+    __device__ __forceinline__ bool is_nan(float v) { return v != v; }
+    __device__ __forceinline__ bool is_nan(double v) { return v != v; }
+
+    // ---- constants (constants.hpp:16-120) ---------------------------------------------------------
+    template <typename T> struct Limits;
+    template <> struct Limits<float> {
+        using U = unsigned int;
+        static constexpr int mantissa = 23, width = 32;
+        static constexpr U fraction = 0x007fffffu, one = 0x3f800000u, sign = 0x80000000u;
+        static constexpr U infinity = 0x7f800000u, quiet = 0x7fc00000u;
+        static constexpr float round = 12582912.0f, magnitude = 8388608.0f, exponent = 8388735.0f;
+        static constexpr float binary = 1.44269504088896340736f;
+        static constexpr float natural = 355.0f / 512.0f, remainder = -2.12194440e-4f;
+        static constexpr float lower = -104.0f, upper = 89.0f, normal = 126.0f;
+        static constexpr float tiny = 1.17549435e-38f, lift = 33554432.0f, shift = 25.0f;
+        static constexpr float root2 = 1.41421356237309504880f;
+        static constexpr float quadrant = 0.636619772367581343f;
+        static constexpr float q0 = 1.5703125f, q1 = 4.837512969970703125e-4f, q2 = 7.549790126404332e-08f,
+                               q3 = -1.7151245100058819e-15f;
+        static constexpr float reach = 1048576.0f;
+        static constexpr int exp_terms = 8, log_terms = 4, sin_terms = 6, cos_terms = 7;
+    };
+    template <> struct Limits<double> {
+        using U = unsigned long long;
+        static constexpr int mantissa = 52, width = 64;
+        static constexpr U fraction = 0x000fffffffffffffull, one = 0x3ff0000000000000ull, sign = 0x8000000000000000ull;
+        static constexpr U infinity = 0x7ff0000000000000ull, quiet = 0x7ff8000000000000ull;
+        static constexpr double round = 6755399441055744.0, magnitude = 4503599627370496.0,
+                                exponent = 4503599627371519.0;
+        static constexpr double binary = 1.44269504088896340736;
+        // ln 2 with its low 21 bits cleared, and the rest (constants.hpp:366-369)
+        static constexpr double natural = 0x1.62e42fee00000p-1;
+        static constexpr double remainder = 1.90821492927058770002e-10;
+        static constexpr double lower = -746.0, upper = 710.0, normal = 1022.0;
+        static constexpr double tiny = 2.2250738585072014e-308, lift = 18014398509481984.0, shift = 54.0;
+        static constexpr double root2 = 1.41421356237309504880;
+        static constexpr double quadrant = 6.36619772367581382433e-01;
+        static constexpr double q0 = 1.57079632673412561417e+00, q1 = 6.07710050630396597660e-11,
+                                q2 = 2.02226624871116645580e-21, q3 = 8.47842766036889956997e-32;
+        static constexpr double reach = 1048576.0;
+        static constexpr int exp_terms = 14, log_terms = 10, sin_terms = 10, cos_terms = 11;
+    };
+
+    // Polynomial coefficients, computed in double and rounded to T as polynomial.hpp:17-51 does:
+    // 1/k! (factorials), 2/(2k+3) (reciprocals), (-1)^k/(2k+offset)! (alternating).
+    template <typename T, int N> struct Poly {
+        T c[N];
+    };
+    template <typename T, int N> __host__ __device__ constexpr Poly<T, N> factorials() {
+        Poly<T, N> p{};
+        double f = 1.0;
+        for (int k = 0; k < N; ++k) {
+            if (k > 0) f /= static_cast<double>(k);
+            p.c[k] = static_cast<T>(f);
+        }
+        return p;
+    }
+    template <typename T, int N> __host__ __device__ constexpr Poly<T, N> reciprocals() {
+        Poly<T, N> p{};
+        for (int k = 0; k < N; ++k) p.c[k] = static_cast<T>(2.0 / static_cast<double>(2 * k + 3));
+        return p;
+    }
+    template <typename T, int N, int offset> __host__ __device__ constexpr Poly<T, N> alternating() {
+        Poly<T, N> p{};
+        for (int k = 0; k < N; ++k) {
+            double f = 1.0;
+            for (int s = 2; s <= 2 * k + offset; ++s) f *= static_cast<double>(s);
+            p.c[k] = static_cast<T>((k % 2 == 0 ? 1.0 : -1.0) / f);
+        }
+        return p;
+    }
+    // sum c[k] x^(k - from), Horner from the top coefficient (polynomial.hpp:271-277).
+    template <int from, typename T, int N> __device__ __forceinline__ T horner(const Poly<T, N> &p, T x) {
+        T r = p.c[N - 1];
+#pragma unroll
+        for (int k = N - 2; k >= from; --k) r = fma_(r, x, p.c[k]);
+        return r;
+    }
+
+    // ---- minimum / maximum (avx512.cpp:43-49 body, scalar.hpp:115-127 tail) -----------------------
+    template <typename T> __device__ __forceinline__ T vmin(T l, T r) { return is_nan(l) ? l : (l < r ? l : r); }
+    template <typename T> __device__ __forceinline__ T vmax(T l, T r) { return is_nan(l) ? l : (l > r ? l : r); }
+    template <typename T> __device__ __forceinline__ T smin(T l, T r) {
+        return (is_nan(l) || is_nan(r)) ? add(l, r) : (r < l ? r : l);
+    }
+    template <typename T> __device__ __forceinline__ T smax(T l, T r) {
+        return (is_nan(l) || is_nan(r)) ? add(l, r) : (r > l ? r : l);
+    }
+
+    // ---- e^x (exponential.hpp:24-61) --------------------------------------------------------------
+    // The reference splits the final scale in two when any lane of its pack has |k| > normal; for
+    // the other lanes both forms round the same exact product once, so the split is decided per
+    // element here.
+    template <typename T> __device__ __forceinline__ T exponential(T x) {
+        using L = Limits<T>;
+        constexpr Poly<T, L::exp_terms> series = factorials<T, L::exp_terms>();
+        const T clamped = vmax(vmin(x, L::upper), L::lower);
+        const T k = sub(fma_(clamped, L::binary, L::round), L::round);
+        const T negative = -k;
+        T reduced = fma_(negative, L::natural, clamped);
+        reduced = fma_(negative, L::remainder, reduced);
+        const T significand = fma_(reduced, horner<1>(series, reduced), T(1));
+        auto scale = [](T e) { return from_bits(bits(add(e, L::exponent)) << L::mantissa); };
+        if (!(fabs(k) > L::normal)) return mul(significand, scale(k));
+        const T half = sub(fma_(k, T(0.5), L::round), L::round);
+        const T rest = sub(k, half);
+        return mul(mul(significand, scale(half)), scale(rest));
+    }
+
+    // ---- ln x (logarithm.hpp:90-126) --------------------------------------------------------------
+    template <typename T> __device__ __forceinline__ T logarithm(T x) {
+        using L = Limits<T>;
+        using U = typename L::U;
+        constexpr Poly<T, L::log_terms> series = reciprocals<T, L::log_terms>();
+        const bool small = x < L::tiny;
+        const T scaled = small ? mul(x, L::lift) : x;
+        const U pattern = bits(scaled);
+        T exponent = sub(from_bits((pattern >> L::mantissa) | bits(L::magnitude)), L::exponent);
+        T mantissa = from_bits((pattern & L::fraction) | L::one);
+        const bool large = mantissa > L::root2;
+        mantissa = large ? mul(mantissa, T(0.5)) : mantissa;
+        exponent = large ? add(exponent, T(1)) : exponent;
+        exponent = small ? sub(exponent, L::shift) : exponent;
+        const T fraction = sub(mantissa, T(1));
+        const T ratio = div(fraction, add(fraction, T(2)));
+        const T square = mul(ratio, ratio);
+        const T tail = mul(square, horner<0>(series, square));
+        const T half = mul(mul(fraction, fraction), T(0.5));
+        const T inner = fma_(ratio, add(half, tail), mul(exponent, L::remainder));
+        T result = sub(mul(exponent, L::natural), sub(sub(half, inner), fraction));
+        const T infinity = from_bits(L::infinity);
+        if (x == infinity) result = x;
+        if (x == T(0)) result = -infinity;
+        if (x < T(0)) result = from_bits(L::quiet);
+        if (is_nan(x)) result = x;
+        return result;
+    }
+
+    // ---- sin / cos (trigonometry.hpp:162-207) -----------------------------------------------------
+    __device__ __forceinline__ float far_circular(float x, bool phase) {
+        const double d = static_cast<double>(x);
+        return static_cast<float>(phase ? cos(d) : sin(d));
+    }
+    __device__ __forceinline__ double far_circular(double x, bool phase) { return phase ? cos(x) : sin(x); }
+
+    template <bool phase, typename T> __device__ __forceinline__ T circular(T x) {
+        using L = Limits<T>;
+        using U = typename L::U;
+        constexpr Poly<T, L::sin_terms> odd = alternating<T, L::sin_terms, 1>();
+        constexpr Poly<T, L::cos_terms> even = alternating<T, L::cos_terms, 0>();
+        const T shifted = fma_(x, L::quadrant, L::round);
+        const T quarters = sub(shifted, L::round);
+        const T negative = -quarters;
+        T reduced = fma_(negative, L::q0, x);
+        reduced = fma_(negative, L::q1, reduced);
+        reduced = fma_(negative, L::q2, reduced);
+        reduced = fma_(negative, L::q3, reduced);
+        const T square = mul(reduced, reduced);
+        const T sine = fma_(mul(reduced, square), horner<1>(odd, square), reduced);
+        const T cosine = fma_(square, horner<1>(even, square), T(1));
+        U quadrant = bits(shifted);
+        if (phase) quadrant ^= quadrant << 1;
+        const U flip = (quadrant & U(2)) << (L::width - 2);
+        const bool swap = (bits(shifted) & U(1)) != 0;
+        T result = phase ? (swap ? sine : cosine) : (swap ? cosine : sine);
+        result = from_bits(bits(result) ^ flip);
+        if (!(x <= L::reach && x >= -L::reach)) result = far_circular(x, phase);
+        return result;
+    }
+
+    // ---- the C-library functions (library.hpp:22-35), in double, rounded once -------------------
+    template <int code> __device__ __forceinline__ double library_d(double x) {
+        if constexpr (code == kAsin) return asin(x);
+        else if constexpr (code == kAcos) return acos(x);
+        else if constexpr (code == kAtan) return atan(x);
+        else if constexpr (code == kSinh) return sinh(x);
+        else if constexpr (code == kCosh) return cosh(x);
+        else if constexpr (code == kTanh) return tanh(x);
+        else if constexpr (code == kAsinh) return asinh(x);
+        else if constexpr (code == kAcosh) return acosh(x);
+        else return atanh(x);
+    }
+    template <int code, typename T> __device__ __forceinline__ T library(T x) {
+        return static_cast<T>(library_d<code>(static_cast<double>(x)));
+    }
+
+    // ---- one code on one element (operation.hpp:25-110) ------------------------------------------
+    template <int code, typename T> __device__ __forceinline__ T apply(T a, T b, T c, bool tail) {
+        using L = Limits<T>;
+        const T one = T(1);
+        if constexpr (code == kCopy) return a;
+        else if constexpr (code == kNegate) return from_bits(bits(a) ^ L::sign);
+        else if constexpr (code == kAbsolute) return from_bits(bits(a) & ~L::sign);
+        else if constexpr (code == kRoot) return root(a);
+        else if constexpr (code == kExponential) return exponential(a);
+        else if constexpr (code == kLogarithm) return logarithm(a);
+        else if constexpr (code == kSin) return circular<false>(a);
+        else if constexpr (code == kCos) return circular<true>(a);
+        else if constexpr (code == kTan) return div(circular<false>(a), circular<true>(a));
+        else if constexpr (code == kAsin || code == kAcos || code == kAtan || code == kSinh || code == kCosh ||
+                           code == kTanh || code == kAsinh || code == kAcosh || code == kAtanh)
+            return library<code>(a);
+        else if constexpr (code == kCsc) return div(one, circular<false>(a));
+        else if constexpr (code == kSec) return div(one, circular<true>(a));
+        else if constexpr (code == kCot) return div(one, div(circular<false>(a), circular<true>(a)));
+        else if constexpr (code == kAcsc) return library<kAsin>(div(one, a));
+        else if constexpr (code == kAsec) return library<kAcos>(div(one, a));
+        else if constexpr (code == kAcot) return library<kAtan>(div(one, a));
+        else if constexpr (code == kCsch) return div(one, library<kSinh>(a));
+        else if constexpr (code == kSech) return div(one, library<kCosh>(a));
+        else if constexpr (code == kCoth) return div(one, library<kTanh>(a));
+        else if constexpr (code == kAcsch) return library<kAsinh>(div(one, a));
+        else if constexpr (code == kAsech) return library<kAcosh>(div(one, a));
+        else if constexpr (code == kAcoth) return library<kAtanh>(div(one, a));
+        else if constexpr (code == kAdd) return add(a, b);
+        else if constexpr (code == kSubtract) return sub(a, b);
+        else if constexpr (code == kMultiply) return mul(a, b);
+        else if constexpr (code == kDivide) return div(a, b);
+        else if constexpr (code == kMinimum) return tail ? smin(a, b) : vmin(a, b);
+        else if constexpr (code == kMaximum) return tail ? smax(a, b) : vmax(a, b);
+        else return fma_(a, b, c);
+    }
+
+} // namespace sci_cuda

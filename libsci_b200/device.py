@@ -1,0 +1,258 @@
+"""Python host layer over the C ABI: a CUDA ``Device`` and arrays that live on it.
+
+Mirrors the parts of libsci's C++ front end the north-star path uses:
+
+- ``Device`` is ``sci::Device`` with a CUDA target (include/core/drivers/device.hpp:27-89):
+  ``execute`` / ``reduce`` / ``synchronize`` / ``name`` and memory.
+- ``DeviceArray`` is a one-dimensional ``sci::Array`` placed on that device (include/array/array.hpp:
+  ``to(device)`` / ``host()`` at :223-237). It records itself into chunks as an input
+  (include/array/reference.hpp:45).
+- ``evaluate`` is ``assign`` (include/array/expression.hpp:158-185) and ``sum`` / ``mean`` /
+  ``minimum`` / ``maximum`` / ``dot`` are the reductions of include/operations/reduce.hpp:19-42 and
+  include/linear/product.hpp:72-76, including ``mean`` as ``float(sum) / float(count)`` in the
+  element type.
+
+Every call goes through libsci_cuda.so; errors raise ``SciCudaError`` and nothing runs on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import chunk as C
+from .native import MEMORY_DEVICE, MEMORY_MANAGED, SciCudaError, check, lib
+
+
+class Device:
+    def __init__(self, ordinal: int = 0):
+        handle = ctypes.c_void_p()
+        status = lib.sci_cuda_open(ordinal, ctypes.byref(handle))
+        if status != 0:
+            raise SciCudaError(status, f"cannot open CUDA device {ordinal}")
+        self.handle = handle
+
+    # -- lifetime -------------------------------------------------------------------------------
+    def close(self) -> None:
+        if self.handle:
+            check(lib.sci_cuda_close(self.handle))
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def name(self) -> str:
+        return lib.sci_cuda_name(self.handle).decode()
+
+    @property
+    def stream(self) -> int:
+        return lib.sci_cuda_stream(self.handle)
+
+    def synchronize(self) -> None:
+        check(lib.sci_cuda_synchronize(self.handle), self.handle)
+
+    def jit_wait(self) -> None:
+        """Waits for queued NVRTC specialisations (chunks run on the interpreter until then)."""
+        check(lib.sci_cuda_jit_wait(self.handle), self.handle)
+
+    # -- memory ---------------------------------------------------------------------------------
+    def allocate(self, nbytes: int, managed: bool = False) -> int:
+        pointer = ctypes.c_void_p()
+        kind = MEMORY_MANAGED if managed else MEMORY_DEVICE
+        check(lib.sci_cuda_allocate(self.handle, nbytes, kind, ctypes.byref(pointer)), self.handle)
+        return pointer.value
+
+    def dispose(self, pointer: int) -> None:
+        check(lib.sci_cuda_dispose(self.handle, pointer), self.handle)
+
+    def empty(self, count: int, dtype=np.float32) -> "DeviceArray":
+        dtype = np.dtype(dtype)
+        return DeviceArray(self, self.allocate(max(count, 1) * dtype.itemsize), count, dtype)
+
+    def array(self, values, dtype=None) -> "DeviceArray":
+        """Array.to(device): a device copy of host values (array.hpp:223-228)."""
+        host = np.ascontiguousarray(values, dtype=dtype)
+        out = self.empty(host.size, host.dtype)
+        out.upload(host)
+        return out
+
+    # -- chunks ---------------------------------------------------------------------------------
+    def execute(self, chunk: C.Chunk, output: int, count: int) -> None:
+        check(lib.sci_cuda_execute(self.handle, ctypes.byref(chunk), output, count), self.handle)
+
+    def reduce_chunk(self, chunk: C.Chunk, fold: int, count: int) -> float:
+        result = ctypes.c_double()
+        check(lib.sci_cuda_reduce(self.handle, ctypes.byref(chunk), fold, count, ctypes.byref(result)), self.handle)
+        return result.value
+
+    def reduce_async(self, chunk: C.Chunk, fold: int, count: int, device_result: int) -> None:
+        check(lib.sci_cuda_reduce_async(self.handle, ctypes.byref(chunk), fold, count, device_result), self.handle)
+
+    def evaluate(self, expression, out: "DeviceArray | None" = None) -> "DeviceArray":
+        """assign(target, expression) (expression.hpp:158-185); allocates the target if needed."""
+        expr = C._operand(expression, None)
+        if out is None:
+            out = self.empty(expr.count, expr.dtype)
+        chunk = C.record_output(expr)
+        if not chunk.valid():
+            raise SciCudaError(1, "expression outgrew the 64-entry chunk")
+        self.execute(chunk, out.pointer, expr.count)
+        return out
+
+    def reduce(self, expression, fold: int) -> float:
+        expr = C._operand(expression, None)
+        chunk = C.record_reduce(expr)
+        if not chunk.valid():
+            raise SciCudaError(1, "expression outgrew the 64-entry chunk")
+        value = self.reduce_chunk(chunk, fold, expr.count)
+        return float(expr.dtype.type(value))  # static_cast<element>(device->reduce(...)) (expression.hpp:198)
+
+
+class DeviceArray:
+    """A one-dimensional array in this device's memory."""
+
+    def __init__(self, device: Device, pointer: int, count: int, dtype):
+        self.device = device
+        self.pointer = int(pointer)
+        self.count = int(count)
+        self.dtype = np.dtype(dtype)
+
+    @property
+    def nbytes(self) -> int:
+        return self.count * self.dtype.itemsize
+
+    def expression(self) -> C.Reference:
+        return C.Reference(self.pointer, self.count, self.dtype, self.device)
+
+    def offset(self, elements: int, count: int | None = None) -> "DeviceArray":
+        """A view starting `elements` in (not owning memory)."""
+        view = DeviceArray.__new__(DeviceArray)
+        view.device, view.dtype = self.device, self.dtype
+        view.pointer = self.pointer + elements * self.dtype.itemsize
+        view.count = self.count - elements if count is None else count
+        view._view = True
+        return view
+
+    def upload(self, host: np.ndarray) -> None:
+        host = np.ascontiguousarray(host, dtype=self.dtype)
+        check(lib.sci_cuda_upload(self.device.handle, self.pointer, host.ctypes.data, host.nbytes), self.device.handle)
+        self.device.synchronize()
+
+    def numpy(self) -> np.ndarray:
+        """Array.host(): waits for queued work, then copies back (array.hpp:232-237)."""
+        out = np.empty(self.count, self.dtype)
+        check(lib.sci_cuda_download(self.device.handle, out.ctypes.data, self.pointer, out.nbytes), self.device.handle)
+        self.device.synchronize()
+        return out
+
+    def free(self) -> None:
+        if self.pointer and not getattr(self, "_view", False):
+            self.device.dispose(self.pointer)
+            self.pointer = 0
+
+    # operators build expressions
+    def __add__(self, other):
+        return self.expression() + other
+
+    def __radd__(self, other):
+        return other + self.expression()
+
+    def __sub__(self, other):
+        return self.expression() - other
+
+    def __rsub__(self, other):
+        return other - self.expression()
+
+    def __mul__(self, other):
+        return self.expression() * other
+
+    def __rmul__(self, other):
+        return other * self.expression()
+
+    def __truediv__(self, other):
+        return self.expression() / other
+
+    def __rtruediv__(self, other):
+        return other / self.expression()
+
+    def __neg__(self):
+        return -self.expression()
+
+
+# ---- numpy-named front end (include/operations/unary.hpp, binary.hpp, reduce.hpp) -------------
+def _unary(code):
+    def op(item):
+        return C.unary(code, item)
+
+    op.__name__ = code
+    return op
+
+
+for _code in C.UNARY:
+    globals()[_code] = _unary(_code)
+negate = _unary("negate")
+
+
+def minimum(first, second=None):
+    """Elementwise with two operands, a reduction with one (include/sci.hpp: numpy.minimum / min)."""
+    if second is None:
+        return _device_of(first).reduce(first, C.MINIMUM)
+    return C.binary("minimum", first, second)
+
+
+def maximum(first, second=None):
+    if second is None:
+        return _device_of(first).reduce(first, C.MAXIMUM)
+    return C.binary("maximum", first, second)
+
+
+def add(a, b):
+    return C.binary("add", a, b)
+
+
+def subtract(a, b):
+    return C.binary("subtract", a, b)
+
+
+def multiply(a, b):
+    return C.binary("multiply", a, b)
+
+
+def divide(a, b):
+    return C.binary("divide", a, b)
+
+
+def sum(item):  # noqa: A001 - numpy name
+    return _device_of(item).reduce(item, C.SUM)
+
+
+def mean(item):
+    """reduce.hpp:24-28: sum / count in the element type."""
+    expr = C._operand(item, None)
+    if expr.count == 0:
+        return 0.0
+    total = expr.dtype.type(sum(item))
+    return float(total / expr.dtype.type(expr.count))
+
+
+def dot(first, second):
+    """linear::dot: reduce(first * second, sum) (product.hpp:72-76), contracted on the device."""
+    return _device_of(first).reduce(C.binary("multiply", first, second), C.SUM)
+
+
+def _device_of(item) -> Device:
+    if isinstance(item, DeviceArray):
+        return item.device
+    expr = C._operand(item, None)
+    for leaf in expr.leaves():
+        if getattr(leaf, "device", None) is not None:
+            return leaf.device
+    raise SciCudaError(1, "expression has no operand on a device")
+
+
+__all__ = ["Device", "DeviceArray", "minimum", "maximum", "add", "subtract", "multiply", "divide", "sum", "mean",
+           "dot", "negate"] + list(C.UNARY)

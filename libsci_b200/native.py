@@ -1,0 +1,78 @@
+"""ctypes binding of libsci_cuda.so (include/sci_cuda.h).
+
+The library is built in-tree by ``python -m libsci_b200.build`` (or ``__graft_entry__.build()``).
+There is no fallback: if the shared library is missing or fails to load, importing this module
+raises, so nothing can silently run on the CPU instead of the B200 kernels.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+from .chunk import ChunkStruct
+
+LIBRARY = Path(__file__).resolve().parent / "libsci_cuda.so"
+
+OK, INVALID, MEMORY, LAUNCH, UNSUPPORTED, DEVICE, TIMEOUT, COMPILE = range(8)
+STATUS = {
+    OK: "ok", INVALID: "invalid argument", MEMORY: "out of device memory", LAUNCH: "CUDA launch error",
+    UNSUPPORTED: "unsupported", DEVICE: "no usable sm_100 device", TIMEOUT: "device wait timed out",
+    COMPILE: "NVRTC compile failed",
+}
+MEMORY_DEVICE, MEMORY_MANAGED = 0, 1
+
+
+class SciCudaError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+def _load() -> ctypes.CDLL:
+    if not LIBRARY.exists():
+        raise ImportError(f"{LIBRARY} is not built; run `python -m libsci_b200.build` (needs nvcc)")
+    lib = ctypes.CDLL(str(LIBRARY))
+    c_ctx = ctypes.c_void_p
+    P = ctypes.POINTER
+    sig = {
+        "sci_cuda_open": (ctypes.c_int, [ctypes.c_uint32, P(c_ctx)]),
+        "sci_cuda_close": (ctypes.c_int, [c_ctx]),
+        "sci_cuda_name": (ctypes.c_char_p, [c_ctx]),
+        "sci_cuda_synchronize": (ctypes.c_int, [c_ctx]),
+        "sci_cuda_last_error": (ctypes.c_int, [c_ctx, ctypes.c_char_p, ctypes.c_size_t]),
+        "sci_cuda_stream": (ctypes.c_void_p, [c_ctx]),
+        "sci_cuda_allocate": (ctypes.c_int, [c_ctx, ctypes.c_uint64, ctypes.c_uint32, P(ctypes.c_void_p)]),
+        "sci_cuda_dispose": (ctypes.c_int, [c_ctx, ctypes.c_void_p]),
+        "sci_cuda_upload": (ctypes.c_int, [c_ctx, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64]),
+        "sci_cuda_download": (ctypes.c_int, [c_ctx, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64]),
+        "sci_cuda_execute": (ctypes.c_int, [c_ctx, P(ChunkStruct), ctypes.c_void_p, ctypes.c_uint64]),
+        "sci_cuda_reduce": (ctypes.c_int, [c_ctx, P(ChunkStruct), ctypes.c_uint32, ctypes.c_uint64, P(ctypes.c_double)]),
+        "sci_cuda_reduce_async": (ctypes.c_int, [c_ctx, P(ChunkStruct), ctypes.c_uint32, ctypes.c_uint64, ctypes.c_void_p]),
+        "sci_cuda_jit_wait": (ctypes.c_int, [c_ctx]),
+    }
+    optional = {
+        "sci_cuda_product": (ctypes.c_int, [c_ctx, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype, fn.argtypes = res, args
+    for name, (res, args) in optional.items():
+        if hasattr(lib, name):
+            fn = getattr(lib, name)
+            fn.restype, fn.argtypes = res, args
+    return lib
+
+
+lib = _load()
+
+
+def check(status: int, context=None) -> None:
+    if status == OK:
+        return
+    message = ""
+    if context:
+        buffer = ctypes.create_string_buffer(512)
+        lib.sci_cuda_last_error(context, buffer, 512)
+        message = buffer.value.decode(errors="replace")
+    raise SciCudaError(status, message)

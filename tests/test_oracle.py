@@ -1,0 +1,145 @@
+"""The oracle, pinned (CPU only).
+
+oracle/sci_oracle.cpp restates libsci's CPU arithmetic; here it is checked bit for bit against
+libsci's own CPU path compiled from the reference sources (oracle/_ref/libsci_ref.so) and against
+the committed golden vectors, which tests/golden/make_golden.py produced from that same library.
+The reference's own pins (tests/operations/test_binary.cpp, test_unary.cpp, test_reduce.cpp,
+tests/linear/test_decompose.cpp, test_solve.cpp) are restated against the oracle as well.
+"""
+import ctypes
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from libsci_b200 import chunk as C
+from tests import _oracle
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+def host_inputs(dtype, count, seed):
+    rng = np.random.default_rng(seed)
+    x = np.concatenate([rng.standard_normal(count // 2) * 3, rng.uniform(-100, 100, count - count // 2)]).astype(dtype)
+    y = rng.uniform(0, 10, count).astype(dtype)
+    specials = np.array([0.0, -0.0, np.inf, -np.inf, np.nan, 1e-45, -1e-45, 1e-38, 3e-39, 88.7, 89.5, -103.9,
+                         -104.5, 1e6, 2e6, -3e7, 1e30, 710.0, -746.0], dtype)
+    x[: specials.size] = specials
+    y[::97] = -0.0
+    y[::101] = np.nan
+    return x, y
+
+
+def expression(code, a, b):
+    if code < C.CODE["add"]:
+        return C.Node(C.CODES[code], [a])
+    if code == C.CODE["fuse"]:
+        return a * b + b
+    return C.Node(C.CODES[code], [a, b])
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_oracle_matches_the_reference_bit_for_bit(oracle, reference, dtype):
+    n = 20011  # crosses 1024-element blocks, leaves a ragged tail
+    x, y = host_inputs(dtype, n, seed=3)
+    a, b = C.Reference(x.ctypes.data, n, dtype), C.Reference(y.ctypes.data, n, dtype)
+    for code in range(C.CODE["fuse"] + 1):
+        chunk = C.record_output(expression(code, a, b))
+        mine = _oracle.execute(oracle, chunk, n, dtype)
+        theirs = _oracle.execute(reference, chunk, n, dtype)
+        bad = _oracle.mismatches(mine, theirs)
+        assert bad.size == 0, f"{C.CODES[code]}: {bad.size} differ"
+
+
+def test_oracle_reductions_against_the_reference(oracle, reference):
+    n = 300_007
+    x, y = host_inputs(np.float32, n, seed=4)
+    x = np.nan_to_num(x, nan=1.0, posinf=2.0, neginf=-2.0)
+    y = np.nan_to_num(y, nan=0.5)
+    a, b = C.Reference(x.ctypes.data, n, np.float32), C.Reference(y.ctypes.data, n, np.float32)
+    for expr in (C.unary("sin", a) * C.unary("cos", b), C.unary("exponential", -a * a), a * b):
+        chunk = C.record_reduce(expr)
+        for fold in (C.SUM, C.MINIMUM, C.MAXIMUM):
+            mine = _oracle.reduce(oracle, chunk, fold, n)
+            theirs = _oracle.reduce(reference, chunk, fold, n)
+            if fold == C.SUM:
+                # the reference folds float partials per 1024-block (dispatch.cpp:121-150)
+                assert abs(mine - theirs) <= 1e-4 * np.abs(x).sum()
+            else:
+                assert mine == theirs
+
+
+def test_golden_vectors(oracle):
+    """Per-code outputs of libsci's CPU path, committed by tests/golden/make_golden.py."""
+    data = np.load(GOLDEN / "codes.npz")
+    for dtype, suffix in ((np.float32, "f32"), (np.float64, "f64")):
+        x, y = data[f"x_{suffix}"], data[f"y_{suffix}"]
+        n = x.size
+        a, b = C.Reference(x.ctypes.data, n, dtype), C.Reference(y.ctypes.data, n, dtype)
+        for code in range(C.CODE["fuse"] + 1):
+            chunk = C.record_output(expression(code, a, b))
+            mine = _oracle.execute(oracle, chunk, n, dtype)
+            want = data[f"{C.CODES[code]}_{suffix}"]
+            assert _oracle.mismatches(mine, want).size == 0, C.CODES[code]
+
+
+def test_golden_workloads(oracle):
+    """The plain fused workload (t, e, s) at 4099 elements, from libsci's CPU path."""
+    data = np.load(GOLDEN / "workloads.npz")
+    a, b, c = data["a"], data["b"], data["c"]
+    n = a.size
+    ra, rb, rc = (C.Reference(v.ctypes.data, n, np.float32) for v in (a, b, c))
+    t = _oracle.execute(oracle, C.record_output(ra * rb + rc * 2.0), n, np.float32)
+    assert _oracle.mismatches(t, data["t"]).size == 0
+    rt = C.Reference(t.ctypes.data, n, np.float32)
+    e = _oracle.execute(oracle, C.record_output(C.unary("exponential", rt) * 0.5), n, np.float32)
+    assert _oracle.mismatches(e, data["e"]).size == 0
+    s = _oracle.reduce(oracle, C.record_reduce(C.unary("sin", rt)), C.SUM, n)
+    assert abs(s - float(data["s"])) <= 1e-5 * abs(float(data["s"]))
+    rows = np.zeros(64, np.uint64)
+    m = data["lu_input"].copy()
+    oracle.sci_oracle_factor_f32(m.ctypes.data, rows.ctypes.data, 64)
+    assert np.array_equal(rows, data["lu_rows"])
+    assert _oracle.mismatches(m.ravel(), data["lu_factors"].ravel()).size == 0
+
+
+def test_reference_pins_restated(oracle):
+    """tests/operations/test_binary.cpp:26-50 and test_unary.cpp:76-102 against the oracle."""
+    n = 300_000
+    first = (np.float64(-3.0) + np.arange(n) * (8.0 / (n - 1.0))).astype(np.float32)
+    second = (np.float64(2.0) + np.arange(n) * (5.0 / (n - 1.0))).astype(np.float32)
+    a, b = C.Reference(first.ctypes.data, n, np.float32), C.Reference(second.ctypes.data, n, np.float32)
+    run = lambda e: _oracle.execute(oracle, C.record_output(e), n, np.float32)
+    assert np.array_equal(run(a + b), first + second)
+    assert np.array_equal(run(a / b), first / second)
+    assert np.array_equal(run(C.binary("minimum", a, b)), np.minimum(first, second))
+    assert np.array_equal(run(a + 2.0), first + np.float32(2.0))
+    chunk = C.record_output(a * b + a)
+    assert C.CODES[chunk.instructions[0].code] == "fuse" and chunk.length == 1
+    wide = (np.float64(-4.0) + np.arange(100_000) * (8.0 / 99_999.0)).astype(np.float32)
+    w = C.Reference(wide.ctypes.data, wide.size, np.float32)
+    for name, fn in (("exponential", np.exp), ("sin", np.sin), ("cos", np.cos), ("tanh", np.tanh), ("atan", np.arctan)):
+        got = _oracle.execute(oracle, C.record_output(C.unary(name, w)), wide.size, np.float32).astype(np.float64)
+        want = fn(wide.astype(np.float64))
+        assert np.all(np.abs(got - want) <= 1e-5 * np.maximum(1.0, np.abs(want))), name
+
+
+def test_factor_restates_the_reference(oracle, reference):
+    """LU pivot order and factors: decompose.hpp:29-72 (zero first pivot: test_decompose.cpp:21-36)."""
+    a = np.array([[0, 2, 1], [4, 1, 3], [2, 5, 7]], np.float64)
+    for lib, fn in ((oracle, "sci_oracle_factor_f64"), (reference, "sci_ref_factor_f64")):
+        m = a.copy()
+        rows = np.zeros(3, np.uint64)
+        getattr(lib, fn)(m.ctypes.data, rows.ctypes.data, 3)
+        lower = np.tril(m, -1) + np.eye(3)
+        upper = np.triu(m)
+        assert np.allclose(a[rows.astype(int)], lower @ upper, atol=1e-12)
+        assert list(rows) == [1, 2, 0]
+    rng = np.random.default_rng(9)
+    g = rng.standard_normal((128, 128)).astype(np.float32)
+    m1, m2 = g.copy(), g.copy()
+    r1, r2 = np.zeros(128, np.uint64), np.zeros(128, np.uint64)
+    oracle.sci_oracle_factor_f32(m1.ctypes.data, r1.ctypes.data, 128)
+    reference.sci_ref_factor_f32(m2.ctypes.data, r2.ctypes.data, 128)
+    assert np.array_equal(r1, r2)
+    assert _oracle.mismatches(m1.ravel(), m2.ravel()).size == 0
