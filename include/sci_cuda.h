@@ -131,6 +131,20 @@ int sci_cuda_reduce(sci_cuda_context *context, const sci_chunk *chunk, uint32_t 
 /* The same reduction, queued: the double result is written to device memory `device_result`. */
 int sci_cuda_reduce_async(sci_cuda_context *context, const sci_chunk *chunk, uint32_t fold, uint64_t count,
                           double *device_result);
+/* No counterpart in the reference. The same reduction for callers that may not allocate device
+ * memory (a host framework that owns the GPU heap through its own pool, a plugin inside one, a
+ * latency-critical thread where an allocation would synchronize the device). It needs no context:
+ * it runs on the calling thread's current device and on `stream` (a cudaStream_t; 0 is the legacy
+ * default stream), reads the chunk's inputs from device memory and writes the double result to
+ * `device_result`, both on that device. Its scratch is one fixed 49,408-byte array compiled into
+ * the library, holding partials for at most 4096 blocks: `blocks` = 0 picks the launch width,
+ * a larger value than 4096 is rejected with SCI_CUDA_ERROR_INVALID. It calls no cudaMalloc or
+ * cudaFree. Every call on a device shares that array: calls whose kernels may overlap on the GPU
+ * race and must be ordered by the caller (one stream, or events). The first call on a device
+ * looks up the array's device address; make it before capturing the stream into a graph. On
+ * failure a message is written to `message` (may be null). */
+int sci_cuda_reduce_noalloc(const sci_chunk *chunk, uint32_t fold, uint64_t count, double *device_result,
+                            void *stream, uint32_t blocks, char *message, size_t message_length);
 /* Waits until every queued NVRTC specialisation has been compiled and loaded
  * (vulkan::Compiler::loop, src/core/drivers/vulkan/compiler.cpp:184-222, compiles in the
  * background the same way; a chunk runs on the interpreter until its kernel is ready).
