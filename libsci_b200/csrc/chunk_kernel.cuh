@@ -1,20 +1,21 @@
 // chunk_kernel.cuh -- the persistent, TMA-fed chunk interpreter for sm_100a.
 //
 // One kernel source serves two programs:
-//  - Dynamic: the generic interpreter. The decoded bytecode is staged in shared memory, each
-//    instruction is dispatched with a warp-uniform switch, and temporaries live in a
-//    shared-memory slot file (one column per thread, so no synchronisation is needed).
+//  - Dynamic: the generic interpreter. Each instruction is read from the launch's constant bank and
+//    dispatched with a warp-uniform switch; temporaries live in a shared-memory slot file (one
+//    column per thread, so no synchronisation is needed).
 //  - Baked<...>: the same kernel with the bytecode fixed at compile time (an NVRTC
 //    specialisation keyed by the chunk's signature, chunk.hpp:209-226). The instruction loop
 //    unrolls, every code folds to straight-line math and temporaries become registers.
 // Both stream their inputs the same way: a persistent grid (a few CTAs per SM) walks tiles of
-// 4 x blockDim elements; one elected thread issues a 1-D TMA bulk copy (cp.async.bulk) per input
-// per tile into a ring of shared-memory stages that an mbarrier guards, so several tiles per
-// input are in flight while the block computes. Results leave with 128-bit stores. Reductions
-// fold in registers, then a warp shuffle, then the block, then a single-pass global fold: every
-// block writes one double partial and the last block to arrive (an atomic ticket) folds them in
-// block order, so the result is deterministic for a given launch shape and a*b is never stored
-// for sum(a*b).
+// 32 bytes x blockDim per input (8 floats or 4 doubles per thread); one elected thread issues a
+// 1-D TMA bulk copy (cp.async.bulk) per input per tile into a ring of shared-memory stages that
+// an mbarrier guards, so several tiles per input are in flight while the block computes. Results
+// leave with 128-bit stores. Reductions fold each thread's lanes in the element type, carry the
+// running total in double, then fold a warp (shuffle), the block, and finally the grid in a
+// single pass: every block writes one double partial and the last block to arrive (an atomic
+// ticket) folds them in block order, so the result is deterministic for a given launch shape and
+// a*b is never stored for sum(a*b).
 //
 // Behavioural reference: the Vulkan interpreter and its entry points
 // (shaders/interpreter.slang:163-248, shaders/common/entries.slang:17-80), the CPU sweep
@@ -27,10 +28,16 @@
 namespace sci_cuda {
 
     constexpr int kCapacity = 64;
-    constexpr int kLanes = 4;          // elements each thread carries through the chunk per tile
     constexpr int kMaxStages = 4;
-    constexpr int kMaxBlocks = 4096;   // bound on the persistent grid (partials of a reduction)
+    constexpr int kMaxBlocks = 4096;           // bound on the persistent grid (partials of a reduction)
     constexpr unsigned kWaitLimit = 1u << 22;  // bounded spin on an mbarrier phase
+
+    // A thread carries 32 bytes of each input through the chunk per tile: two 16-byte vectors.
+    template <typename T> struct Lanes {
+        static constexpr int count = 32 / sizeof(T);   // elements per thread per tile
+        static constexpr int width = 16 / sizeof(T);   // elements per 16-byte vector
+        static constexpr int vectors = count / width;  // 16-byte vectors per thread per tile
+    };
 
     enum Mode : int { kEvaluate = 0, kReduce = 1, kDot = 2 };
     enum Slot : int { kInput = 0x00, kLiteral = 0x40, kTemporary = 0x80, kOutput = 0xC0, kNone = 0xFF, kTypes = 0xC0 };
@@ -59,6 +66,7 @@ namespace sci_cuda {
         unsigned int fold;         // 0 sum, 1 minimum, 2 maximum
         unsigned int dot_left, dot_right;
         unsigned int stages;       // TMA ring depth, 0 when the inputs are read directly
+        unsigned int tailed;       // the chunk has a minimum or maximum (loop-tail forms matter)
         T constants[kCapacity];
         const T *inputs[kCapacity];
         T *output;
@@ -79,6 +87,12 @@ namespace sci_cuda {
     template <class Chunk> struct Baked {
         static constexpr bool baked = true;
         using chunk = Chunk;
+        __host__ __device__ static constexpr bool tailed() {
+            for (int i = 0; i < Chunk::length; ++i) {
+                if (Chunk::steps[i].code == kMinimum || Chunk::steps[i].code == kMaximum) return true;
+            }
+            return false;
+        }
     };
 
     template <int... I> struct Sequence {};
@@ -96,22 +110,11 @@ namespace sci_cuda {
         for_each(f, typename MakeSequence<N>::type{});
     }
 
-    // ---- element placement ---------------------------------------------------------------------
-    // A thread's four elements sit in 16-byte vectors: for float one vector, for double two. Lane e
-    // of thread t in a tile starting at `base` is element base + (e / W) * (W * threads) + W * t + e % W,
-    // with W = 16 / sizeof(T), so every 128-bit shared or global access is contiguous across a warp.
-    template <typename T> struct Place {
-        static constexpr int W = 16 / sizeof(T);
-        __device__ static __forceinline__ unsigned offset(int lane, unsigned t, unsigned threads) {
-            return (lane / W) * (W * threads) + W * t + lane % W;
-        }
-    };
-
     // ---- applying one code to a thread's lanes -------------------------------------------------
     template <int code, typename T>
     __device__ __forceinline__ void apply_lanes(const T *a, const T *b, const T *c, T *r, const bool *tail) {
 #pragma unroll
-        for (int e = 0; e < kLanes; ++e) r[e] = apply<code>(a[e], b[e], c[e], tail[e]);
+        for (int e = 0; e < Lanes<T>::count; ++e) r[e] = apply<code>(a[e], b[e], c[e], tail[e]);
     }
 
     template <typename T>
@@ -127,7 +130,7 @@ namespace sci_cuda {
 #undef SCI_CASE
         default:
 #pragma unroll
-            for (int e = 0; e < kLanes; ++e) r[e] = T(0);
+            for (int e = 0; e < Lanes<T>::count; ++e) r[e] = T(0);
         }
     }
 
@@ -169,7 +172,7 @@ namespace sci_cuda {
     }
 
     // ---- 16-byte vector access ------------------------------------------------------------------
-    template <typename T> __device__ __forceinline__ void load4(const T *p, T *v) {
+    template <typename T> __device__ __forceinline__ void load16(const T *p, T *v) {
         if constexpr (sizeof(T) == 4) {
             const float4 q = *reinterpret_cast<const float4 *>(p);
             v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
@@ -178,7 +181,7 @@ namespace sci_cuda {
             v[0] = q.x, v[1] = q.y;
         }
     }
-    template <typename T> __device__ __forceinline__ void store4(T *p, const T *v) {
+    template <typename T> __device__ __forceinline__ void store16(T *p, const T *v) {
         if constexpr (sizeof(T) == 4) {
             *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
         } else {
@@ -187,35 +190,51 @@ namespace sci_cuda {
     }
 
     // ---- the per-block working state -------------------------------------------------------------
+    // Lane e of thread t sits at in-tile position (e / W) * (W * threads) + W * t + e % W, with W the
+    // elements of a 16-byte vector, so every 128-bit shared or global access is contiguous across a
+    // warp. The positions are fixed per thread; only the tile's base moves.
     template <typename T, class Program> struct Work {
+        static constexpr int N = Lanes<T>::count, W = Lanes<T>::width, V = Lanes<T>::vectors;
         const Launch<T> &L;
         const T *stage;     // this tile's staged inputs (A x tile elements), or null for direct reads
         T *slots;           // the dynamic program's temporaries (temporaries x tile), shared memory
         unsigned long long base;
-        unsigned tile;      // elements in a full tile (4 x threads)
+        unsigned tile;      // elements in a full tile (N x threads)
         unsigned live;      // elements of this tile that exist
-        unsigned t, threads;
-        bool tail[kLanes];
-        unsigned idx[kLanes];  // in-tile position of each lane
+        unsigned first;     // position of this thread's first vector
+        bool tailed;        // whether loop-tail forms can matter for this chunk
+        bool tail[N];
 
-        __device__ __forceinline__ void prepare() {
+        __device__ __forceinline__ Work(const Launch<T> &launch, T *slot_file, unsigned threads, unsigned t)
+            : L(launch), stage(nullptr), slots(slot_file), base(0), tile(N * threads), live(N * threads),
+              first(W * t), tailed(false) {
+            if constexpr (Program::baked) tailed = Program::tailed();
+            else tailed = launch.tailed != 0;
 #pragma unroll
-            for (int e = 0; e < kLanes; ++e) {
-                idx[e] = Place<T>::offset(e, t, threads);
-                tail[e] = base + idx[e] >= L.tail_start;
+            for (int e = 0; e < N; ++e) tail[e] = false;
+        }
+
+        __device__ __forceinline__ unsigned position(int e) const { return (e / W) * (tile / V) + first + e % W; }
+
+        __device__ __forceinline__ void at(unsigned long long tile_base, unsigned tile_live, const T *staged) {
+            base = tile_base;
+            live = tile_live;
+            stage = staged;
+            if (tailed) {
+#pragma unroll
+                for (int e = 0; e < N; ++e) tail[e] = base + position(e) >= L.tail_start;
             }
         }
 
         // Values of one input for this thread's lanes.
         __device__ __forceinline__ void input(unsigned a, T *v) const {
             if (stage) {
-                constexpr int W = 16 / sizeof(T);
 #pragma unroll
-                for (int j = 0; j < kLanes / W; ++j) load4(stage + a * tile + idx[j * W], v + j * W);
+                for (int j = 0; j < V; ++j) load16(stage + a * tile + position(j * W), v + j * W);
             } else {
                 const T *src = L.inputs[a] + base;
 #pragma unroll
-                for (int e = 0; e < kLanes; ++e) v[e] = idx[e] < live ? src[idx[e]] : src[0];
+                for (int e = 0; e < N; ++e) v[e] = position(e) < live ? src[position(e)] : src[0];
             }
         }
 
@@ -227,21 +246,19 @@ namespace sci_cuda {
             } else if (kind == kLiteral) {
                 const T c = L.constants[slot];
 #pragma unroll
-                for (int e = 0; e < kLanes; ++e) v[e] = c;
+                for (int e = 0; e < N; ++e) v[e] = c;
             } else if (id != kNone) {
-                constexpr int W = 16 / sizeof(T);
 #pragma unroll
-                for (int j = 0; j < kLanes / W; ++j) load4(slots + slot * tile + idx[j * W], v + j * W);
+                for (int j = 0; j < V; ++j) load16(slots + slot * tile + position(j * W), v + j * W);
             } else {
 #pragma unroll
-                for (int e = 0; e < kLanes; ++e) v[e] = T(0);
+                for (int e = 0; e < N; ++e) v[e] = T(0);
             }
         }
 
         __device__ __forceinline__ void store_temp(unsigned slot, const T *v) const {
-            constexpr int W = 16 / sizeof(T);
 #pragma unroll
-            for (int j = 0; j < kLanes / W; ++j) store4(slots + slot * tile + idx[j * W], v + j * W);
+            for (int j = 0; j < V; ++j) store16(slots + slot * tile + position(j * W), v + j * W);
         }
 
         __device__ __forceinline__ void write_output(const T *v) const {
@@ -249,13 +266,12 @@ namespace sci_cuda {
             // 128-bit stores only on the staged path, whose operands the host checked to be 16-byte
             // aligned; the direct path serves unaligned outputs and stores element by element.
             if (stage != nullptr && live == tile) {
-                constexpr int W = 16 / sizeof(T);
 #pragma unroll
-                for (int j = 0; j < kLanes / W; ++j) store4(dst + idx[j * W], v + j * W);
+                for (int j = 0; j < V; ++j) store16(dst + position(j * W), v + j * W);
             } else {
 #pragma unroll
-                for (int e = 0; e < kLanes; ++e)
-                    if (idx[e] < live) dst[idx[e]] = v[e];
+                for (int e = 0; e < N; ++e)
+                    if (position(e) < live) dst[position(e)] = v[e];
             }
         }
     };
@@ -264,24 +280,25 @@ namespace sci_cuda {
     // the reduced value (kReduce) or the two operands of the contracted multiply (kDot).
     template <typename T, class Program, int MODE>
     __device__ __forceinline__ void run_tile(const Work<T, Program> &w, T *value, T *second) {
+        constexpr int N = Lanes<T>::count;
         if constexpr (!Program::baked) {
             const Launch<T> &L = w.L;
-            T last[kLanes];
+            T last[N];
 #pragma unroll
-            for (int e = 0; e < kLanes; ++e) last[e] = T(0);
+            for (int e = 0; e < N; ++e) last[e] = T(0);
             for (unsigned s = 0; s < L.length; ++s) {
                 const Step st = L.steps[s];
-                T a[kLanes], b[kLanes], c[kLanes];
+                T a[N], b[N], c[N];
                 w.fetch(st.a, a);
                 if (st.code >= kAdd) w.fetch(st.b, b);
                 else {
 #pragma unroll
-                    for (int e = 0; e < kLanes; ++e) b[e] = T(0);
+                    for (int e = 0; e < N; ++e) b[e] = T(0);
                 }
                 if (st.code == kFuse) w.fetch(st.c, c);
                 else {
 #pragma unroll
-                    for (int e = 0; e < kLanes; ++e) c[e] = T(0);
+                    for (int e = 0; e < N; ++e) c[e] = T(0);
                 }
                 apply_dynamic<T>(st.code, a, b, c, last, w.tail);
                 if (st.target == kOutput) {
@@ -293,7 +310,7 @@ namespace sci_cuda {
             if constexpr (MODE == kReduce) {
                 if (L.value == kOutput) {
 #pragma unroll
-                    for (int e = 0; e < kLanes; ++e) value[e] = last[e];
+                    for (int e = 0; e < N; ++e) value[e] = last[e];
                 } else {
                     w.fetch(L.value, value);
                 }
@@ -304,8 +321,8 @@ namespace sci_cuda {
         } else {
             using C = typename Program::chunk;
             constexpr int R = C::temporaries > 0 ? C::temporaries : 1;
-            T regs[R][kLanes];
-            T last[kLanes];
+            T regs[R][N];
+            T last[N];
             auto get = [&](auto id_c, T *v) {
                 constexpr int id = decltype(id_c)::value;
                 if constexpr ((id & kTypes) == kInput) {
@@ -313,21 +330,21 @@ namespace sci_cuda {
                 } else if constexpr ((id & kTypes) == kLiteral) {
                     const T c = w.L.constants[id & 63];
 #pragma unroll
-                    for (int e = 0; e < kLanes; ++e) v[e] = c;
+                    for (int e = 0; e < N; ++e) v[e] = c;
                 } else if constexpr (id == kNone) {
 #pragma unroll
-                    for (int e = 0; e < kLanes; ++e) v[e] = T(0);
+                    for (int e = 0; e < N; ++e) v[e] = T(0);
                 } else if constexpr (id == kOutput) {
 #pragma unroll
-                    for (int e = 0; e < kLanes; ++e) v[e] = last[e];
+                    for (int e = 0; e < N; ++e) v[e] = last[e];
                 } else {
 #pragma unroll
-                    for (int e = 0; e < kLanes; ++e) v[e] = regs[id & 63][e];
+                    for (int e = 0; e < N; ++e) v[e] = regs[id & 63][e];
                 }
             };
             static_for<C::length>([&](auto step_c) {
                 constexpr Step st = C::steps[decltype(step_c)::value];
-                T a[kLanes], b[kLanes], c[kLanes];
+                T a[N], b[N], c[N];
                 get(Int<st.a>{}, a);
                 get(Int<st.b>{}, b);
                 get(Int<st.c>{}, c);
@@ -336,7 +353,7 @@ namespace sci_cuda {
                     if constexpr (MODE == kEvaluate) w.write_output(last);
                 } else {
 #pragma unroll
-                    for (int e = 0; e < kLanes; ++e) regs[st.target & 63][e] = last[e];
+                    for (int e = 0; e < N; ++e) regs[st.target & 63][e] = last[e];
                 }
             });
             if constexpr (MODE == kReduce) {
@@ -348,33 +365,65 @@ namespace sci_cuda {
         }
     }
 
-    // Per-thread fold state: a double total plus a NaN flag (minimum and maximum skip NaN and the
-    // flag restores numpy's propagation, as entries.slang:55-78 and accumulator.hpp:28-34 do).
+    // Per-thread fold state: a double total plus a NaN flag. Minimum and maximum skip NaN and the
+    // flag restores numpy's propagation, as entries.slang:55-78 and accumulator.hpp:28-34 do; a sum
+    // lets NaN (and inf - inf) propagate arithmetically.
     struct Fold {
         double total;
-        int poisoned;
+        unsigned magnitude;  // largest |bits| seen by a minimum / maximum: above +inf's bits is NaN
     };
 
     __device__ __forceinline__ double combine(unsigned fold, double a, double b) {
         return fold == 0 ? a + b : (fold == 1 ? fmin(a, b) : fmax(a, b));
     }
 
-    template <typename T, int MODE>
-    __device__ __forceinline__ void accumulate(Fold &f, unsigned fold, const T *value, const T *second, unsigned live,
-                                               const unsigned *idx) {
+    __device__ __forceinline__ unsigned magnitude_bits(float v) { return __float_as_uint(v) & 0x7fffffffu; }
+    __device__ __forceinline__ unsigned magnitude_bits(double v) {
+        // A double is NaN iff its high word without sign exceeds 0x7ff00000, or equals it with a
+        // nonzero low word; folding the low word in as one bit keeps that order.
+        const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(v)) & 0x7fffffffffffffffull;
+        return static_cast<unsigned>(b >> 32) | (static_cast<unsigned>(b) != 0u ? 1u : 0u);
+    }
+    template <typename T> __device__ __forceinline__ unsigned nan_floor() {
+        return sizeof(T) == 4 ? 0x7f800000u : 0x7ff00000u;
+    }
+
+    // Folds one tile of this thread's lanes. A full tile folds its lanes in the element type first
+    // (the reference folds whole 1024-element blocks that way, dispatch.cpp:121-150), then adds the
+    // lane total to the double running total.
+    template <typename T, int MODE, class W>
+    __device__ __forceinline__ void fold_tile(Fold &f, unsigned fold, const T *value, const T *second, const W &w,
+                                              bool full) {
+        constexpr int N = Lanes<T>::count;
+        if (MODE == kDot || fold == 0) {
+            T lanes[N];
 #pragma unroll
-        for (int e = 0; e < kLanes; ++e) {
-            if (idx[e] >= live) continue;
-            if constexpr (MODE == kDot) {
-                f.total = fma(static_cast<double>(value[e]), static_cast<double>(second[e]), f.total);
-            } else {
-                const double v = static_cast<double>(value[e]);
-                if (v != v) {
-                    f.poisoned = 1;
-                } else {
-                    f.total = combine(fold, f.total, v);
+            for (int e = 0; e < N; ++e) {
+                T v;
+                if constexpr (MODE == kDot) v = fma_(value[e], second[e], T(0));
+                else v = value[e];
+                lanes[e] = (full || w.position(e) < w.live) ? v : T(0);
+            }
+            // pairwise within the thread, in the element type
+#pragma unroll
+            for (int width = N / 2; width > 0; width /= 2) {
+#pragma unroll
+                for (int e = 0; e < width; ++e) lanes[e] = add(lanes[e], lanes[e + width]);
+            }
+            f.total += static_cast<double>(lanes[0]);
+        } else {
+            T best = fold == 1 ? from_bits(Limits<T>::infinity) : -from_bits(Limits<T>::infinity);
+            unsigned magnitude = 0;
+#pragma unroll
+            for (int e = 0; e < N; ++e) {
+                if (full || w.position(e) < w.live) {
+                    const T v = value[e];
+                    magnitude = max(magnitude, magnitude_bits(v));
+                    best = fold == 1 ? fmin(best, v) : fmax(best, v);
                 }
             }
+            f.magnitude = max(f.magnitude, magnitude);
+            f.total = combine(fold, f.total, static_cast<double>(best));
         }
     }
 
@@ -389,24 +438,25 @@ namespace sci_cuda {
         extern __shared__ __align__(128) unsigned char shared[];
         __shared__ unsigned long long bars[kMaxStages];
         __shared__ double block_total[32];
-        __shared__ int block_poisoned[32];
+        __shared__ unsigned block_magnitude[32];
         __shared__ bool last_block;
+        constexpr int N = Lanes<T>::count;
 
         const unsigned threads = blockDim.x, t = threadIdx.x;
-        const unsigned tile = kLanes * threads;
+        const unsigned tile = N * threads;
         const unsigned A = arguments_of<Program>(L);
         const unsigned S = L.stages;
         T *ring = reinterpret_cast<T *>(shared);
         T *slots = ring + static_cast<unsigned long long>(S) * A * tile;
         const unsigned long long full = L.count / tile;
         const unsigned long long grid = gridDim.x;
+        const unsigned op = MODE == kDot ? 0u : L.fold;
 
-        Fold fold{L.fold == 0 ? 0.0 : (L.fold == 1 ? __longlong_as_double(0x7ff0000000000000ll)
-                                                    : __longlong_as_double((long long)0xfff0000000000000ull)),
-                  0};
-        if constexpr (MODE == kDot) fold.total = 0.0;
+        Fold fold{op == 0 ? 0.0 : (op == 1 ? __longlong_as_double(0x7ff0000000000000ll)
+                                           : __longlong_as_double((long long)0xfff0000000000000ull)),
+                  0u};
 
-        Work<T, Program> w{L, nullptr, slots, 0, tile, tile, t, threads, {}, {}};
+        Work<T, Program> w(L, slots, threads, t);
 
         // Full tiles through the TMA ring.
         if (S > 0) {
@@ -437,13 +487,10 @@ namespace sci_cuda {
                     failed = true;
                     break;
                 }
-                w.stage = ring + static_cast<unsigned long long>(s) * A * tile;
-                w.base = k * tile;
-                w.live = tile;
-                w.prepare();
-                T value[kLanes], second[kLanes];
+                w.at(k * tile, tile, ring + static_cast<unsigned long long>(s) * A * tile);
+                T value[N], second[N];
                 run_tile<T, Program, MODE>(w, value, second);
-                if constexpr (MODE != kEvaluate) accumulate<T, MODE>(fold, L.fold, value, second, tile, w.idx);
+                if constexpr (MODE != kEvaluate) fold_tile<T, MODE>(fold, op, value, second, w, true);
                 __syncthreads();
                 if (t == 0) {
                     const unsigned long long next = k + S * grid;
@@ -461,53 +508,46 @@ namespace sci_cuda {
             }
         } else {
             // Direct reads: inputs that are not 16-byte aligned, or too wide to stage.
-            w.stage = nullptr;
             for (unsigned long long k = blockIdx.x; k < full; k += grid) {
-                w.base = k * tile;
-                w.live = tile;
-                w.prepare();
-                T value[kLanes], second[kLanes];
+                w.at(k * tile, tile, nullptr);
+                T value[N], second[N];
                 run_tile<T, Program, MODE>(w, value, second);
-                if constexpr (MODE != kEvaluate) accumulate<T, MODE>(fold, L.fold, value, second, tile, w.idx);
+                if constexpr (MODE != kEvaluate) fold_tile<T, MODE>(fold, op, value, second, w, true);
             }
         }
 
         // The ragged last tile, read directly by the block whose turn it is.
         const unsigned long long rest = L.count - full * tile;
         if (rest > 0 && blockIdx.x == full % grid) {
-            w.stage = nullptr;
-            w.base = full * tile;
-            w.live = static_cast<unsigned>(rest);
-            w.prepare();
-            T value[kLanes], second[kLanes];
+            w.at(full * tile, static_cast<unsigned>(rest), nullptr);
+            T value[N], second[N];
             run_tile<T, Program, MODE>(w, value, second);
-            if constexpr (MODE != kEvaluate) accumulate<T, MODE>(fold, L.fold, value, second, w.live, w.idx);
+            if constexpr (MODE != kEvaluate) fold_tile<T, MODE>(fold, op, value, second, w, false);
         }
 
         if constexpr (MODE != kEvaluate) {
-            const unsigned op = MODE == kDot ? 0u : L.fold;
             // warp
 #pragma unroll
             for (int offset = 16; offset > 0; offset >>= 1) {
                 const double other = __shfl_xor_sync(0xffffffffu, fold.total, offset);
                 fold.total = combine(op, fold.total, other);
-                fold.poisoned |= __shfl_xor_sync(0xffffffffu, fold.poisoned, offset);
+                fold.magnitude = max(fold.magnitude, __shfl_xor_sync(0xffffffffu, fold.magnitude, offset));
             }
             const unsigned warp = t / 32, warps = (threads + 31) / 32;
             if ((t & 31) == 0) {
                 block_total[warp] = fold.total;
-                block_poisoned[warp] = fold.poisoned;
+                block_magnitude[warp] = fold.magnitude;
             }
             __syncthreads();
             if (t == 0) {
                 double total = block_total[0];
-                int poisoned = block_poisoned[0];
+                unsigned magnitude = block_magnitude[0];
                 for (unsigned i = 1; i < warps; ++i) {
                     total = combine(op, total, block_total[i]);
-                    poisoned |= block_poisoned[i];
+                    magnitude = max(magnitude, block_magnitude[i]);
                 }
                 L.state->partial[blockIdx.x] = total;
-                L.state->poisoned[blockIdx.x] = poisoned;
+                L.state->poisoned[blockIdx.x] = magnitude > nan_floor<T>() ? 1 : 0;
                 __threadfence();
                 const unsigned ticket = atomicAdd(&L.state->ticket, 1u);
                 last_block = ticket == gridDim.x - 1;

@@ -126,6 +126,10 @@ namespace sci_cuda {
         L.arguments = chunk.arguments;
         L.temporaries = chunk.temporaries;
         L.fold = fold;
+        for (int i = 0; i < chunk.length; ++i) {
+            const int code = chunk.instructions[i].code;
+            if (code == SCI_CODE_MINIMUM || code == SCI_CODE_MAXIMUM) L.tailed = 1;
+        }
         for (int i = 0; i < chunk.literals; ++i) L.constants[i] = static_cast<T>(chunk.constants[i]);
         for (int i = 0; i < chunk.arguments; ++i) {
             if (!chunk.inputs[i] || !reachable(ctx, chunk.inputs[i]))
@@ -173,7 +177,7 @@ namespace sci_cuda {
         unsigned stages = 0;
         size_t smem = 0;
         for (; threads >= 32; threads /= 2) {
-            const size_t tile_bytes = size_t(kLanes) * threads * sizeof(T);
+            const size_t tile_bytes = size_t(Lanes<T>::count) * threads * sizeof(T);
             const size_t temps = special ? 0 : size_t(L.temporaries) * tile_bytes;
             if (temps > budget) continue;
             stages = 0;
@@ -189,7 +193,7 @@ namespace sci_cuda {
         if (threads < 32) return ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "chunk too wide for shared memory");
         L.stages = stages;
 
-        const uint64_t tile = uint64_t(kLanes) * threads;
+        const uint64_t tile = uint64_t(Lanes<T>::count) * threads;
         const uint64_t tiles = (L.count + tile - 1) / tile;
         void *args[] = {&L};
         if (special) {

@@ -126,6 +126,10 @@ namespace sci_cuda {
             L.arguments = chunk.arguments;
             L.temporaries = chunk.temporaries;
             L.fold = fold;
+            for (int i = 0; i < chunk.length; ++i) {
+                const int code = chunk.instructions[i].code;
+                if (code == SCI_CODE_MINIMUM || code == SCI_CODE_MAXIMUM) L.tailed = 1;
+            }
             bool aligned = true;
             for (int i = 0; i < chunk.literals; ++i) L.constants[i] = static_cast<T>(chunk.constants[i]);
             for (int i = 0; i < chunk.arguments; ++i) {
@@ -147,7 +151,7 @@ namespace sci_cuda {
             unsigned stages = 0;
             unsigned long long smem = 0;
             for (; threads >= 32; threads /= 2) {
-                const unsigned long long tile_bytes = 1ull * kLanes * threads * sizeof(T);
+                const unsigned long long tile_bytes = 1ull * Lanes<T>::count * threads * sizeof(T);
                 const unsigned long long temps = 1ull * L.temporaries * tile_bytes;
                 if (temps > budget) continue;
                 stages = 0;
@@ -168,7 +172,7 @@ namespace sci_cuda {
             int per_sm = 1;
             if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
                 per_sm = 1;
-            const unsigned long long tile = 1ull * kLanes * threads;
+            const unsigned long long tile = 1ull * Lanes<T>::count * threads;
             unsigned long long grid = (count + tile - 1) / tile;
             const unsigned long long wide = 1ull * per_sm * setup.sms;
             if (grid > wide) grid = wide;

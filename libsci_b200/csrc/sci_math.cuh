@@ -230,8 +230,53 @@ namespace sci_cuda {
         else if constexpr (code == kAcosh) return acosh(x);
         else return atanh(x);
     }
+    // tanh of a float, in double and rounded once. With 2|x| = k ln 2 + r, |r| <= ln 2 / 2:
+    //   e^{2|x|} - 1 = 2^k (1 + q) - 1 and e^{2|x|} + 1 = 2^k (1 + q) + 1, q = e^r - 1,
+    // q from its Taylor series through r^12/12! (truncation below 2^-51 relative), and the quotient
+    // of the two by Newton-Raphson refinement of an approximate reciprocal, then one correction of
+    // the quotient with its residual. Relative error about 2^-50, so the float rounding is the
+    // correctly rounded one except when the true value lies within ~2^-50 of a rounding midpoint.
+    // k = 0 keeps q itself as the numerator, so small |x| loses nothing to cancellation.
+    // |x| < 2^-12 rounds to x (tanh x = x (1 - x^2/3 + ...), and x^2/3 < 2^-25.5); |x| > 9.03
+    // rounds to 1 (1 - tanh x < 2 e^{-18.06} < 2^-25).
+    __device__ __forceinline__ float tanh_float(float x) {
+        const float a = fabsf(x);
+        if (!(a >= 0x1p-12f)) return a < 0x1p-12f ? x : __fadd_rn(x, x);  // tiny, or NaN
+        if (a > 9.03125f) return copysignf(1.0f, x);
+        const double d = 2.0 * static_cast<double>(a);
+        const double k = __dadd_rn(__dadd_rn(__dmul_rn(d, 0x1.71547652b82fep+0), 0x1.8p52), -0x1.8p52);
+        double r = __fma_rn(-k, 0x1.62e42fefa3800p-1, d);
+        r = __fma_rn(-k, 0x1.ef35793c76730p-45, r);
+        // 1/2!, 1/3!, ..., 1/12!
+        double p = 1.0 / 479001600.0;
+        p = __fma_rn(p, r, 1.0 / 39916800.0);
+        p = __fma_rn(p, r, 1.0 / 3628800.0);
+        p = __fma_rn(p, r, 1.0 / 362880.0);
+        p = __fma_rn(p, r, 1.0 / 40320.0);
+        p = __fma_rn(p, r, 1.0 / 5040.0);
+        p = __fma_rn(p, r, 1.0 / 720.0);
+        p = __fma_rn(p, r, 1.0 / 120.0);
+        p = __fma_rn(p, r, 1.0 / 24.0);
+        p = __fma_rn(p, r, 1.0 / 6.0);
+        p = __fma_rn(p, r, 0.5);
+        const double q = __fma_rn(__dmul_rn(r, r), p, r);
+        const double s = __longlong_as_double(static_cast<long long>(static_cast<int>(k) + 1023) << 52);
+        const double num = __fma_rn(s, q, __dsub_rn(s, 1.0));
+        const double den = __fma_rn(s, q, __dadd_rn(s, 1.0));
+        double y;
+        asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(den));
+        double e = __fma_rn(-den, y, 1.0);
+        y = __fma_rn(y, e, y);
+        e = __fma_rn(-den, y, 1.0);
+        y = __fma_rn(y, e, y);
+        double t = __dmul_rn(num, y);
+        t = __fma_rn(__fma_rn(-den, t, num), y, t);
+        return copysignf(static_cast<float>(t), x);
+    }
+
     template <int code, typename T> __device__ __forceinline__ T library(T x) {
-        return static_cast<T>(library_d<code>(static_cast<double>(x)));
+        if constexpr (code == kTanh && sizeof(T) == 4) return tanh_float(x);
+        else return static_cast<T>(library_d<code>(static_cast<double>(x)));
     }
 
     // ---- one code on one element (operation.hpp:25-110) ------------------------------------------
