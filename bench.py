@@ -174,8 +174,76 @@ def run_reference_arm(args, rank: int) -> int:
     return 0
 
 
+def run_product(args) -> int:
+    """linear::product at M = N = K (default 8192), float32 inputs ~ U[-1,1): every mode timed on the
+    device (conversion to bf16 included), error against FP64 rows, reference CPU multiply sampled."""
+    import torch
+
+    from libsci_b200.device import Device
+    from tests import _oracle
+
+    size = args.size
+    device = Device(0)
+    stream = torch.cuda.ExternalStream(device.stream)
+    rng = np.random.default_rng(0)
+    a = rng.uniform(-1, 1, (size, size)).astype(np.float32)
+    b = rng.uniform(-1, 1, (size, size)).astype(np.float32)
+    da, db, dc = device.array(a.ravel()), device.array(b.ravel()), device.empty(size * size)
+    flops = 2.0 * size ** 3
+    peak = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["bf16_tflops"] if (ROOT / "MEASURED_PEAKS.json").exists() else 1590.0
+    oracle = _oracle.port()
+    sample_rows = np.sort(rng.choice(size, 64, replace=False))
+    want = np.zeros((len(sample_rows), size))
+    for i, r in enumerate(sample_rows):
+        oracle.sci_oracle_product_rows(a.ctypes.data, b.ctypes.data, want[i].ctypes.data, size, size, size, int(r), int(r) + 1)
+    modes = {}
+    for mode, name in ((0, "bf16"), (1, "split_bf16"), (2, "fp32")):
+        for _ in range(args.warmup):
+            device.product(da, db, size, size, size, mode=mode, out=dc)
+        device.synchronize()
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        steps = args.steps if mode != 2 else max(1, args.steps // 4)
+        start.record(stream)
+        for _ in range(steps):
+            device.product(da, db, size, size, size, mode=mode, out=dc)
+        stop.record(stream)
+        stop.synchronize()
+        ms = start.elapsed_time(stop) / steps
+        got = dc.numpy().reshape(size, size)[sample_rows]
+        err = np.abs(got - want)
+        modes[name] = {"ms": ms, "TFLOP/s": flops / (ms * 1e-3) / 1e12, "frac_of_bf16_peak": flops / (ms * 1e-3) / 1e12 / peak,
+                       "tensor_TFLOP/s": (3 if mode == 1 else 1) * flops / (ms * 1e-3) / 1e12 if mode != 2 else None,
+                       "max_abs_err": float(err.max()), "rel_fro_err": float(np.linalg.norm(err) / np.linalg.norm(want))}
+    cpu = None
+    ref = _oracle.reference()
+    if ref is not None and not args.no_cpu:
+        n = 2048
+        x = rng.uniform(-1, 1, (n, n)).astype(np.float32)
+        y = rng.uniform(-1, 1, (n, n)).astype(np.float32)
+        z = np.empty((n, n), np.float32)
+        t0 = time.perf_counter()
+        ref.sci_ref_product(0, x.ctypes.data, y.ctypes.data, z.ctypes.data, n, n, n)
+        seconds = time.perf_counter() - t0
+        cpu = {"value": 2.0 * n ** 3 / seconds / 1e12, "unit": "TFLOP/s", "cores": int(ref.sci_ref_threads()),
+               "kind": "reference", "sample": "libsci multiply (dispatch.cpp:171-224) at 2048^3, fp32, timed once"}
+    best = modes["bf16"]
+    line = {"metric": "product TFLOP/s", "value": best["TFLOP/s"], "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": best["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16 (fp32 accumulate)", "data": "synthetic",
+            "config": {"workload": f"product M=N=K={size}, float32 ~ U[-1,1)", "modes": list(modes)},
+            "modes": modes,
+            "roofline": {"bound": "tensor", "achieved": best["TFLOP/s"], "peak": peak, "unit": "TFLOP/s",
+                         "frac": best["TFLOP/s"] / peak, "traffic": None, "peak_source": "measured bf16_tflops (burst)"},
+            "cpu_baseline": cpu, "gpu_launches": 3 * args.steps}
+    print(json.dumps(line))
+    device.close()
+    return 0
+
+
 def main() -> int:
     parser = argparse.ArgumentParser()
+    parser.add_argument("--workload", default="chunks", choices=["chunks", "product"])
+    parser.add_argument("--size", type=int, default=8192)
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=20)
     parser.add_argument("--warmup", type=int, default=3)
@@ -191,6 +259,8 @@ def main() -> int:
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference_arm(args, rank)
+    if args.workload == "product":
+        return run_product(args)
 
     import torch
 

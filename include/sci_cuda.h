@@ -131,6 +131,20 @@ int sci_cuda_reduce(sci_cuda_context *context, const sci_chunk *chunk, uint32_t 
 /* The same reduction, queued: the double result is written to device memory `device_result`. */
 int sci_cuda_reduce_async(sci_cuda_context *context, const sci_chunk *chunk, uint32_t fold, uint64_t count,
                           double *device_result);
+/* ---- matrix product ------------------------------------------------------------------------ */
+enum {
+    SCI_PRODUCT_BF16 = 0,       /* bf16 operands on tcgen05 tensor cores, FP32 accumulation           */
+    SCI_PRODUCT_SPLIT_BF16 = 1, /* hi+lo bf16 split, three tensor-core products, ~16-bit operands      */
+    SCI_PRODUCT_FP32 = 2        /* plain FP32 SIMT: the comparison form (double always runs plain FP64) */
+};
+/* Device::product(precision, left, right, output, rows, columns, depth) (device.hpp:79-80,
+ * device.cpp:318-352; linear::product, include/linear/product.hpp:22-65): row-major
+ * output (rows x columns) = left (rows x depth) * right (depth x columns), queued. `mode` chooses
+ * how single-precision products run; depth 0 writes zeros (dispatch.cpp:270-273). The bf16 modes
+ * use a workspace of the context that grows to 2 bytes x (rows + columns) x depth (x2 split). */
+int sci_cuda_product(sci_cuda_context *context, uint32_t precision, uint32_t mode, const void *left, const void *right,
+                     void *output, uint64_t rows, uint64_t columns, uint64_t depth);
+
 /* No counterpart in the reference. The same reduction for callers that may not allocate device
  * memory (a host framework that owns the GPU heap through its own pool, a plugin inside one, a
  * latency-critical thread where an allocation would synchronize the device). It needs no context:

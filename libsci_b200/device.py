@@ -92,6 +92,20 @@ class Device:
     def reduce_async(self, chunk: C.Chunk, fold: int, count: int, device_result: int) -> None:
         check(lib.sci_cuda_reduce_async(self.handle, ctypes.byref(chunk), fold, count, device_result), self.handle)
 
+    def product(self, left: "DeviceArray", right: "DeviceArray", rows: int, columns: int, depth: int,
+                mode: int = 0, out: "DeviceArray | None" = None) -> "DeviceArray":
+        """linear::product (include/linear/product.hpp:22-65): row-major out = left @ right.
+
+        mode: 0 bf16 tensor cores, 1 split-bf16 (three tensor-core products), 2 plain FP32 SIMT;
+        double operands always multiply in plain FP64."""
+        dtype = left.dtype
+        if out is None:
+            out = self.empty(rows * columns, dtype)
+        precision = C.WIDE if dtype == np.float64 else C.SINGLE
+        check(lib.sci_cuda_product(self.handle, precision, mode, left.pointer, right.pointer, out.pointer, rows, columns,
+                                   depth), self.handle)
+        return out
+
     def evaluate(self, expression, out: "DeviceArray | None" = None) -> "DeviceArray":
         """assign(target, expression) (expression.hpp:158-185); allocates the target if needed."""
         expr = C._operand(expression, None)

@@ -49,11 +49,10 @@ def _load() -> ctypes.CDLL:
         "sci_cuda_reduce": (ctypes.c_int, [c_ctx, P(ChunkStruct), ctypes.c_uint32, ctypes.c_uint64, P(ctypes.c_double)]),
         "sci_cuda_reduce_async": (ctypes.c_int, [c_ctx, P(ChunkStruct), ctypes.c_uint32, ctypes.c_uint64, ctypes.c_void_p]),
         "sci_cuda_jit_wait": (ctypes.c_int, [c_ctx]),
-    }
-    optional = {
         "sci_cuda_product": (ctypes.c_int, [c_ctx, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
     }
+    optional = {}
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
         fn.restype, fn.argtypes = res, args
