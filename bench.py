@@ -240,9 +240,71 @@ def run_product(args) -> int:
     return 0
 
 
+def run_solve(args) -> int:
+    """linear::solve at n = 8192 with 16 right-hand sides ~ N(0,1), for A = G + n I and A = G
+    (G ~ N(0,1)): FP32 LU + FP64 refinement against plain FP64 LU on the same GPU, both to a
+    normwise backward error <= 1e-14; libsci's CPU solve<double> timed once on a 2048 sample."""
+    import torch
+
+    from libsci_b200.device import Device
+    from tests import _oracle
+
+    n, width = args.size, 16
+    device = Device(0)
+    stream = torch.cuda.ExternalStream(device.stream)
+    flops = 2.0 / 3.0 * n ** 3 + 2.0 * n * n * width
+    cases = {}
+    for name, shift in (("G+nI", True), ("G", False)):
+        rng = np.random.default_rng(17 + int(shift))
+        a = rng.standard_normal((n, n)) + (n * np.eye(n) if shift else 0.0)
+        b = rng.standard_normal((n, width))
+        da, db, dx = device.array(a.ravel()), device.array(b.ravel()), device.empty(n * width, np.float64)
+        result = {}
+        for label, refine in (("fp32_lu_fp64_refine", True), ("fp64_lu", False)):
+            device.solve(da, db, n, width, refine=refine, out=dx)  # warm-up (workspaces, module loads)
+            times, berr, iterations = [], None, None
+            for _ in range(args.steps):
+                start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                start.record(stream)
+                _, berr, iterations = device.solve(da, db, n, width, refine=refine, out=dx)
+                stop.record(stream)
+                stop.synchronize()
+                times.append(start.elapsed_time(stop))
+            ms = statistics.median(times)
+            result[label] = {"ms": ms, "GFLOP/s": flops / (ms * 1e-3) / 1e9, "backward_error": berr,
+                             "iterations": iterations}
+        result["speedup_refined_vs_fp64"] = result["fp64_lu"]["ms"] / result["fp32_lu_fp64_refine"]["ms"]
+        cases[name] = result
+        for arr in (da, db, dx):
+            arr.free()
+    cpu = None
+    ref = _oracle.reference()
+    if ref is not None and not args.no_cpu:
+        m = 2048
+        rng = np.random.default_rng(5)
+        a = rng.standard_normal((m, m)) + m * np.eye(m)
+        b = rng.standard_normal((m, width))
+        x = np.empty((m, width))
+        t0 = time.perf_counter()
+        ref.sci_ref_solve_f64(a.ctypes.data, b.ctypes.data, x.ctypes.data, m, width)
+        seconds = time.perf_counter() - t0
+        cpu = {"value": (2.0 / 3.0 * m ** 3 + 2.0 * m * m * width) / seconds / 1e9, "unit": "GFLOP/s",
+               "cores": int(ref.sci_ref_threads()), "kind": "reference",
+               "sample": "libsci solve<double> (factor + substitute) at n=2048, 16 RHS, timed once"}
+    headline = cases["G+nI"]["fp32_lu_fp64_refine"]
+    line = {"metric": "solve speedup vs plain FP64 LU at equal backward error", "value": cases["G+nI"]["speedup_refined_vs_fp64"],
+            "unit": "x", "n_gpus": 1, "steps": args.steps, "warmup": 1, "ms_per_step": headline["ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 LU + f64 refinement",
+            "data": "synthetic", "config": {"workload": f"solve n={n}, 16 RHS ~ N(0,1); A=G+nI and A=G"},
+            "cases": cases, "cpu_baseline": cpu}
+    print(json.dumps(line))
+    device.close()
+    return 0
+
+
 def main() -> int:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--workload", default="chunks", choices=["chunks", "product"])
+    parser.add_argument("--workload", default="chunks", choices=["chunks", "product", "solve"])
     parser.add_argument("--size", type=int, default=8192)
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=20)
@@ -261,6 +323,8 @@ def main() -> int:
         return run_reference_arm(args, rank)
     if args.workload == "product":
         return run_product(args)
+    if args.workload == "solve":
+        return run_solve(args)
 
     import torch
 

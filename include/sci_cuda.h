@@ -135,15 +135,43 @@ int sci_cuda_reduce_async(sci_cuda_context *context, const sci_chunk *chunk, uin
 enum {
     SCI_PRODUCT_BF16 = 0,       /* bf16 operands on tcgen05 tensor cores, FP32 accumulation           */
     SCI_PRODUCT_SPLIT_BF16 = 1, /* hi+lo bf16 split, three tensor-core products, ~16-bit operands      */
-    SCI_PRODUCT_FP32 = 2        /* plain FP32 SIMT: the comparison form (double always runs plain FP64) */
+    SCI_PRODUCT_FP32 = 2,       /* plain FP32 SIMT: the comparison form (double always runs plain FP64) */
+    SCI_PRODUCT_SPLIT3_BF16 = 3 /* hi+mid+lo bf16 split, six tensor-core products, ~FP32-accurate      */
 };
 /* Device::product(precision, left, right, output, rows, columns, depth) (device.hpp:79-80,
  * device.cpp:318-352; linear::product, include/linear/product.hpp:22-65): row-major
  * output (rows x columns) = left (rows x depth) * right (depth x columns), queued. `mode` chooses
  * how single-precision products run; depth 0 writes zeros (dispatch.cpp:270-273). The bf16 modes
- * use a workspace of the context that grows to 2 bytes x (rows + columns) x depth (x2 split). */
+ * use a workspace of the context that grows to 2 bytes x (rows + columns) x depth x terms. */
 int sci_cuda_product(sci_cuda_context *context, uint32_t precision, uint32_t mode, const void *left, const void *right,
                      void *output, uint64_t rows, uint64_t columns, uint64_t depth);
+
+/* ---- LU and solve -------------------------------------------------------------------------- */
+enum {
+    SCI_FACTOR_TENSOR = 0, /* float: trailing updates on the tensor cores (split-bf16, FP32 accumulation) */
+    SCI_FACTOR_PLAIN = 1   /* float: trailing updates in plain FP32 SIMT (double always plain FP64)     */
+};
+enum { SCI_REFINE_NONE = 0, SCI_REFINE_FP64 = 1 };
+
+typedef struct sci_solve_report {
+    double backward_error; /* max over columns of |b - A x|_inf / (|A|_inf |x|_inf + |b|_inf), in FP64 */
+    int iterations;        /* refinement iterations (0 without refinement) */
+} sci_solve_report;
+
+/* linear::factor (include/linear/decompose.hpp:29-72): in-place LU with partial pivoting of the
+ * order x order row-major device matrix; on return the strict lower triangle holds L (unit
+ * diagonal implied), the rest U, and host array rows[i] is the original row now at position i.
+ * The pivot is the first row with the strictly largest |a|; a zero pivot is skipped. Waits.
+ * order <= 8192. */
+int sci_cuda_factor(sci_cuda_context *context, uint32_t precision, uint32_t mode, void *matrix, uint64_t *rows,
+                    uint64_t order);
+/* linear::solve (include/linear/solve.hpp:60-76): solution (order x width) with matrix * solution =
+ * right, all device memory, row-major. refine = SCI_REFINE_NONE factors and substitutes in the
+ * element type (the reference's behaviour); SCI_REFINE_FP64 (double operands) factors in FP32
+ * and iterates r = b - A x in FP64 until the normwise backward error is <= 1e-15 or stalls.
+ * `report` (may be null) receives the backward error and iteration count. Waits. order <= 8192. */
+int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uint32_t refine, const void *matrix, const void *right,
+                   void *solution, uint64_t order, uint64_t width, sci_solve_report *report);
 
 /* No counterpart in the reference. The same reduction for callers that may not allocate device
  * memory (a host framework that owns the GPU heap through its own pool, a plugin inside one, a

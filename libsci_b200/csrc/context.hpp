@@ -85,7 +85,8 @@ namespace sci_cuda {
         std::vector<Retired> retired;  // frees deferred until queued work is done
         std::map<std::tuple<const void *, int, size_t>, int> occupancy;  // (kernel, threads, smem) -> blocks/SM
         std::unique_ptr<Specializer> specializer;
-        std::unique_ptr<Workspace> workspace;
+        std::unique_ptr<Workspace> workspace;  // product / trailing-update operands
+        std::unique_ptr<Workspace> solver;     // LU copies, pivots, residuals
         int jit_mode{1};  // 0 off, 1 background, 2 synchronous (SCI_CUDA_JIT)
         bool jit_trace{false};
 
@@ -128,6 +129,17 @@ namespace sci_cuda {
     inline const void *generic_chunk_kernel(bool wide, int mode) {
         return wide ? generic_chunk_kernel_f64(mode) : generic_chunk_kernel_f32(mode);
     }
+
+    // Row-major GEMMs on submatrices (product.cu): C (pitch ldc) = A (pitch lda) * B (pitch ldb),
+    // or C -= A * B with `subtract`. tensor_gemm splits each operand into `terms` (1-3) bf16 parts
+    // and multiplies on the tensor cores; simt_gemm is the plain FP32 / FP64 form. Both queue on
+    // ctx.stream.
+    int tensor_gemm(Context &ctx, int terms, const float *a, unsigned long long lda, const float *b,
+                    unsigned long long ldb, float *c, unsigned long long ldc, unsigned long long m, unsigned long long n,
+                    unsigned long long k, bool subtract);
+    template <typename T>
+    int simt_gemm(Context &ctx, const T *a, unsigned long long lda, const T *b, unsigned long long ldb, T *c,
+                  unsigned long long ldc, unsigned long long m, unsigned long long n, unsigned long long k, bool subtract);
 
     // Validates a chunk before anything is launched: counts, codes, and every value id in range.
     int validate(Context &ctx, const sci_chunk *chunk, bool reducing);

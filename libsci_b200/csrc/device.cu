@@ -278,6 +278,7 @@ int sci_cuda_open(uint32_t ordinal, sci_cuda_context **context) {
     }
     ctx->specializer = make_specializer(*ctx);
     ctx->workspace = std::make_unique<Workspace>();
+    ctx->solver = std::make_unique<Workspace>();
     *context = ctx.release();
     return SCI_CUDA_OK;
 }
@@ -290,6 +291,7 @@ int sci_cuda_close(sci_cuda_context *context) {
         cudaStreamSynchronize(context->stream);
         context->specializer.reset();
         if (context->workspace) context->workspace->release();
+        if (context->solver) context->solver->release();
         for (auto &r : context->retired) {
             cudaEventDestroy(r.done);
             cudaFree(r.memory);

@@ -1,0 +1,890 @@
+// lu.cu -- linear::factor / linear::solve on sm_100a, with FP64 iterative refinement.
+//
+// The reference factors in place, unblocked and right-looking, one row swap and one rank-1 update
+// per column, on the host (include/linear/decompose.hpp:29-72), then substitutes forward through
+// the unit lower triangle and back through the upper one (include/linear/solve.hpp:25-52). Pivoting
+// is partial: the first row with the strictly largest |a| (decompose.hpp:35-38); a zero pivot is
+// skipped (decompose.hpp:44-45). This file keeps those rules and blocks the work for the GPU:
+//
+//  for each outer block of 256 columns:
+//    for each narrow panel of W columns (W = 32 float, 16 double) inside it:
+//      1. panel_factor: one 8-CTA thread-block cluster, 1024 threads per CTA, one panel row per
+//         thread held in registers (so up to 8192 rows). Per column: a warp-shuffle argmax, a block
+//         argmax in shared memory, then one cluster barrier after which the 8 CTA candidates, the
+//         winner's row and the displaced row are read through distributed shared memory; then every
+//         thread eliminates its own row.
+//      2. move_rows: the panel's net row movement applied to every other column (one gather).
+//      3. trsm_rows + rank_update: U rows of the panel and the rows below it, inside the block.
+//    after the block: its U rows for the columns beyond it (trsm_rows + rank_update per panel, once
+//    the block's pivots are final), then the trailing update of everything right of and below it
+//    (GEMM, K = 256): on the tensor cores for float (three-term bf16 split, six products, about
+//    FP32 accuracy, FP32 accumulation), or plain FP32 / FP64 SIMT.
+//
+// solve with refinement (SCI_REFINE_FP64): the matrix is factored in FP32, then
+//    x = 0, r = b;  repeat: solve LU d = P r in FP32; x += d;  r = b - A x in FP64
+// until the normwise backward error |r|_inf / (|A|_inf |x|_inf + |b|_inf) of every column is at
+// most 1e-15 or stops improving. Only the residual and the update run in FP64.
+#include "context.hpp"
+#include "workspace.hpp"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace sci_cuda {
+
+    namespace {
+
+        constexpr int kClusterCtas = 8;
+        constexpr int kPanelThreads = 1024;
+        constexpr unsigned long long kPanelRows = 1ull * kClusterCtas * kPanelThreads;
+        constexpr unsigned long long kOuter = 256;
+        constexpr int kSolveBlock = 128;
+
+        template <typename T> struct PanelWidth {
+            static constexpr int value = sizeof(T) == 4 ? 32 : 16;
+        };
+
+        // ---- cluster primitives ------------------------------------------------------------------
+        __device__ __forceinline__ unsigned cluster_rank() {
+            unsigned r;
+            asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+            return r;
+        }
+        __device__ __forceinline__ void cluster_sync() {
+            asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+        }
+        __device__ __forceinline__ unsigned remote(const void *local, unsigned rank) {
+            const unsigned address = static_cast<unsigned>(__cvta_generic_to_shared(local));
+            unsigned mapped;
+            asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(mapped) : "r"(address), "r"(rank));
+            return mapped;
+        }
+        __device__ __forceinline__ float load_remote(unsigned address, float) {
+            float v;
+            asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(address) : "memory");
+            return v;
+        }
+        __device__ __forceinline__ double load_remote(unsigned address, double) {
+            double v;
+            asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(address) : "memory");
+            return v;
+        }
+        __device__ __forceinline__ unsigned long long load_remote_u64(unsigned address) {
+            unsigned long long v;
+            asm volatile("ld.shared::cluster.u64 %0, [%1];" : "=l"(v) : "r"(address) : "memory");
+            return v;
+        }
+
+        // (magnitude, row) pairs: larger magnitude wins, equal magnitudes go to the lower row -- the
+        // row the reference's "first strictly larger" scan keeps.
+        template <typename T> __device__ __forceinline__ bool better(T m1, unsigned long long r1, T m2, unsigned long long r2) {
+            return m1 > m2 || (m1 == m2 && r1 < r2);
+        }
+        template <typename T> __device__ __forceinline__ void warp_argmax(T &m, unsigned long long &r) {
+#pragma unroll
+            for (int offset = 16; offset > 0; offset >>= 1) {
+                const T om = __shfl_xor_sync(0xffffffffu, m, offset);
+                const unsigned long long orow = __shfl_xor_sync(0xffffffffu, r, offset);
+                if (better(om, orow, m, r)) {
+                    m = om;
+                    r = orow;
+                }
+            }
+        }
+
+        // The panel's net row movement: after its exchanges, row rows[i] holds what row src[i] held.
+        // Only rows the panel touched appear (at most twice its width).
+        struct Movement {
+            long long count;
+            long long rows[64];
+            long long src[64];
+        };
+
+        // Factors columns [j0, j0 + width) of rows [j0, n) in place; piv[j0 + j] = the row swapped into
+        // position j0 + j, and *moved = the net movement of the panel's exchanges. One cluster of 8
+        // CTAs; thread t of CTA c owns row j0 + 1024 c + t, its panel values in registers.
+        //
+        // Per column, one cluster barrier: before it, each CTA publishes its best candidate (|value|,
+        // row, and the candidate row's values), and CTA 0 publishes the row at the pivot position;
+        // after it, every CTA reads the 8 candidates, the winner's row and (the pivot row's owner) the
+        // displaced row through distributed shared memory. Publication buffers alternate by column
+        // parity, so a buffer is rewritten only after a later barrier every reader has passed.
+        template <typename T>
+        __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kPanelThreads, 1)
+                panel_factor(T *a, unsigned long long n, unsigned long long j0, int width, long long *piv, Movement *moved) {
+            constexpr int W = PanelWidth<T>::value;
+            __shared__ T warp_mag[32];
+            __shared__ unsigned long long warp_row[32];
+            __shared__ T cand_mag[2];
+            __shared__ unsigned long long cand_row[2];
+            __shared__ T cand_values[2][W];  // the CTA winner's row
+            __shared__ T jbuf[2][W];         // CTA 0: the row at the pivot position
+            __shared__ T pivot_row[W];
+            __shared__ unsigned long long winner;
+
+            const unsigned c = cluster_rank(), t = threadIdx.x, lane = t % 32, warp = t / 32;
+            const unsigned long long r = j0 + 1ull * c * kPanelThreads + t;
+            const bool valid = r < n;
+            T v[W];
+#pragma unroll
+            for (int k = 0; k < W; ++k) v[k] = (valid && k < width) ? a[r * n + j0 + k] : T(0);
+
+#pragma unroll
+            for (int j = 0; j < W; ++j) {
+                if (j < width) {
+                    const int par = j & 1;
+                    const unsigned long long row_j = j0 + j;
+                    // 1. this row's candidacy; a NaN only stands at the pivot position itself, where the
+                    //    reference's comparisons against it all fail (decompose.hpp:35-38).
+                    T mag = T(-1);
+                    if (valid && r >= row_j) {
+                        const T m = fabs(v[j]);
+                        mag = (m == m) ? m : (r == row_j ? T(INFINITY) : T(-1));
+                    }
+                    unsigned long long mrow = r;
+                    warp_argmax(mag, mrow);
+                    if (lane == 0) {
+                        warp_mag[warp] = mag;
+                        warp_row[warp] = mrow;
+                    }
+                    if (c == 0 && t == static_cast<unsigned>(j)) {
+#pragma unroll
+                        for (int k = 0; k < W; ++k) jbuf[par][k] = v[k];
+                    }
+                    __syncthreads();
+                    if (warp == 0) {
+                        T m2 = warp_mag[lane];
+                        unsigned long long r2 = warp_row[lane];
+                        warp_argmax(m2, r2);
+                        if (lane == 0) {
+                            cand_mag[par] = m2;
+                            cand_row[par] = r2;
+                            winner = r2;
+                        }
+                    }
+                    __syncthreads();
+                    if (r == winner) {
+#pragma unroll
+                        for (int k = 0; k < W; ++k) cand_values[par][k] = v[k];
+                    }
+                    cluster_sync();  // the candidates and the pivot-position row are published
+                    // 2. the cluster's pivot, computed identically by every warp
+                    T pm = T(-1);
+                    unsigned long long prow = ~0ull;
+                    if (lane < kClusterCtas) {
+                        pm = load_remote(remote(&cand_mag[par], lane), T(0));
+                        prow = load_remote_u64(remote(&cand_row[par], lane));
+                    }
+                    warp_argmax(pm, prow);
+                    if (pm < T(0)) prow = row_j;  // no candidate (cannot happen for a valid pivot row)
+                    const unsigned prank = static_cast<unsigned>((prow - j0) / kPanelThreads);
+                    if (warp == 0 && lane < W) pivot_row[lane] = load_remote(remote(&cand_values[par][lane], prank), T(0));
+                    if (r == prow && prow != row_j) {
+                        // this row moves to the pivot's old place: it takes the displaced row's values
+#pragma unroll
+                        for (int k = 0; k < W; ++k) v[k] = load_remote(remote(&jbuf[par][k], 0), T(0));
+                    }
+                    __syncthreads();
+                    if (r == row_j) {
+#pragma unroll
+                        for (int k = 0; k < W; ++k) v[k] = pivot_row[k];
+                    }
+                    if (c == 0 && t == 0) piv[row_j] = static_cast<long long>(prow);
+                    // 3. eliminate below the pivot: l = a / pivot; a[k] -= l * pivot_row[k]
+                    const T diagonal = pivot_row[j];
+                    if (diagonal != T(0) && valid && r > row_j) {
+                        const T l = div(v[j], diagonal);
+                        v[j] = l;
+#pragma unroll
+                        for (int k = j + 1; k < W; ++k) v[k] = sub(v[k], mul(l, pivot_row[k]));
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < W; ++k)
+                if (valid && k < width) a[r * n + j0 + k] = v[k];
+            if (c == 0 && warp == 0) {
+                // The net movement of rows: the exchanges applied in order to a table of the rows they
+                // touch (at most 2W), one warp, each lane holding two table entries.
+                __syncwarp();
+                long long row_a = lane < static_cast<unsigned>(width) ? static_cast<long long>(j0 + lane) : -1;
+                long long row_b = -1;
+                long long src_a = row_a, src_b = -1;
+                int count = width;
+                for (int j = 0; j < width; ++j) {
+                    const long long p = piv[j0 + j];
+                    // where p sits in the table: entry index, or -1
+                    const unsigned in_a = __ballot_sync(0xffffffffu, row_a == p);
+                    const unsigned in_b = __ballot_sync(0xffffffffu, row_b == p);
+                    int at = in_a ? __ffs(in_a) - 1 : (in_b ? 32 + __ffs(in_b) - 1 : -1);
+                    if (at < 0) {
+                        at = count++;
+                        if (at < 32) {
+                            if (lane == static_cast<unsigned>(at)) row_a = src_a = p;
+                        } else if (lane == static_cast<unsigned>(at - 32)) {
+                            row_b = src_b = p;
+                        }
+                    }
+                    // exchange the contents of entries j and at
+                    const long long from_j = __shfl_sync(0xffffffffu, src_a, j);
+                    const long long from_at = at < 32 ? __shfl_sync(0xffffffffu, src_a, at & 31)
+                                                      : __shfl_sync(0xffffffffu, src_b, at & 31);
+                    if (lane == static_cast<unsigned>(j)) src_a = from_at;
+                    if (at < 32) {
+                        if (lane == static_cast<unsigned>(at)) src_a = from_j;
+                    } else if (lane == static_cast<unsigned>(at - 32)) {
+                        src_b = from_j;
+                    }
+                }
+                // keep the entries that moved, in order
+                const bool keep_a = static_cast<int>(lane) < count && row_a != src_a;
+                const bool keep_b = static_cast<int>(lane) + 32 < count && row_b != src_b;
+                const unsigned mask_a = __ballot_sync(0xffffffffu, keep_a), mask_b = __ballot_sync(0xffffffffu, keep_b);
+                const unsigned below = (1u << lane) - 1u;
+                if (keep_a) {
+                    const int slot = __popc(mask_a & below);
+                    moved->rows[slot] = row_a;
+                    moved->src[slot] = src_a;
+                }
+                if (keep_b) {
+                    const int slot = __popc(mask_a) + __popc(mask_b & below);
+                    moved->rows[slot] = row_b;
+                    moved->src[slot] = src_b;
+                }
+                if (lane == 0) moved->count = __popc(mask_a) + __popc(mask_b);
+            }
+            cluster_sync();  // no CTA leaves while another may still read its shared memory
+        }
+
+        // Applies a panel's net row movement to every column outside [skip0, skip1): all reads first,
+        // then all writes, so no exchange waits on another.
+        template <typename T>
+        __global__ void move_rows(T *a, unsigned long long n, const Movement *moved, unsigned long long skip0,
+                                  unsigned long long skip1) {
+            const unsigned long long col = blockIdx.x * 256ull + threadIdx.x;
+            if (col >= n || (col >= skip0 && col < skip1)) return;
+            const int count = static_cast<int>(moved->count);
+            T values[64];
+#pragma unroll
+            for (int i = 0; i < 64; ++i)
+                if (i < count) values[i] = a[static_cast<unsigned long long>(moved->src[i]) * n + col];
+#pragma unroll
+            for (int i = 0; i < 64; ++i)
+                if (i < count) a[static_cast<unsigned long long>(moved->rows[i]) * n + col] = values[i];
+        }
+
+        // rows[] of the factorisation (the original row at each position) from the exchanges, in
+        // shared memory by one thread: the only sequential step of the permutation.
+        __global__ void order_rows(const long long *piv, unsigned *rows, unsigned long long n) {
+            extern __shared__ unsigned order[];
+            for (unsigned long long i = threadIdx.x; i < n; i += blockDim.x) order[i] = static_cast<unsigned>(i);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                for (unsigned long long i = 0; i < n; ++i) {
+                    const unsigned long long p = static_cast<unsigned long long>(piv[i]);
+                    const unsigned x = order[i];
+                    order[i] = order[p];
+                    order[p] = x;
+                }
+            }
+            __syncthreads();
+            for (unsigned long long i = threadIdx.x; i < n; i += blockDim.x) rows[i] = order[i];
+        }
+
+        // x[i][:] = (U) b[rows[i]][:], optionally narrowing double to float: P b for the substitution.
+        template <typename S, typename D>
+        __global__ void gather_rows(const S *b, D *x, const unsigned *rows, unsigned long long n, unsigned long long width) {
+            const unsigned long long total = n * width;
+            for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < total; i += 256ull * gridDim.x) {
+                const unsigned long long row = i / width, column = i % width;
+                x[i] = static_cast<D>(b[static_cast<unsigned long long>(rows[row]) * width + column]);
+            }
+        }
+
+        // C (m x n, pitch ldc) -= A (m x k, pitch lda) * B (k x n, pitch ldb) for small k: 64 x BN tiles,
+        // K in slices of 32 through shared memory, 4 x (BN / 16) outputs per thread.
+        template <typename T, int BN>
+        __global__ void __launch_bounds__(256) rank_update(const T *__restrict__ a, unsigned long long lda,
+                                                           const T *__restrict__ b, unsigned long long ldb, T *c,
+                                                           unsigned long long ldc, unsigned long long m, unsigned long long n,
+                                                           unsigned long long k) {
+            constexpr int BM = 64, BK = 32, TN = BN / 16;
+            __shared__ T as[BK][BM + 1];
+            __shared__ T bs[BK][BN + 1];
+            const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+            const unsigned long long m0 = blockIdx.y * 1ull * BM, n0 = blockIdx.x * 1ull * BN;
+            T acc[4][TN];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
+            for (unsigned long long k0 = 0; k0 < k; k0 += BK) {
+                for (int i = threadIdx.x; i < BM * BK; i += 256) {
+                    const int row = i / BK, q = i % BK;
+                    const unsigned long long gr = m0 + row, gk = k0 + q;
+                    as[q][row] = (gr < m && gk < k) ? a[gr * lda + gk] : T(0);
+                }
+                for (int i = threadIdx.x; i < BK * BN; i += 256) {
+                    const int q = i / BN, col = i % BN;
+                    const unsigned long long gk = k0 + q, gc = n0 + col;
+                    bs[q][col] = (gk < k && gc < n) ? b[gk * ldb + gc] : T(0);
+                }
+                __syncthreads();
+#pragma unroll 8
+                for (int q = 0; q < BK; ++q) {
+                    T av[4], bv[TN];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) av[i] = as[q][ty * 4 + i];
+#pragma unroll
+                    for (int j = 0; j < TN; ++j) bv[j] = bs[q][tx * TN + j];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < TN; ++j) acc[i][j] = fma_(av[i], bv[j], acc[i][j]);
+                }
+                __syncthreads();
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const unsigned long long row = m0 + ty * 4 + i;
+                if (row >= m) continue;
+#pragma unroll
+                for (int j = 0; j < TN; ++j) {
+                    const unsigned long long col = n0 + tx * TN + j;
+                    if (col < n) c[row * ldc + col] = sub(c[row * ldc + col], acc[i][j]);
+                }
+            }
+        }
+
+        template <typename T>
+        int update(Context &ctx, const T *a, unsigned long long lda, const T *b, unsigned long long ldb, T *c,
+                   unsigned long long ldc, unsigned long long m, unsigned long long n, unsigned long long k) {
+            if (m == 0 || n == 0 || k == 0) return SCI_CUDA_OK;
+            if ((m + 63) / 64 > 65535) return ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "update: too many rows");
+            if (n <= 16) {
+                rank_update<T, 16><<<dim3(static_cast<unsigned>((n + 15) / 16), static_cast<unsigned>((m + 63) / 64)), 256, 0,
+                                     ctx.stream>>>(a, lda, b, ldb, c, ldc, m, n, k);
+            } else {
+                rank_update<T, 64><<<dim3(static_cast<unsigned>((n + 63) / 64), static_cast<unsigned>((m + 63) / 64)), 256, 0,
+                                     ctx.stream>>>(a, lda, b, ldb, c, ldc, m, n, k);
+            }
+            return ctx.check(cudaGetLastError(), "launching a rank update");
+        }
+
+        // Rows [j0, j0 + w) of columns [c0, c1) := L^-1 times themselves, L the unit lower triangle
+        // of the panel's top w x w block. One thread per column, the column's w values in registers.
+        template <typename T>
+        __global__ void trsm_rows(T *a, unsigned long long n, unsigned long long j0, int w, unsigned long long c0,
+                                  unsigned long long c1) {
+            constexpr int W = PanelWidth<T>::value;
+            __shared__ T lower[W][W];
+            for (int i = threadIdx.x; i < W * W; i += blockDim.x) {
+                const int row = i / W, k = i % W;
+                lower[row][k] = (row < w && k < w) ? a[(j0 + row) * n + j0 + k] : T(0);
+            }
+            __syncthreads();
+            const unsigned long long col = c0 + blockIdx.x * 1ull * blockDim.x + threadIdx.x;
+            if (col >= c1) return;
+            T x[W];
+#pragma unroll
+            for (int i = 0; i < W; ++i) x[i] = i < w ? a[(j0 + i) * n + col] : T(0);
+#pragma unroll
+            for (int i = 1; i < W; ++i) {
+#pragma unroll
+                for (int k = 0; k < i; ++k) x[i] = sub(x[i], mul(lower[i][k], x[k]));
+            }
+#pragma unroll
+            for (int i = 0; i < W; ++i)
+                if (i < w) a[(j0 + i) * n + col] = x[i];
+        }
+
+        // ---- substitution (solve.hpp:25-52), blocked ----------------------------------------------------
+        // One diagonal block of `size` rows: lower (unit) or upper (divide by the diagonal) solve of
+        // `width` right-hand-side columns in place. Warp w solves column (blockIdx.y * 32 + w); lane l
+        // holds rows l, l + 32, ... of the block.
+        template <typename T, bool upper>
+        __global__ void __launch_bounds__(1024) solve_block(const T *lu, unsigned long long n, unsigned long long s, int size, T *x,
+                                    unsigned long long width) {
+            extern __shared__ __align__(16) unsigned char solve_shared[];
+            T(*tri)[kSolveBlock + 1] = reinterpret_cast<T(*)[kSolveBlock + 1]>(solve_shared);
+            for (int i = threadIdx.x; i < size * size; i += blockDim.x) {
+                const int row = i / size, k = i % size;
+                tri[row][k] = lu[(s + row) * n + s + k];
+            }
+            __syncthreads();
+            const unsigned lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+            const unsigned long long column = blockIdx.y * 32ull + warp;
+            if (column >= width) return;
+            constexpr int R = kSolveBlock / 32;
+            T b[R];
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+                const int row = lane + 32 * q;
+                b[q] = row < size ? x[(s + row) * width + column] : T(0);
+            }
+            for (int step = 0; step < size; ++step) {
+                const int i = upper ? size - 1 - step : step;
+                const int owner = i % 32, slot = i / 32;
+                T value = T(0);
+#pragma unroll
+                for (int q = 0; q < R; ++q)
+                    if (q == slot) value = b[q];
+                if (upper) value = div(value, tri[i][i]);
+                value = __shfl_sync(0xffffffffu, value, owner);
+#pragma unroll
+                for (int q = 0; q < R; ++q) {
+                    const int row = lane + 32 * q;
+                    if (row == i) b[q] = value;
+                    else if (upper ? row < i : (row > i && row < size)) b[q] = sub(b[q], mul(tri[row][i], value));
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < R; ++q) {
+                const int row = lane + 32 * q;
+                if (row < size) x[(s + row) * width + column] = b[q];
+            }
+        }
+
+        // Inverses of the diagonal blocks of L (unit lower) and U, kSolveBlock x kSolveBlock each, zero
+        // padded past the matrix: inv[2 b] is L's block b, inv[2 b + 1] U's. Thread c computes column c
+        // of both by substitution against the identity (solve.hpp:25-52 applied to e_c), reading back
+        // only the entries it wrote itself.
+        template <typename T>
+        __global__ void __launch_bounds__(kSolveBlock) invert_blocks(const T *lu, unsigned long long n, T *inv) {
+            constexpr int B = kSolveBlock;
+            const unsigned long long s = blockIdx.x * 1ull * B;
+            const int size = static_cast<int>(n - s < B ? n - s : B);
+            const int c = threadIdx.x;
+            T *lower = inv + 2ull * blockIdx.x * B * B;
+            T *upper = lower + 1ull * B * B;
+            const T *d = lu + s * n + s;
+            for (int i = 0; i < B; ++i) {
+                T value = T(0);
+                if (c < size && i < size && i >= c) {
+                    value = i == c ? T(1) : T(0);
+                    for (int k = c; k < i; ++k) value = fma_(-d[i * n + k], lower[k * B + c], value);
+                }
+                lower[i * B + c] = value;
+            }
+            for (int i = B - 1; i >= 0; --i) {
+                T value = T(0);
+                if (c < size && i < size && i <= c) {
+                    value = i == c ? T(1) : T(0);
+                    for (int k = i + 1; k <= c; ++k) value = fma_(-d[i * n + k], upper[k * B + c], value);
+                    value = div(value, d[i * n + i]);
+                }
+                upper[i * B + c] = value;
+            }
+        }
+
+        // x[s + r][col] := sum_k inv[r][k] x[s + k][col] for the `size` rows of one diagonal block, 32
+        // columns per CTA (blockIdx.y): the block's inverse and its rows of x are read whole into
+        // shared memory before any row is written. Warp w computes rows 4w .. 4w + 3, lane = column.
+        // inv is triangular: lower blocks sum over k <= r, upper ones over k >= r.
+        template <typename T, bool upper>
+        __global__ void __launch_bounds__(1024) apply_inverse(const T *inv, unsigned long long s, int size, T *x,
+                                                              unsigned long long width) {
+            constexpr int B = kSolveBlock;
+            extern __shared__ __align__(16) unsigned char apply_shared[];
+            T *ms = reinterpret_cast<T *>(apply_shared);  // [B][B]: the inverse
+            T *xs = ms + B * B;                           // [B][32]: the block of x
+            const unsigned long long c0 = blockIdx.y * 32ull;
+            for (int i = threadIdx.x; i < B * B; i += 1024) ms[i] = inv[i];
+            for (int i = threadIdx.x; i < B * 32; i += 1024) {
+                const int k = i / 32, col = i % 32;
+                xs[i] = (k < size && c0 + col < width) ? x[(s + k) * width + c0 + col] : T(0);
+            }
+            __syncthreads();
+            const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
+            const unsigned long long col = c0 + lane;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = warp * 4 + q;
+                if (r >= size) break;
+                const int k0 = upper ? r : 0, k1 = upper ? size : r + 1;
+                T acc = T(0);
+                for (int k = k0; k < k1; ++k) acc = fma_(ms[r * B + k], xs[k * 32 + lane], acc);
+                if (col < width) x[(s + r) * width + col] = acc;
+            }
+        }
+
+        // ---- FP64 helpers of the refinement -----------------------------------------------------------
+        __global__ void narrow(const double *in, float *out, unsigned long long count) {
+            for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < count; i += 256ull * gridDim.x)
+                out[i] = static_cast<float>(in[i]);
+        }
+        __global__ void widen_add(const float *d, double *x, unsigned long long count) {
+            for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < count; i += 256ull * gridDim.x)
+                x[i] += static_cast<double>(d[i]);
+        }
+        // |rows of a|_1, the infinity norm's terms: one warp per row.
+        template <typename T> __global__ void row_sums(const T *a, unsigned long long n, double *out) {
+            const unsigned long long row = blockIdx.x * 8ull + threadIdx.x / 32;
+            if (row >= n) return;
+            double s = 0.0;
+            for (unsigned long long k = threadIdx.x % 32; k < n; k += 32) s += fabs(static_cast<double>(a[row * n + k]));
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (threadIdx.x % 32 == 0) out[row] = s;
+        }
+        // Per column of an n x width matrix: the largest |entry| (NaN propagates).
+        __global__ void column_max(const double *m, unsigned long long n, unsigned long long width, double *out) {
+            const unsigned long long column = blockIdx.x;
+            double best = 0.0;
+            for (unsigned long long i = threadIdx.x; i < n; i += blockDim.x) {
+                const double v = fabs(m[i * width + column]);
+                best = (v > best || v != v) ? v : best;
+            }
+            __shared__ double shared[256];
+            shared[threadIdx.x] = best;
+            __syncthreads();
+            for (unsigned s = blockDim.x / 2; s > 0; s >>= 1) {
+                if (threadIdx.x < s) {
+                    const double o = shared[threadIdx.x + s];
+                    shared[threadIdx.x] = (o > shared[threadIdx.x] || o != o) ? o : shared[threadIdx.x];
+                }
+                __syncthreads();
+            }
+            if (threadIdx.x == 0) out[column] = shared[0];
+        }
+
+        unsigned blocks_for(unsigned long long count, int sms) {
+            return static_cast<unsigned>(std::max<unsigned long long>(1, std::min<unsigned long long>((count + 255) / 256, sms * 32ull)));
+        }
+
+        // In-place blocked LU of an n x n row-major matrix on the context's stream; pivots to piv
+        // (device, LAPACK style: at step k row k was exchanged with row piv[k]).
+        template <typename T>
+        int factor_device(Context &ctx, T *a, unsigned long long n, long long *piv, Movement *moved, bool tensor,
+                          bool split) {
+            constexpr int W = PanelWidth<T>::value;
+            if (n > kPanelRows) return ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "factor: order %llu above %llu", n, kPanelRows);
+            if (tensor && sizeof(T) == 4 && n > kOuter) {
+                // the largest trailing update reserves the product workspace once
+                const unsigned long long big = n - kOuter;
+                if (int code = ctx.check(ctx.workspace->reserve((split ? 3 : 1) * (2 * big * kOuter * 2 + 2048) + 1024),
+                                         "reserving the trailing-update workspace"))
+                    return code;
+            }
+            for (unsigned long long J0 = 0; J0 < n; J0 += kOuter) {
+                const unsigned long long ob = std::min<unsigned long long>(kOuter, n - J0);
+                for (unsigned long long j0 = J0; j0 < J0 + ob; j0 += W) {
+                    const int w = static_cast<int>(std::min<unsigned long long>(W, J0 + ob - j0));
+                    panel_factor<T><<<kClusterCtas, kPanelThreads, 0, ctx.stream>>>(a, n, j0, w, piv, moved);
+                    if (int code = ctx.check(cudaGetLastError(), "launching the panel factorisation")) return code;
+                    move_rows<T><<<static_cast<unsigned>((n + 255) / 256), 256, 0, ctx.stream>>>(a, n, moved, j0, j0 + w);
+                    // Inside the outer block only: U rows of the panel, then the rows below it. Columns
+                    // beyond the block wait until the block's pivots are all known (a later pivot of
+                    // this block may still bring a row up from below).
+                    const unsigned long long right = j0 + w, block_end = J0 + ob;
+                    if (right < block_end) {
+                        trsm_rows<T><<<static_cast<unsigned>((block_end - right + 127) / 128), 128, 0, ctx.stream>>>(
+                                a, n, j0, w, right, block_end);
+                        if (int code = update<T>(ctx, a + right * n + j0, n, a + j0 * n + right, n, a + right * n + right, n,
+                                                 n - right, block_end - right, w))
+                            return code;
+                    }
+                    if (int code = ctx.check(cudaGetLastError(), "launching the panel updates")) return code;
+                }
+                // U12 (the block's rows, columns beyond it) = L11^-1 A12, panel by panel, now that
+                // every row exchange of the block has been applied.
+                const unsigned long long block_end = J0 + ob;
+                if (block_end < n) {
+                    for (unsigned long long j0 = J0; j0 < block_end; j0 += W) {
+                        const int w = static_cast<int>(std::min<unsigned long long>(W, block_end - j0));
+                        trsm_rows<T><<<static_cast<unsigned>((n - block_end + 127) / 128), 128, 0, ctx.stream>>>(
+                                a, n, j0, w, block_end, n);
+                        const unsigned long long below = j0 + w;
+                        if (below < block_end) {
+                            if (int code = update<T>(ctx, a + below * n + j0, n, a + j0 * n + block_end, n,
+                                                     a + below * n + block_end, n, block_end - below, n - block_end, w))
+                                return code;
+                        }
+                    }
+                    if (int code = ctx.check(cudaGetLastError(), "launching the block's U rows")) return code;
+                }
+                // trailing update: A22 -= L21 * U12, K = ob
+                const unsigned long long t0 = J0 + ob;
+                if (t0 < n) {
+                    int code;
+                    if constexpr (sizeof(T) == 4) {
+                        if (tensor) {
+                            code = tensor_gemm(ctx, split ? 3 : 1, a + t0 * n + J0, n, a + J0 * n + t0, n, a + t0 * n + t0, n,
+                                               n - t0, n - t0, ob, true);
+                        } else {
+                            code = simt_gemm<T>(ctx, a + t0 * n + J0, n, a + J0 * n + t0, n, a + t0 * n + t0, n, n - t0,
+                                                n - t0, ob, true);
+                        }
+                    } else {
+                        code = simt_gemm<T>(ctx, a + t0 * n + J0, n, a + J0 * n + t0, n, a + t0 * n + t0, n, n - t0, n - t0,
+                                            ob, true);
+                    }
+                    if (code) return code;
+                }
+            }
+            return SCI_CUDA_OK;
+        }
+
+        unsigned long long inverse_elements(unsigned long long n) {
+            return 2ull * ((n + kSolveBlock - 1) / kSolveBlock) * kSolveBlock * kSolveBlock;
+        }
+
+        template <typename T> int invert_diagonal(Context &ctx, const T *lu, unsigned long long n, T *inv) {
+            invert_blocks<T><<<static_cast<unsigned>((n + kSolveBlock - 1) / kSolveBlock), kSolveBlock, 0, ctx.stream>>>(lu, n,
+                                                                                                                       inv);
+            return ctx.check(cudaGetLastError(), "inverting the diagonal blocks");
+        }
+
+        // x (n x width, in place: holds P b on entry) := U^-1 L^-1 x. With inv (from invert_diagonal)
+        // each diagonal block is one small product; without it, a substitution in the reference's
+        // order inside the block (FP64 solves keep that form).
+        template <typename T>
+        int substitute_device(Context &ctx, const T *lu, const T *inv, unsigned long long n, T *x, unsigned long long width) {
+            const dim3 groups(1, static_cast<unsigned>((width + 31) / 32));
+            const size_t smem = inv ? sizeof(T) * (kSolveBlock * kSolveBlock + kSolveBlock * 32)
+                                    : sizeof(T) * kSolveBlock * (kSolveBlock + 1);
+            const void *forward = inv ? reinterpret_cast<const void *>(&apply_inverse<T, false>)
+                                      : reinterpret_cast<const void *>(&solve_block<T, false>);
+            const void *backward = inv ? reinterpret_cast<const void *>(&apply_inverse<T, true>)
+                                       : reinterpret_cast<const void *>(&solve_block<T, true>);
+            cudaFuncSetAttribute(forward, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+            cudaFuncSetAttribute(backward, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+            constexpr unsigned long long block_elements = 1ull * kSolveBlock * kSolveBlock;
+            for (unsigned long long s = 0; s < n; s += kSolveBlock) {
+                const int size = static_cast<int>(std::min<unsigned long long>(kSolveBlock, n - s));
+                if (inv)
+                    apply_inverse<T, false><<<groups, 1024, smem, ctx.stream>>>(inv + 2 * (s / kSolveBlock) * block_elements, s,
+                                                                                size, x, width);
+                else
+                    solve_block<T, false><<<groups, 1024, smem, ctx.stream>>>(lu, n, s, size, x, width);
+                const unsigned long long below = s + size;
+                if (below < n) {
+                    if (int code = update<T>(ctx, lu + below * n + s, n, x + s * width, width, x + below * width, width,
+                                             n - below, width, size))
+                        return code;
+                }
+            }
+            const unsigned long long last = (n - 1) / kSolveBlock * kSolveBlock;
+            for (long long s = static_cast<long long>(last); s >= 0; s -= kSolveBlock) {
+                const unsigned long long us = static_cast<unsigned long long>(s);
+                const int size = static_cast<int>(std::min<unsigned long long>(kSolveBlock, n - us));
+                if (inv)
+                    apply_inverse<T, true><<<groups, 1024, smem, ctx.stream>>>(
+                            inv + (2 * (us / kSolveBlock) + 1) * block_elements, us, size, x, width);
+                else
+                    solve_block<T, true><<<groups, 1024, smem, ctx.stream>>>(lu, n, us, size, x, width);
+                if (us > 0) {
+                    if (int code = update<T>(ctx, lu + us, n, x + us * width, width, x, width, us, width, size))
+                        return code;
+                }
+            }
+            return ctx.check(cudaGetLastError(), "launching the substitution");
+        }
+
+        // rows[] (device) from the exchanges of factor_device.
+        int row_order(Context &ctx, const long long *piv, unsigned *rows, unsigned long long n) {
+            order_rows<<<1, 1024, n * sizeof(unsigned), ctx.stream>>>(piv, rows, n);
+            return ctx.check(cudaGetLastError(), "ordering the rows");
+        }
+
+        // x = (P b) in the element type D.
+        template <typename S, typename D>
+        void permute(Context &ctx, const S *b, D *x, const unsigned *rows, unsigned long long n, unsigned long long width) {
+            gather_rows<S, D><<<blocks_for(n * width, ctx.sms), 256, 0, ctx.stream>>>(b, x, rows, n, width);
+        }
+
+        // Workspace carving helper.
+        struct Carve {
+            unsigned char *base;
+            unsigned long long used{0};
+            template <typename T> T *take(unsigned long long count) {
+                T *p = reinterpret_cast<T *>(base + used);
+                used += (count * sizeof(T) + 255) / 256 * 256;
+                return p;
+            }
+        };
+
+    } // namespace
+
+} // namespace sci_cuda
+
+using namespace sci_cuda;
+
+extern "C" int sci_cuda_factor(sci_cuda_context *context, uint32_t precision, uint32_t mode, void *matrix, uint64_t *rows,
+                               uint64_t order) {
+    if (!context) return SCI_CUDA_ERROR_INVALID;
+    std::lock_guard<std::recursive_mutex> lock(context->guard);
+    if (precision > SCI_PRECISION_WIDE || mode > SCI_FACTOR_PLAIN)
+        return context->fail(SCI_CUDA_ERROR_INVALID, "unknown precision %u or mode %u", precision, mode);
+    if (order == 0) return SCI_CUDA_OK;
+    if (!matrix || !rows) return context->fail(SCI_CUDA_ERROR_INVALID, "null matrix or rows");
+    cudaSetDevice(context->device);
+    if (int code = context->check(context->solver->reserve(order * 8 + sizeof(Movement) + 1024), "pivot storage")) return code;
+    Carve carve{static_cast<unsigned char *>(context->solver->memory)};
+    long long *piv = carve.take<long long>(order);
+    Movement *moved = carve.take<Movement>(1);
+    int code = precision == SCI_PRECISION_WIDE
+                       ? factor_device<double>(*context, static_cast<double *>(matrix), order, piv, moved, false, false)
+                       : factor_device<float>(*context, static_cast<float *>(matrix), order, piv, moved,
+                                              mode != SCI_FACTOR_PLAIN, true);
+    std::vector<long long> host(order);
+    if (!code) code = context->check(cudaMemcpyAsync(host.data(), piv, order * sizeof(long long), cudaMemcpyDeviceToHost,
+                                                     context->stream),
+                                     "reading the pivots");
+    if (!code) code = context->drain();
+    if (code) return code;
+    // rows[i] = the original row now at position i (decompose.hpp:30-42)
+    for (uint64_t i = 0; i < order; ++i) rows[i] = i;
+    for (uint64_t i = 0; i < order; ++i) std::swap(rows[i], rows[static_cast<uint64_t>(host[i])]);
+    return SCI_CUDA_OK;
+}
+
+namespace {
+
+    // The normwise backward error max_j |b_j - A x_j|_inf / (|A|_inf |x_j|_inf + |b_j|_inf), in FP64.
+    // r is scratch (n x width), sums (n), norms (2 width); waits for the stream.
+    int backward_error(Context &ctx, const double *a, const double *b, const double *x, double *r, double *sums,
+                       double *norms, unsigned long long n, unsigned long long width, double a_norm, const double *b_norm,
+                       double &berr) {
+        cudaMemcpyAsync(r, b, n * width * 8, cudaMemcpyDeviceToDevice, ctx.stream);
+        if (int code = update<double>(ctx, a, n, x, width, r, width, n, width, n)) return code;
+        column_max<<<static_cast<unsigned>(width), 256, 0, ctx.stream>>>(r, n, width, norms);
+        column_max<<<static_cast<unsigned>(width), 256, 0, ctx.stream>>>(x, n, width, norms + width);
+        std::vector<double> host(2 * width);
+        cudaMemcpyAsync(host.data(), norms, 2 * width * 8, cudaMemcpyDeviceToHost, ctx.stream);
+        if (int code = ctx.drain()) return code;
+        berr = 0.0;
+        for (unsigned long long j = 0; j < width; ++j) {
+            const double e = host[j] / (a_norm * host[width + j] + b_norm[j]);
+            berr = (e > berr || e != e) ? e : berr;
+        }
+        return SCI_CUDA_OK;
+    }
+
+    // |A|_inf and |b_j|_inf on the host.
+    int norms_of(Context &ctx, const double *a, const double *b, double *sums, double *norms, unsigned long long n,
+                 unsigned long long width, double &a_norm, std::vector<double> &b_norm) {
+        row_sums<double><<<static_cast<unsigned>((n + 7) / 8), 256, 0, ctx.stream>>>(a, n, sums);
+        column_max<<<static_cast<unsigned>(width), 256, 0, ctx.stream>>>(b, n, width, norms);
+        std::vector<double> host_sums(n);
+        b_norm.assign(width, 0.0);
+        cudaMemcpyAsync(host_sums.data(), sums, n * 8, cudaMemcpyDeviceToHost, ctx.stream);
+        cudaMemcpyAsync(b_norm.data(), norms, width * 8, cudaMemcpyDeviceToHost, ctx.stream);
+        if (int code = ctx.drain()) return code;
+        a_norm = 0.0;
+        for (double v : host_sums) a_norm = std::max(a_norm, v);
+        return SCI_CUDA_OK;
+    }
+
+} // namespace
+
+extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uint32_t refine, const void *matrix,
+                              const void *right, void *solution, uint64_t order, uint64_t width, sci_solve_report *report) {
+    if (!context) return SCI_CUDA_ERROR_INVALID;
+    std::lock_guard<std::recursive_mutex> lock(context->guard);
+    if (precision > SCI_PRECISION_WIDE || refine > SCI_REFINE_FP64)
+        return context->fail(SCI_CUDA_ERROR_INVALID, "unknown precision %u or refinement %u", precision, refine);
+    if (refine == SCI_REFINE_FP64 && precision != SCI_PRECISION_WIDE)
+        return context->fail(SCI_CUDA_ERROR_INVALID, "FP64 refinement needs double operands");
+    if (report) std::memset(report, 0, sizeof(*report));
+    if (order == 0 || width == 0) return SCI_CUDA_OK;
+    if (!matrix || !right || !solution) return context->fail(SCI_CUDA_ERROR_INVALID, "null operand");
+    if (order > kPanelRows) return context->fail(SCI_CUDA_ERROR_UNSUPPORTED, "solve: order %llu above %llu",
+                                                 static_cast<unsigned long long>(order), kPanelRows);
+    cudaSetDevice(context->device);
+    const unsigned long long n = order, nw = order * width;
+    const bool wide = precision == SCI_PRECISION_WIDE;
+    const size_t element = (wide && refine == SCI_REFINE_NONE) ? 8 : 4;
+    const unsigned long long need = n * n * element + n * 8 + sizeof(Movement) + n * 4 + nw * 12 + n * 8 + width * 16 +
+                                    inverse_elements(n) * 4 + 8192;
+    if (int code = context->check(context->solver->reserve(need), "reserving the solver workspace")) return code;
+    Carve carve{static_cast<unsigned char *>(context->solver->memory)};
+    long long *piv = carve.take<long long>(n);
+    Movement *moved = carve.take<Movement>(1);
+    unsigned *rows = carve.take<unsigned>(n);
+
+    if (refine == SCI_REFINE_NONE) {
+        // linear::solve (solve.hpp:60-76): factor a copy, substitute, in the element type.
+        int code;
+        if (wide) {
+            double *lu = carve.take<double>(n * n);
+            cudaMemcpyAsync(lu, matrix, n * n * 8, cudaMemcpyDeviceToDevice, context->stream);
+            code = factor_device<double>(*context, lu, n, piv, moved, false, false);
+            if (!code) code = row_order(*context, piv, rows, n);
+            if (!code) permute<double, double>(*context, static_cast<const double *>(right), static_cast<double *>(solution),
+                                               rows, n, width);
+            if (!code) code = substitute_device<double>(*context, lu, nullptr, n, static_cast<double *>(solution), width);
+            if (!code && report) {
+                double *r = carve.take<double>(nw);
+                double *sums = carve.take<double>(n);
+                double *norms = carve.take<double>(2 * width);
+                double a_norm = 0.0, berr = 0.0;
+                std::vector<double> b_norm;
+                code = norms_of(*context, static_cast<const double *>(matrix), static_cast<const double *>(right), sums,
+                                norms, n, width, a_norm, b_norm);
+                if (!code)
+                    code = backward_error(*context, static_cast<const double *>(matrix), static_cast<const double *>(right),
+                                          static_cast<const double *>(solution), r, sums, norms, n, width, a_norm,
+                                          b_norm.data(), berr);
+                if (!code) report->backward_error = berr;
+            }
+        } else {
+            float *lu = carve.take<float>(n * n);
+            float *inv = carve.take<float>(inverse_elements(n));
+            cudaMemcpyAsync(lu, matrix, n * n * 4, cudaMemcpyDeviceToDevice, context->stream);
+            code = factor_device<float>(*context, lu, n, piv, moved, true, true);
+            if (!code) code = invert_diagonal<float>(*context, lu, n, inv);
+            if (!code) code = row_order(*context, piv, rows, n);
+            if (!code) permute<float, float>(*context, static_cast<const float *>(right), static_cast<float *>(solution), rows,
+                                             n, width);
+            if (!code) code = substitute_device<float>(*context, lu, inv, n, static_cast<float *>(solution), width);
+        }
+        if (!code) code = context->drain();
+        return code;
+    }
+
+    // FP32 factorisation, FP64 residual and update.
+    const double *a = static_cast<const double *>(matrix);
+    const double *b = static_cast<const double *>(right);
+    double *x = static_cast<double *>(solution);
+    float *lu = carve.take<float>(n * n);
+    float *inv = carve.take<float>(inverse_elements(n));
+    double *r = carve.take<double>(nw);
+    float *d = carve.take<float>(nw);
+    double *sums = carve.take<double>(n);
+    double *norms = carve.take<double>(2 * width);
+    const int sms = context->sms;
+
+    narrow<<<blocks_for(n * n, sms), 256, 0, context->stream>>>(a, lu, n * n);
+    if (int code = factor_device<float>(*context, lu, n, piv, moved, true, true)) return code;
+    if (int code = invert_diagonal<float>(*context, lu, n, inv)) return code;
+    if (int code = row_order(*context, piv, rows, n)) return code;
+    double a_norm = 0.0;
+    std::vector<double> b_norm;
+    if (int code = norms_of(*context, a, b, sums, norms, n, width, a_norm, b_norm)) return code;
+    cudaMemsetAsync(x, 0, nw * 8, context->stream);
+
+    double previous = INFINITY, berr = INFINITY;
+    int iterations = 0;
+    constexpr int kMaxIterations = 30;
+    const double *residual = b;  // the first correction solves for b itself
+    while (iterations < kMaxIterations) {
+        permute<double, float>(*context, residual, d, rows, n, width);
+        if (int code = substitute_device<float>(*context, lu, inv, n, d, width)) return code;
+        widen_add<<<blocks_for(nw, sms), 256, 0, context->stream>>>(d, x, nw);
+        ++iterations;
+        if (int code = backward_error(*context, a, b, x, r, sums, norms, n, width, a_norm, b_norm.data(), berr)) return code;
+        residual = r;
+        if (!(berr > 1e-15) || !(berr < 0.5 * previous)) break;
+        previous = berr;
+    }
+    if (report) {
+        report->backward_error = berr;
+        report->iterations = iterations;
+    }
+    return SCI_CUDA_OK;
+}

@@ -9,12 +9,14 @@
 //  - SCI_PRODUCT_SPLIT_BF16: each operand split into hi + lo bf16 parts, three tensor-core
 //    products hi*hi + hi*lo + lo*hi accumulated in the same TMEM tile (the lo*lo term, below
 //    2^-16 relative, is dropped);
+//  - SCI_PRODUCT_SPLIT3_BF16: hi + mid + lo parts and the six products down to 2^-24 relative,
+//    about FP32 accuracy (the LU's trailing update uses it);
 //  - SCI_PRODUCT_FP32: a plain FP32 SIMT kernel, the comparison form.
 // Double products run a plain FP64 SIMT kernel.
 //
-// The tensor-core kernel: one CTA per 128 x 256 output tile, six warps. Warp 4 issues TMA loads of
-// 64-deep K slices of A (128 x 64) and of B^T (256 x 64) into a ring of shared-memory stages
-// (128-byte swizzle); warp 5 issues tcgen05.mma (M=128, N=256, K=16) from one thread and
+// The tensor-core kernel: one CTA per 128 x 256 output tile (128 x 128 with three terms), six warps.
+// Warp 4 issues TMA loads of 64-deep K slices of every term of A (128 x 64) and of B^T (N x 64) into
+// a ring of shared-memory stages (128-byte swizzle); warp 5 issues tcgen05.mma (M=128, K=16) from one thread and
 // commits each stage back to the producer; warps 0-3 read the FP32 accumulator out of tensor
 // memory (tcgen05.ld, 32 lanes each) and store C. Every mbarrier wait is bounded: on timeout the
 // kernel records an error word, stops issuing, frees its tensor memory and returns.
@@ -32,48 +34,49 @@ namespace sci_cuda {
 
     namespace {
 
-        constexpr int kBM = 128, kBN = 256, kBK = 64;  // output tile and K slice (bf16: 64 x 2 = 128 bytes)
+        constexpr int kBM = 128, kBK = 64;  // output tile and K slice (bf16: 64 x 2 = 128 bytes)
         constexpr int kUmmaK = 16;
-        constexpr int kStagesPlain = 4, kStagesSplit = 2;
-        constexpr unsigned kTmemColumns = 256;
-        constexpr unsigned kProductWait = 1u << 24;
+                        constexpr unsigned kProductWait = 1u << 24;
 
-        // ---- conversion: fp32 -> bf16 (hi, and lo = bf16(a - hi)), padded along K ----------------
-        // A is M x K row-major; its bf16 copies are M x Kp (Kp = K rounded up to 64, zero-filled).
-        __global__ void split_rows(const float *__restrict__ a, __nv_bfloat16 *__restrict__ hi,
-                                   __nv_bfloat16 *__restrict__ lo, unsigned long long rows, unsigned long long k,
-                                   unsigned long long kp) {
+        // ---- conversion: fp32 -> up to three bf16 terms, padded along K -------------------------------
+        // a = t0 + t1 + t2 + (a remainder): t0 = bf16(a), t1 = bf16(a - t0), t2 = bf16(a - t0 - t1), each
+        // difference exact in float. A is M x K row-major (pitch lda); its terms are M x Kp (Kp = K
+        // rounded up to 64, zero-filled).
+        struct Terms {
+            __nv_bfloat16 *t[3];
+        };
+        __device__ __forceinline__ void split_value(float v, int terms, const Terms &out, unsigned long long at) {
+            float rest = v;
+            for (int q = 0; q < terms; ++q) {
+                const __nv_bfloat16 h = __float2bfloat16_rn(rest);
+                out.t[q][at] = h;
+                rest = rest - __bfloat162float(h);
+            }
+        }
+        __global__ void split_rows(const float *__restrict__ a, unsigned long long lda, Terms out, int terms,
+                                   unsigned long long rows, unsigned long long k, unsigned long long kp) {
             const unsigned long long total = rows * kp;
             for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < total; i += 256ull * gridDim.x) {
                 const unsigned long long r = i / kp, c = i % kp;
-                const float v = c < k ? a[r * k + c] : 0.0f;
-                const __nv_bfloat16 h = __float2bfloat16_rn(v);
-                hi[i] = h;
-                if (lo) lo[i] = __float2bfloat16_rn(v - __bfloat162float(h));
+                split_value(c < k ? a[r * lda + c] : 0.0f, terms, out, i);
             }
         }
 
-        // B is K x N row-major; its bf16 copies are the transpose, N x Kp, so both operands are
+        // B is K x N row-major (pitch ldb); its terms are the transpose, N x Kp, so both operands are
         // K-major. 32 x 32 tiles through shared memory keep both sides coalesced.
-        __global__ void split_transpose(const float *__restrict__ b, __nv_bfloat16 *__restrict__ hi,
-                                        __nv_bfloat16 *__restrict__ lo, unsigned long long k, unsigned long long n,
-                                        unsigned long long kp) {
+        __global__ void split_transpose(const float *__restrict__ b, unsigned long long ldb, Terms out, int terms,
+                                        unsigned long long k, unsigned long long n, unsigned long long kp) {
             __shared__ float tile[32][33];
             const unsigned long long k0 = blockIdx.y * 32ull, n0 = blockIdx.x * 32ull;
             const unsigned tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
             for (unsigned j = ty; j < 32; j += 8) {
                 const unsigned long long kk = k0 + j, nn = n0 + tx;
-                tile[j][tx] = (kk < k && nn < n) ? b[kk * n + nn] : 0.0f;
+                tile[j][tx] = (kk < k && nn < n) ? b[kk * ldb + nn] : 0.0f;
             }
             __syncthreads();
             for (unsigned j = ty; j < 32; j += 8) {
                 const unsigned long long nn = n0 + j, kk = k0 + tx;
-                if (nn < n && kk < kp) {
-                    const float v = tile[tx][j];
-                    const __nv_bfloat16 h = __float2bfloat16_rn(v);
-                    hi[nn * kp + kk] = h;
-                    if (lo) lo[nn * kp + kk] = __float2bfloat16_rn(v - __bfloat162float(h));
-                }
+                if (nn < n && kk < kp) split_value(tile[tx][j], terms, out, nn * kp + kk);
             }
         }
 
@@ -122,14 +125,14 @@ namespace sci_cuda {
             const unsigned long long lbo = 1ull, sbo = 1024ull >> 4;
             return start | (lbo << 16) | (sbo << 32) | (1ull << 46) | (2ull << 61);
         }
-        // kind::f16 instruction descriptor: D = F32, A = B = BF16, both K-major, M = 128, N = 256.
-        constexpr unsigned kInstr = (1u << 4) | (1u << 7) | (1u << 10) | (unsigned(kBN >> 3) << 17) | (unsigned(kBM >> 4) << 24);
-
-        __device__ __forceinline__ void mma_bf16(unsigned tmem, unsigned long long a, unsigned long long b, unsigned accumulate) {
+        // kind::f16 instruction descriptor (cute/arch/mma_sm100_desc.hpp InstrDescriptor layout):
+        // D = F32 (bits 4-5), A = B = BF16 (bits 7-9, 10-12), both K-major, N >> 3 at bit 17, M >> 4 at bit 24.
+        __device__ __forceinline__ void mma_bf16(unsigned tmem, unsigned long long a, unsigned long long b, unsigned instr,
+                                                 unsigned accumulate) {
             asm volatile(
                     "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-                    "l"(a), "l"(b), "r"(kInstr), "r"(accumulate)
+                    "l"(a), "l"(b), "r"(instr), "r"(accumulate)
                     : "memory");
         }
         __device__ __forceinline__ void mma_commit(unsigned long long *bar) {
@@ -139,19 +142,40 @@ namespace sci_cuda {
 
         struct ProductArgs {
             float *c;
-            unsigned long long m, n, kp;
+            unsigned long long m, n, kp, ldc;
+            int subtract;  // C -= A B instead of C = A B
             int *status;
         };
 
-        // One 128 x 256 tile of C per CTA. `split` adds the hi*lo and lo*hi products.
-        template <bool split>
-        __global__ void __launch_bounds__(192, 1)
-                tensor_product(const __grid_constant__ CUtensorMap a_hi, const __grid_constant__ CUtensorMap a_lo,
-                               const __grid_constant__ CUtensorMap b_hi, const __grid_constant__ CUtensorMap b_lo,
-                               const ProductArgs args) {
-            constexpr int S = split ? kStagesSplit : kStagesPlain;
-            constexpr unsigned A_BYTES = kBM * kBK * 2, B_BYTES = kBN * kBK * 2;
-            constexpr unsigned STAGE = split ? 2 * (A_BYTES + B_BYTES) : (A_BYTES + B_BYTES);
+        // The bf16 term products a tensor-core tile accumulates: (i, j) multiplies term i of A by term
+        // j of B. One term: t0 t0. Two: + t0 t1 + t1 t0. Three: + t0 t2 + t1 t1 + t2 t0 (the dropped
+        // products are below 2^-24 relative).
+        template <int TERMS> struct Products {
+            static constexpr int count = TERMS == 1 ? 1 : (TERMS == 2 ? 3 : 6);
+        };
+        // product p multiplies term product_a(p) of A by term product_b(p) of B:
+        // (0,0) (0,1) (1,0) (0,2) (1,1) (2,0)
+        __host__ __device__ constexpr int product_a(int p) { return (p == 2 || p == 4) ? 1 : (p == 5 ? 2 : 0); }
+        __host__ __device__ constexpr int product_b(int p) { return (p == 1 || p == 4) ? 1 : (p == 3 ? 2 : 0); }
+        template <int TERMS> struct Shape {
+            static constexpr int BN = TERMS == 3 ? 128 : 256;  // N of the tile and of the MMA
+            static constexpr int stages = TERMS == 1 ? 4 : 2;
+            static constexpr unsigned a_bytes = kBM * kBK * 2, b_bytes = BN * kBK * 2;
+            static constexpr unsigned stage = TERMS * (a_bytes + b_bytes);
+            static constexpr unsigned instr =
+                    (1u << 4) | (1u << 7) | (1u << 10) | (unsigned(BN >> 3) << 17) | (unsigned(kBM >> 4) << 24);
+        };
+
+        struct Maps {
+            CUtensorMap a[3], b[3];
+        };
+
+        // One 128 x BN tile of C per CTA.
+        template <int TERMS>
+        __global__ void __launch_bounds__(192, 1) tensor_product(const __grid_constant__ Maps maps, const ProductArgs args) {
+            using Sh = Shape<TERMS>;
+            using Pr = Products<TERMS>;
+            constexpr int S = Sh::stages, BN = Sh::BN;
             extern __shared__ unsigned char raw[];
             __shared__ unsigned long long full[S], empty[S], done;
             __shared__ unsigned tmem_slot;
@@ -160,7 +184,7 @@ namespace sci_cuda {
 
             const unsigned warp = threadIdx.x / 32, lane = threadIdx.x % 32;
             const unsigned long long m0 = static_cast<unsigned long long>(blockIdx.y) * kBM;
-            const unsigned long long n0 = static_cast<unsigned long long>(blockIdx.x) * kBN;
+            const unsigned long long n0 = static_cast<unsigned long long>(blockIdx.x) * BN;
             const int kblocks = static_cast<int>(args.kp / kBK);
 
             if (threadIdx.x == 0) {
@@ -172,14 +196,14 @@ namespace sci_cuda {
                 abort_flag = 0;
                 asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
             }
-            if (warp == 0) tmem_alloc(&tmem_slot, kTmemColumns);
+            if (warp == 0) tmem_alloc(&tmem_slot, BN);
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncthreads();
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const unsigned tmem = tmem_slot;
 
             if (warp == 4 && lane == 0) {
-                // TMA producer
+                // TMA producer: stage = [A term 0 .. TERMS-1][B term 0 .. TERMS-1]
                 for (int kb = 0; kb < kblocks; ++kb) {
                     const int s = kb % S;
                     if (kb >= S && !mbar_wait(&empty[s], ((kb / S) - 1) & 1)) {
@@ -187,14 +211,14 @@ namespace sci_cuda {
                         break;
                     }
                     if (*static_cast<volatile int *>(&abort_flag)) break;
-                    unsigned char *stage = ring + s * STAGE;
-                    mbar_expect(&full[s], STAGE);
+                    unsigned char *stage = ring + s * Sh::stage;
+                    mbar_expect(&full[s], Sh::stage);
                     const int x = kb * kBK;
-                    tma_load_2d(stage, &a_hi, x, static_cast<int>(m0), &full[s]);
-                    tma_load_2d(stage + A_BYTES, &b_hi, x, static_cast<int>(n0), &full[s]);
-                    if constexpr (split) {
-                        tma_load_2d(stage + A_BYTES + B_BYTES, &a_lo, x, static_cast<int>(m0), &full[s]);
-                        tma_load_2d(stage + 2 * A_BYTES + B_BYTES, &b_lo, x, static_cast<int>(n0), &full[s]);
+#pragma unroll
+                    for (int q = 0; q < TERMS; ++q) {
+                        tma_load_2d(stage + q * Sh::a_bytes, &maps.a[q], x, static_cast<int>(m0), &full[s]);
+                        tma_load_2d(stage + TERMS * Sh::a_bytes + q * Sh::b_bytes, &maps.b[q], x, static_cast<int>(n0),
+                                    &full[s]);
                     }
                 }
             } else if (warp == 5 && lane == 0) {
@@ -208,17 +232,15 @@ namespace sci_cuda {
                         break;
                     }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    unsigned char *stage = ring + s * STAGE;
-                    const unsigned long long ah = smem_desc(stage), bh = smem_desc(stage + A_BYTES);
+                    unsigned char *stage = ring + s * Sh::stage;
 #pragma unroll
                     for (int kk = 0; kk < kBK / kUmmaK; ++kk) {
                         const unsigned long long step = (kk * kUmmaK * 2) >> 4;  // 32 bytes along K
-                        mma_bf16(tmem, ah + step, bh + step, (kb | kk) != 0);
-                        if constexpr (split) {
-                            const unsigned long long al = smem_desc(stage + A_BYTES + B_BYTES);
-                            const unsigned long long bl = smem_desc(stage + 2 * A_BYTES + B_BYTES);
-                            mma_bf16(tmem, ah + step, bl + step, 1);
-                            mma_bf16(tmem, al + step, bh + step, 1);
+#pragma unroll
+                        for (int p = 0; p < Pr::count; ++p) {
+                            const unsigned long long da = smem_desc(stage + product_a(p) * Sh::a_bytes) + step;
+                            const unsigned long long db = smem_desc(stage + TERMS * Sh::a_bytes + product_b(p) * Sh::b_bytes) + step;
+                            mma_bf16(tmem, da, db, Sh::instr, (kb | kk | p) != 0);
                         }
                     }
                     mma_commit(&empty[s]);  // frees the stage once these MMAs have read it
@@ -234,7 +256,7 @@ namespace sci_cuda {
                 if (ok) {
                     const unsigned long long row = m0 + warp * 32 + lane;
 #pragma unroll 1
-                    for (int chunk = 0; chunk < kBN / 32; ++chunk) {
+                    for (int chunk = 0; chunk < BN / 32; ++chunk) {
                         unsigned v[32];
                         const unsigned address = tmem + ((warp * 32u) << 16) + chunk * 32u;
                         asm volatile(
@@ -249,17 +271,23 @@ namespace sci_cuda {
                         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
                         const unsigned long long col = n0 + chunk * 32;
                         if (row < args.m) {
-                            float *dst = args.c + row * args.n + col;
-                            if (col + 32 <= args.n && (args.n % 4) == 0 &&
+                            float *dst = args.c + row * args.ldc + col;
+                            if (col + 32 <= args.n && (args.ldc % 4) == 0 &&
                                 (reinterpret_cast<unsigned long long>(args.c) % 16) == 0) {
 #pragma unroll
-                                for (int j = 0; j < 32; j += 4)
-                                    *reinterpret_cast<float4 *>(dst + j) = make_float4(
-                                            __uint_as_float(v[j]), __uint_as_float(v[j + 1]), __uint_as_float(v[j + 2]),
-                                            __uint_as_float(v[j + 3]));
+                                for (int j = 0; j < 32; j += 4) {
+                                    float4 out = make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]),
+                                                             __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
+                                    if (args.subtract) {
+                                        const float4 old = *reinterpret_cast<const float4 *>(dst + j);
+                                        out = make_float4(old.x - out.x, old.y - out.y, old.z - out.z, old.w - out.w);
+                                    }
+                                    *reinterpret_cast<float4 *>(dst + j) = out;
+                                }
                             } else {
                                 for (int j = 0; j < 32; ++j)
-                                    if (col + j < args.n) dst[j] = __uint_as_float(v[j]);
+                                    if (col + j < args.n)
+                                        dst[j] = args.subtract ? dst[j] - __uint_as_float(v[j]) : __uint_as_float(v[j]);
                             }
                         }
                     }
@@ -271,7 +299,7 @@ namespace sci_cuda {
             __syncthreads();
             if (warp == 0) {
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                tmem_free(tmem, kTmemColumns);
+                tmem_free(tmem, BN);
             }
         }
 
@@ -280,8 +308,10 @@ namespace sci_cuda {
         // memory. T = float accumulates in float, T = double in double (the reference's
         // multiply<type> accumulates in the element type, dispatch.cpp:171-224).
         template <typename T>
-        __global__ void __launch_bounds__(256) simt_product(const T *__restrict__ a, const T *__restrict__ b, T *__restrict__ c,
-                                                            unsigned long long m, unsigned long long n, unsigned long long k) {
+        __global__ void __launch_bounds__(256) simt_product(const T *__restrict__ a, unsigned long long lda,
+                                                            const T *__restrict__ b, unsigned long long ldb, T *__restrict__ c,
+                                                            unsigned long long ldc, unsigned long long m, unsigned long long n,
+                                                            unsigned long long k, int subtract) {
             constexpr int BM = 128, BN = 128, BK = 8, TM = 8, TN = 8;
             __shared__ T as[BK][BM + 4];
             __shared__ T bs[BK][BN + 4];
@@ -298,12 +328,12 @@ namespace sci_cuda {
                 for (int i = threadIdx.x; i < BM * BK; i += 256) {
                     const int r = i / BK, q = i % BK;
                     const unsigned long long gr = m0 + r, gk = k0 + q;
-                    as[q][r] = (gr < m && gk < k) ? a[gr * k + gk] : T(0);
+                    as[q][r] = (gr < m && gk < k) ? a[gr * lda + gk] : T(0);
                 }
                 for (int i = threadIdx.x; i < BK * BN; i += 256) {
                     const int q = i / BN, col = i % BN;
                     const unsigned long long gk = k0 + q, gc = n0 + col;
-                    bs[q][col] = (gk < k && gc < n) ? b[gk * n + gc] : T(0);
+                    bs[q][col] = (gk < k && gc < n) ? b[gk * ldb + gc] : T(0);
                 }
                 __syncthreads();
 #pragma unroll
@@ -327,7 +357,7 @@ namespace sci_cuda {
 #pragma unroll
                 for (int j = 0; j < TN; ++j) {
                     const unsigned long long col = n0 + tx * TN + j;
-                    if (col < n) c[r * n + col] = acc[i][j];
+                    if (col < n) c[r * ldc + col] = subtract ? c[r * ldc + col] - acc[i][j] : acc[i][j];
                 }
             }
         }
@@ -363,60 +393,69 @@ namespace sci_cuda {
                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
         }
 
-        int tensor_path(Context &ctx, bool split, const float *a, const float *b, float *c, unsigned long long m,
-                        unsigned long long n, unsigned long long k) {
-            const unsigned long long kp = (k + kBK - 1) / kBK * kBK;
-            if (kp > (1ull << 31) || m > (1ull << 31) || n > (1ull << 31))
-                return ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "product dimensions beyond 2^31");
-            const unsigned long long a_bytes = m * kp * 2, b_bytes = n * kp * 2;
-            const unsigned long long need = (split ? 2 : 1) * (a_bytes + b_bytes) + 1024;
-            if (int code = ctx.check(ctx.workspace->reserve(need), "reserving the product workspace")) return code;
-            auto *base = static_cast<unsigned char *>(ctx.workspace->memory);
-            auto *a_hi = reinterpret_cast<__nv_bfloat16 *>(base);
-            auto *b_hi = reinterpret_cast<__nv_bfloat16 *>(base + a_bytes);
-            __nv_bfloat16 *a_lo = split ? reinterpret_cast<__nv_bfloat16 *>(base + a_bytes + b_bytes) : nullptr;
-            __nv_bfloat16 *b_lo = split ? reinterpret_cast<__nv_bfloat16 *>(base + 2 * a_bytes + b_bytes) : nullptr;
-
-            const unsigned grid = static_cast<unsigned>(std::min<unsigned long long>((m * kp + 255) / 256, ctx.sms * 16ull));
-            split_rows<<<grid, 256, 0, ctx.stream>>>(a, a_hi, a_lo, m, k, kp);
-            const dim3 tgrid(static_cast<unsigned>((n + 31) / 32), static_cast<unsigned>((kp + 31) / 32));
-            split_transpose<<<tgrid, dim3(32, 8), 0, ctx.stream>>>(b, b_hi, b_lo, k, n, kp);
-            if (int code = ctx.check(cudaGetLastError(), "launching the bf16 conversion")) return code;
-
-            CUtensorMap maps[4];
-            std::memset(maps, 0, sizeof(maps));
-            if (!make_map(&maps[0], a_hi, m, kp, kBM) || !make_map(&maps[2], b_hi, n, kp, kBN))
-                return ctx.fail(SCI_CUDA_ERROR_LAUNCH, "cuTensorMapEncodeTiled failed");
-            if (split && (!make_map(&maps[1], a_lo, m, kp, kBM) || !make_map(&maps[3], b_lo, n, kp, kBN)))
-                return ctx.fail(SCI_CUDA_ERROR_LAUNCH, "cuTensorMapEncodeTiled failed");
-            if (!split) {
-                maps[1] = maps[0];
-                maps[3] = maps[2];
-            }
-            const int stages = split ? kStagesSplit : kStagesPlain;
-            const unsigned stage_bytes = (split ? 2u : 1u) * (kBM * kBK * 2 + kBN * kBK * 2);
-            const size_t smem = static_cast<size_t>(stages) * stage_bytes + 1024;
-            const void *kernel = split ? reinterpret_cast<const void *>(&tensor_product<true>)
-                                       : reinterpret_cast<const void *>(&tensor_product<false>);
-            if (int code = ctx.check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
-                                     "raising the product kernel's shared memory"))
-                return code;
-            ProductArgs args{c, m, n, kp, ctx.status};
-            void *params[] = {&maps[0], &maps[1], &maps[2], &maps[3], &args};
-            const dim3 pgrid(static_cast<unsigned>((n + kBN - 1) / kBN), static_cast<unsigned>((m + kBM - 1) / kBM));
-            return ctx.check(cudaLaunchKernel(kernel, pgrid, dim3(192), params, smem, ctx.stream), "launching the tensor product");
-        }
-
-        template <typename T>
-        int simt_path(Context &ctx, const T *a, const T *b, T *c, unsigned long long m, unsigned long long n,
-                      unsigned long long k) {
-            const dim3 grid(static_cast<unsigned>((n + 127) / 128), static_cast<unsigned>((m + 127) / 128));
-            if (grid.y > 65535) return ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "too many rows for one launch");
-            simt_product<T><<<grid, 256, 0, ctx.stream>>>(a, b, c, m, n, k);
-            return ctx.check(cudaGetLastError(), "launching the SIMT product");
-        }
-
     } // namespace
+
+    // C (m x n, row pitch ldc) = or -= A (m x k, pitch lda) * B (k x n, pitch ldb) on the tensor cores, each
+    // operand split into `terms` bf16 parts (1, 2 or 3).
+    int tensor_gemm(Context &ctx, int terms, const float *a, unsigned long long lda, const float *b,
+                    unsigned long long ldb, float *c, unsigned long long ldc, unsigned long long m, unsigned long long n,
+                    unsigned long long k, bool subtract) {
+        if (terms < 1 || terms > 3) return ctx.fail(SCI_CUDA_ERROR_INVALID, "bf16 terms %d", terms);
+        const unsigned long long kp = (k + kBK - 1) / kBK * kBK;
+        if (kp > (1ull << 31) || m > (1ull << 31) || n > (1ull << 31))
+            return ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "product dimensions beyond 2^31");
+        const unsigned long long a_bytes = (m * kp * 2 + 1023) / 1024 * 1024, b_bytes = (n * kp * 2 + 1023) / 1024 * 1024;
+        const unsigned long long need = terms * (a_bytes + b_bytes) + 1024;
+        if (int code = ctx.check(ctx.workspace->reserve(need), "reserving the product workspace")) return code;
+        auto *base = static_cast<unsigned char *>(ctx.workspace->memory);
+        Terms at{}, bt{};
+        for (int q = 0; q < terms; ++q) {
+            at.t[q] = reinterpret_cast<__nv_bfloat16 *>(base + q * a_bytes);
+            bt.t[q] = reinterpret_cast<__nv_bfloat16 *>(base + terms * a_bytes + q * b_bytes);
+        }
+        const unsigned grid = static_cast<unsigned>(std::min<unsigned long long>((m * kp + 255) / 256, ctx.sms * 16ull));
+        split_rows<<<grid, 256, 0, ctx.stream>>>(a, lda, at, terms, m, k, kp);
+        const dim3 tgrid(static_cast<unsigned>((n + 31) / 32), static_cast<unsigned>((kp + 31) / 32));
+        split_transpose<<<tgrid, dim3(32, 8), 0, ctx.stream>>>(b, ldb, bt, terms, k, n, kp);
+        if (int code = ctx.check(cudaGetLastError(), "launching the bf16 conversion")) return code;
+
+        const unsigned bn = terms == 3 ? 128u : 256u;
+        Maps maps;
+        std::memset(&maps, 0, sizeof(maps));
+        for (int q = 0; q < terms; ++q) {
+            if (!make_map(&maps.a[q], at.t[q], m, kp, kBM) || !make_map(&maps.b[q], bt.t[q], n, kp, bn))
+                return ctx.fail(SCI_CUDA_ERROR_LAUNCH, "cuTensorMapEncodeTiled failed");
+        }
+        const void *kernel = terms == 1 ? reinterpret_cast<const void *>(&tensor_product<1>)
+                           : terms == 2 ? reinterpret_cast<const void *>(&tensor_product<2>)
+                                        : reinterpret_cast<const void *>(&tensor_product<3>);
+        const size_t smem = terms == 1 ? Shape<1>::stages * Shape<1>::stage + 1024
+                          : terms == 2 ? Shape<2>::stages * Shape<2>::stage + 1024
+                                       : Shape<3>::stages * Shape<3>::stage + 1024;
+        if (int code = ctx.check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                                 "raising the product kernel's shared memory"))
+            return code;
+        ProductArgs args{c, m, n, kp, ldc, subtract ? 1 : 0, ctx.status};
+        void *params[] = {&maps, &args};
+        const dim3 pgrid(static_cast<unsigned>((n + bn - 1) / bn), static_cast<unsigned>((m + kBM - 1) / kBM));
+        return ctx.check(cudaLaunchKernel(kernel, pgrid, dim3(192), params, smem, ctx.stream), "launching the tensor product");
+    }
+
+    // C (pitch ldc) = or -= A (pitch lda) * B (pitch ldb) with the plain SIMT kernel.
+    template <typename T>
+    int simt_gemm(Context &ctx, const T *a, unsigned long long lda, const T *b, unsigned long long ldb, T *c,
+                  unsigned long long ldc, unsigned long long m, unsigned long long n, unsigned long long k, bool subtract) {
+        const dim3 grid(static_cast<unsigned>((n + 127) / 128), static_cast<unsigned>((m + 127) / 128));
+        if (grid.y > 65535) return ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "too many rows for one launch");
+        if (m == 0 || n == 0) return SCI_CUDA_OK;
+        simt_product<T><<<grid, 256, 0, ctx.stream>>>(a, lda, b, ldb, c, ldc, m, n, k, subtract ? 1 : 0);
+        return ctx.check(cudaGetLastError(), "launching the SIMT product");
+    }
+    template int simt_gemm<float>(Context &, const float *, unsigned long long, const float *, unsigned long long, float *,
+                                  unsigned long long, unsigned long long, unsigned long long, unsigned long long, bool);
+    template int simt_gemm<double>(Context &, const double *, unsigned long long, const double *, unsigned long long,
+                                   double *, unsigned long long, unsigned long long, unsigned long long, unsigned long long,
+                                   bool);
 
 } // namespace sci_cuda
 
@@ -426,7 +465,7 @@ extern "C" int sci_cuda_product(sci_cuda_context *context, uint32_t precision, u
                                 const void *right, void *output, uint64_t rows, uint64_t columns, uint64_t depth) {
     if (!context) return SCI_CUDA_ERROR_INVALID;
     std::lock_guard<std::recursive_mutex> lock(context->guard);
-    if (precision > SCI_PRECISION_WIDE || mode > SCI_PRODUCT_FP32)
+    if (precision > SCI_PRECISION_WIDE || mode > SCI_PRODUCT_SPLIT3_BF16)
         return context->fail(SCI_CUDA_ERROR_INVALID, "unknown precision %u or mode %u", precision, mode);
     if (rows == 0 || columns == 0) return SCI_CUDA_OK;
     if (!left || !right || !output) return context->fail(SCI_CUDA_ERROR_INVALID, "null matrix");
@@ -436,13 +475,15 @@ extern "C" int sci_cuda_product(sci_cuda_context *context, uint32_t precision, u
         return context->check(cudaMemsetAsync(output, 0, rows * columns * element, context->stream), "zeroing the product");
     }
     if (precision == SCI_PRECISION_WIDE) {
-        return simt_path<double>(*context, static_cast<const double *>(left), static_cast<const double *>(right),
-                                 static_cast<double *>(output), rows, columns, depth);
+        return simt_gemm<double>(*context, static_cast<const double *>(left), depth, static_cast<const double *>(right),
+                                 columns, static_cast<double *>(output), columns, rows, columns, depth, false);
     }
     if (mode == SCI_PRODUCT_FP32) {
-        return simt_path<float>(*context, static_cast<const float *>(left), static_cast<const float *>(right),
-                                static_cast<float *>(output), rows, columns, depth);
+        return simt_gemm<float>(*context, static_cast<const float *>(left), depth, static_cast<const float *>(right),
+                                columns, static_cast<float *>(output), columns, rows, columns, depth, false);
     }
-    return tensor_path(*context, mode == SCI_PRODUCT_SPLIT_BF16, static_cast<const float *>(left),
-                       static_cast<const float *>(right), static_cast<float *>(output), rows, columns, depth);
+    return tensor_gemm(*context, mode == SCI_PRODUCT_SPLIT3_BF16 ? 3 : (mode == SCI_PRODUCT_SPLIT_BF16 ? 2 : 1),
+                       static_cast<const float *>(left), depth,
+                       static_cast<const float *>(right), columns, static_cast<float *>(output), columns, rows, columns,
+                       depth, false);
 }

@@ -106,6 +106,28 @@ class Device:
                                    depth), self.handle)
         return out
 
+    def factor(self, matrix: "DeviceArray", order: int, plain: bool = False) -> np.ndarray:
+        """linear::factor (decompose.hpp:29-72) in place; returns rows[] (original row at each position)."""
+        rows = np.zeros(order, np.uint64)
+        precision = C.WIDE if matrix.dtype == np.float64 else C.SINGLE
+        check(lib.sci_cuda_factor(self.handle, precision, 1 if plain else 0, matrix.pointer, rows.ctypes.data, order),
+              self.handle)
+        return rows
+
+    def solve(self, matrix: "DeviceArray", right: "DeviceArray", order: int, width: int, refine: bool = False,
+              out: "DeviceArray | None" = None):
+        """linear::solve (solve.hpp:60-76). refine=True: FP32 LU plus FP64 refinement (double operands).
+        Returns (solution, backward_error, iterations)."""
+        from .native import SolveReport
+
+        if out is None:
+            out = self.empty(order * width, right.dtype)
+        precision = C.WIDE if matrix.dtype == np.float64 else C.SINGLE
+        report = SolveReport()
+        check(lib.sci_cuda_solve(self.handle, precision, 1 if refine else 0, matrix.pointer, right.pointer, out.pointer,
+                                 order, width, ctypes.byref(report)), self.handle)
+        return out, report.backward_error, report.iterations
+
     def evaluate(self, expression, out: "DeviceArray | None" = None) -> "DeviceArray":
         """assign(target, expression) (expression.hpp:158-185); allocates the target if needed."""
         expr = C._operand(expression, None)

@@ -28,6 +28,12 @@ class SciCudaError(RuntimeError):
         self.status = status
 
 
+class SolveReport(ctypes.Structure):
+    """sci_solve_report (include/sci_cuda.h)."""
+
+    _fields_ = [("backward_error", ctypes.c_double), ("iterations", ctypes.c_int)]
+
+
 def _load() -> ctypes.CDLL:
     if not LIBRARY.exists():
         raise ImportError(f"{LIBRARY} is not built; run `python -m libsci_b200.build` (needs nvcc)")
@@ -53,7 +59,11 @@ def _load() -> ctypes.CDLL:
                                             ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
     }
     optional = {}
-    for name, (res, args) in sig.items():
+    sig["sci_cuda_factor"] = (ctypes.c_int, [c_ctx, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                             ctypes.c_uint64])
+    sig["sci_cuda_solve"] = (ctypes.c_int, [c_ctx, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, P(SolveReport)])
+    for name, (res, args) in list(sig.items()):
         fn = getattr(lib, name)
         fn.restype, fn.argtypes = res, args
     for name, (res, args) in optional.items():

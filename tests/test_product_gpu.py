@@ -4,6 +4,7 @@ Bounds, with S = |A| @ |B| (elementwise absolute values) and k the depth:
 - FP32 SIMT: |C - C64| <= k 2^-23 S (k roundings of a float accumulator);
 - BF16 tensor cores: <= (2^-7 + k 2^-22) S (each operand rounded to 8 bits);
 - split BF16: <= (2^-14 + k 2^-22) S (hi + lo keeps about 16 bits per operand; lo*lo dropped);
+- three-term split BF16: <= (2^-21 + k 2^-22) S (hi + mid + lo, six products);
 - FP64: <= k 2^-51 S.
 The reference pins its product at 37 x 53 x 29 with patterned values within 1e-3 of a double
 loop (tests/linear/test_product.cpp:8-33); that case is exact in every mode here.
@@ -15,14 +16,15 @@ from tests import _oracle
 
 pytestmark = pytest.mark.gpu
 
-BF16, SPLIT, FP32 = 0, 1, 2
-NAMES = {BF16: "bf16", SPLIT: "split_bf16", FP32: "fp32"}
+BF16, SPLIT, FP32, SPLIT3 = 0, 1, 2, 3
+NAMES = {BF16: "bf16", SPLIT: "split_bf16", FP32: "fp32", SPLIT3: "split3_bf16"}
 
 
 def bound(mode, k, s, wide=False):
     if wide:
         return k * 2.0 ** -51 * s + 1e-300
-    return {FP32: k * 2.0 ** -23, BF16: 2.0 ** -7 + k * 2.0 ** -22, SPLIT: 2.0 ** -14 + k * 2.0 ** -22}[mode] * s + 1e-30
+    return {FP32: k * 2.0 ** -23, BF16: 2.0 ** -7 + k * 2.0 ** -22, SPLIT: 2.0 ** -14 + k * 2.0 ** -22,
+            SPLIT3: 2.0 ** -21 + k * 2.0 ** -22}[mode] * s + 1e-30
 
 
 def run(device, a, b, mode):
@@ -33,7 +35,7 @@ def run(device, a, b, mode):
     return out.numpy().reshape(m, n)
 
 
-@pytest.mark.parametrize("mode", [BF16, SPLIT, FP32], ids=NAMES.get)
+@pytest.mark.parametrize("mode", [BF16, SPLIT, SPLIT3, FP32], ids=NAMES.get)
 def test_reference_pin(device, mode):
     rows, inner, columns = 37, 53, 29
     left = np.fromfunction(lambda r, c: ((r * 7 + c * 3) % 11) - 5.0, (rows, inner)).astype(np.float32)
@@ -45,7 +47,7 @@ def test_reference_pin(device, mode):
 
 @pytest.mark.parametrize("shape", [(128, 256, 64), (129, 257, 70), (300, 500, 200), (64, 8, 1000), (1024, 1024, 1024),
                                    (1, 1, 1), (700, 9, 3)])
-@pytest.mark.parametrize("mode", [BF16, SPLIT, FP32], ids=NAMES.get)
+@pytest.mark.parametrize("mode", [BF16, SPLIT, SPLIT3, FP32], ids=NAMES.get)
 def test_product_against_fp64(device, mode, shape):
     m, n, k = shape
     rng = np.random.default_rng(m * 7 + n * 3 + k)
