@@ -197,7 +197,7 @@ def run_product(args) -> int:
     for i, r in enumerate(sample_rows):
         oracle.sci_oracle_product_rows(a.ctypes.data, b.ctypes.data, want[i].ctypes.data, size, size, size, int(r), int(r) + 1)
     modes = {}
-    for mode, name in ((0, "bf16"), (1, "split_bf16"), (2, "fp32")):
+    for mode, name in ((0, "bf16"), (1, "split_bf16"), (3, "split3_bf16"), (2, "fp32")):
         for _ in range(args.warmup):
             device.product(da, db, size, size, size, mode=mode, out=dc)
         device.synchronize()
@@ -212,7 +212,7 @@ def run_product(args) -> int:
         got = dc.numpy().reshape(size, size)[sample_rows]
         err = np.abs(got - want)
         modes[name] = {"ms": ms, "TFLOP/s": flops / (ms * 1e-3) / 1e12, "frac_of_bf16_peak": flops / (ms * 1e-3) / 1e12 / peak,
-                       "tensor_TFLOP/s": (3 if mode == 1 else 1) * flops / (ms * 1e-3) / 1e12 if mode != 2 else None,
+                       "tensor_TFLOP/s": {0: 1, 1: 3, 3: 6}.get(mode, 0) * flops / (ms * 1e-3) / 1e12 if mode != 2 else None,
                        "max_abs_err": float(err.max()), "rel_fro_err": float(np.linalg.norm(err) / np.linalg.norm(want))}
     cpu = None
     ref = _oracle.reference()
@@ -234,10 +234,33 @@ def run_product(args) -> int:
             "modes": modes,
             "roofline": {"bound": "tensor", "achieved": best["TFLOP/s"], "peak": peak, "unit": "TFLOP/s",
                          "frac": best["TFLOP/s"] / peak, "traffic": None, "peak_source": "measured bf16_tflops (burst)"},
-            "cpu_baseline": cpu, "gpu_launches": 3 * args.steps}
+            "cpu_baseline": cpu, "gpu_launches": 3 * args.steps}  # per bf16 product: two conversions + one GEMM
     print(json.dumps(line))
     device.close()
     return 0
+
+
+def torch_solve(torch, a, b, args):
+    """An external sanity point, not a product path: torch.linalg.solve in FP64 on the same GPU
+    (cuSOLVER getrf + getrs), timed with events, with its normwise backward error."""
+    ta, tb = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+    for _ in range(args.warmup):
+        torch.linalg.solve(ta, tb)
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.steps):
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        x = torch.linalg.solve(ta, tb)
+        stop.record()
+        stop.synchronize()
+        times.append(start.elapsed_time(stop))
+    x = x.cpu().numpy()
+    r = np.abs(b - a @ x).max(axis=0)
+    berr = r / (np.abs(a).sum(axis=1).max() * np.abs(x).max(axis=0) + np.abs(b).max(axis=0))
+    del ta, tb
+    torch.cuda.empty_cache()
+    return {"ms": statistics.median(times), "backward_error": float(berr.max())}
 
 
 def run_solve(args) -> int:
@@ -261,7 +284,8 @@ def run_solve(args) -> int:
         da, db, dx = device.array(a.ravel()), device.array(b.ravel()), device.empty(n * width, np.float64)
         result = {}
         for label, refine in (("fp32_lu_fp64_refine", True), ("fp64_lu", False)):
-            device.solve(da, db, n, width, refine=refine, out=dx)  # warm-up (workspaces, module loads)
+            for _ in range(args.warmup):  # workspaces, module loads
+                device.solve(da, db, n, width, refine=refine, out=dx)
             times, berr, iterations = [], None, None
             for _ in range(args.steps):
                 start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -274,6 +298,7 @@ def run_solve(args) -> int:
             result[label] = {"ms": ms, "GFLOP/s": flops / (ms * 1e-3) / 1e9, "backward_error": berr,
                              "iterations": iterations}
         result["speedup_refined_vs_fp64"] = result["fp64_lu"]["ms"] / result["fp32_lu_fp64_refine"]["ms"]
+        result["external_torch_linalg_solve_fp64"] = torch_solve(torch, a, b, args)
         cases[name] = result
         for arr in (da, db, dx):
             arr.free()
@@ -293,7 +318,7 @@ def run_solve(args) -> int:
                "sample": "libsci solve<double> (factor + substitute) at n=2048, 16 RHS, timed once"}
     headline = cases["G+nI"]["fp32_lu_fp64_refine"]
     line = {"metric": "solve speedup vs plain FP64 LU at equal backward error", "value": cases["G+nI"]["speedup_refined_vs_fp64"],
-            "unit": "x", "n_gpus": 1, "steps": args.steps, "warmup": 1, "ms_per_step": headline["ms"],
+            "unit": "x", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": headline["ms"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 LU + f64 refinement",
             "data": "synthetic", "config": {"workload": f"solve n={n}, 16 RHS ~ N(0,1); A=G+nI and A=G"},
             "cases": cases, "cpu_baseline": cpu}

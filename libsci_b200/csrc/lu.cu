@@ -10,9 +10,9 @@
 //    for each narrow panel of W columns (W = 32 float, 16 double) inside it:
 //      1. panel_factor: one 8-CTA thread-block cluster, 1024 threads per CTA, one panel row per
 //         thread held in registers (so up to 8192 rows). Per column: a warp-shuffle argmax, a block
-//         argmax in shared memory, then one cluster barrier after which the 8 CTA candidates, the
-//         winner's row and the displaced row are read through distributed shared memory; then every
-//         thread eliminates its own row.
+//         argmax in shared memory, then one cluster barrier after which one warp per CTA reads the
+//         8 CTA candidates, the winner's row and the displaced row through distributed shared
+//         memory; then every thread eliminates its own row.
 //      2. move_rows: the panel's net row movement applied to every other column (one gather).
 //      3. trsm_rows + rank_update: U rows of the panel and the rows below it, inside the block.
 //    after the block: its U rows for the columns beyond it (trsm_rows + rank_update per panel, once
@@ -39,8 +39,8 @@ namespace sci_cuda {
     namespace {
 
         constexpr int kClusterCtas = 8;
-        constexpr int kPanelThreads = 1024;
-        constexpr unsigned long long kPanelRows = 1ull * kClusterCtas * kPanelThreads;
+        constexpr int kCtaRows = 1024;
+        constexpr unsigned long long kPanelRows = 1ull * kClusterCtas * kCtaRows;
         constexpr unsigned long long kOuter = 256;
         constexpr int kSolveBlock = 128;
 
@@ -104,109 +104,274 @@ namespace sci_cuda {
             long long src[64];
         };
 
+        constexpr int kRowsPerThread = 2;
+        constexpr int kPanelBlock = kCtaRows / kRowsPerThread;  // threads per panel CTA
+        // Dynamic shared memory of panel_factor: the staged multipliers, W x (1024 + 1).
+        template <typename T> constexpr size_t panel_shared_bytes() {
+            return sizeof(T) * PanelWidth<T>::value * (kCtaRows + 1);
+        }
+
+        __device__ __forceinline__ void named_sync(unsigned id, unsigned count) {
+            asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+        }
+        __device__ __forceinline__ void named_arrive(unsigned id, unsigned count) {
+            asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
+        }
+        // W values (128 bytes) from a 16-byte aligned address.
+        __device__ __forceinline__ void load_row(const float *p, float *v) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const float4 x = reinterpret_cast<const float4 *>(p)[q];
+                v[4 * q] = x.x;
+                v[4 * q + 1] = x.y;
+                v[4 * q + 2] = x.z;
+                v[4 * q + 3] = x.w;
+            }
+        }
+        __device__ __forceinline__ void load_row(const double *p, double *v) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const double2 x = reinterpret_cast<const double2 *>(p)[q];
+                v[2 * q] = x.x;
+                v[2 * q + 1] = x.y;
+            }
+        }
+
         // Factors columns [j0, j0 + width) of rows [j0, n) in place; piv[j0 + j] = the row swapped into
         // position j0 + j, and *moved = the net movement of the panel's exchanges. One cluster of 8
-        // CTAs; thread t of CTA c owns row j0 + 1024 c + t, its panel values in registers.
+        // CTAs of 512 threads, 1024 rows per CTA: thread t of CTA c holds rows j0 + 1024 c + t and
+        // j0 + 1024 c + 512 + t, their panel values in registers, shifted left one column per step so
+        // the current column is always v[i][0] (the column loop stays rolled: unrolled, every column
+        // ran cold out of the instruction cache).
         //
-        // Per column, one cluster barrier: before it, each CTA publishes its best candidate (|value|,
-        // row, and the candidate row's values), and CTA 0 publishes the row at the pivot position;
-        // after it, every CTA reads the 8 candidates, the winner's row and (the pivot row's owner) the
-        // displaced row through distributed shared memory. Publication buffers alternate by column
-        // parity, so a buffer is rewritten only after a later barrier every reader has passed.
+        // Each finished value belongs to the row's original position (`origin`). A multiplier of L
+        // whose row is still at its origin is staged in shared memory and written out coalesced at
+        // the end; one of a row the exchanges moved, and each pivot row of U, goes to global memory
+        // at once. A final permutation moves the at most 2 W displaced rows to their positions.
+        //
+        // Per column: each warp's best row is published in shared memory; warp 0 alone waits for
+        // them (a named barrier the other warps only arrive at) and publishes the CTA's candidate
+        // with its values; one cluster barrier; warp 0 of every CTA then reads all 8 candidates, their
+        // rows and the row at the pivot position in one round of distributed shared-memory loads,
+        // picks the pivot, and one CTA barrier hands it to every thread. Buffers read across the
+        // cluster alternate by column parity, so one is rewritten only after a later cluster barrier
+        // every reader has passed.
         template <typename T>
-        __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kPanelThreads, 1)
+        __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kPanelBlock, 1)
                 panel_factor(T *a, unsigned long long n, unsigned long long j0, int width, long long *piv, Movement *moved) {
-            constexpr int W = PanelWidth<T>::value;
-            __shared__ T warp_mag[32];
-            __shared__ unsigned long long warp_row[32];
+            constexpr int W = PanelWidth<T>::value, R = kRowsPerThread, TH = kPanelBlock, WARPS = TH / 32;
+            constexpr int P = kCtaRows + 1;  // pitch of the staged multipliers
+            extern __shared__ __align__(16) unsigned char panel_shared[];
+            T *stage = reinterpret_cast<T *>(panel_shared);  // stage[k * P + local row]
+            __shared__ unsigned home[kCtaRows];          // bit k: stage holds column k of the row
+            __shared__ T warp_mag[WARPS];
+            __shared__ unsigned long long warp_row[WARPS], warp_origin[WARPS];
+            __shared__ __align__(16) T warp_values[WARPS][W];
             __shared__ T cand_mag[2];
-            __shared__ unsigned long long cand_row[2];
-            __shared__ T cand_values[2][W];  // the CTA winner's row
-            __shared__ T jbuf[2][W];         // CTA 0: the row at the pivot position
-            __shared__ T pivot_row[W];
-            __shared__ unsigned long long winner;
+            __shared__ unsigned long long cand_row[2], cand_origin[2];
+            __shared__ __align__(16) T cand_values[2][W];
+            __shared__ __align__(16) T jbuf[2][W];  // CTA 0: the row at the pivot position
+            __shared__ unsigned long long jbuf_origin[2];
+            __shared__ __align__(16) T pivot_row[W];
+            __shared__ __align__(16) T displaced[W];
+            __shared__ unsigned long long pivot_at, pivot_origin, displaced_origin;
+            __shared__ long long exchanges[W];  // CTA 0: piv[j0 + j]
 
             const unsigned c = cluster_rank(), t = threadIdx.x, lane = t % 32, warp = t / 32;
-            const unsigned long long r = j0 + 1ull * c * kPanelThreads + t;
-            const bool valid = r < n;
-            T v[W];
+            const unsigned long long first = j0 + 1ull * c * kCtaRows;  // this CTA's first row
+            unsigned long long r[R], origin[R];
+            bool valid[R];
+            unsigned mask[R];
+            T v[R][W];  // at step j: v[i][p] = column j0 + j + p of row i
+            const bool vector = width == W && (n * sizeof(T)) % 16 == 0;
 #pragma unroll
-            for (int k = 0; k < W; ++k) v[k] = (valid && k < width) ? a[r * n + j0 + k] : T(0);
-
+            for (int i = 0; i < R; ++i) {
+                r[i] = first + 1ull * i * TH + t;
+                valid[i] = r[i] < n;
+                origin[i] = r[i];
+                mask[i] = 0;
+                if (valid[i] && vector) {
+                    load_row(a + r[i] * n + j0, v[i]);
+                } else {
 #pragma unroll
-            for (int j = 0; j < W; ++j) {
-                if (j < width) {
-                    const int par = j & 1;
-                    const unsigned long long row_j = j0 + j;
-                    // 1. this row's candidacy; a NaN only stands at the pivot position itself, where the
-                    //    reference's comparisons against it all fail (decompose.hpp:35-38).
-                    T mag = T(-1);
-                    if (valid && r >= row_j) {
-                        const T m = fabs(v[j]);
-                        mag = (m == m) ? m : (r == row_j ? T(INFINITY) : T(-1));
-                    }
-                    unsigned long long mrow = r;
-                    warp_argmax(mag, mrow);
-                    if (lane == 0) {
-                        warp_mag[warp] = mag;
-                        warp_row[warp] = mrow;
-                    }
-                    if (c == 0 && t == static_cast<unsigned>(j)) {
-#pragma unroll
-                        for (int k = 0; k < W; ++k) jbuf[par][k] = v[k];
-                    }
-                    __syncthreads();
-                    if (warp == 0) {
-                        T m2 = warp_mag[lane];
-                        unsigned long long r2 = warp_row[lane];
-                        warp_argmax(m2, r2);
-                        if (lane == 0) {
-                            cand_mag[par] = m2;
-                            cand_row[par] = r2;
-                            winner = r2;
-                        }
-                    }
-                    __syncthreads();
-                    if (r == winner) {
-#pragma unroll
-                        for (int k = 0; k < W; ++k) cand_values[par][k] = v[k];
-                    }
-                    cluster_sync();  // the candidates and the pivot-position row are published
-                    // 2. the cluster's pivot, computed identically by every warp
-                    T pm = T(-1);
-                    unsigned long long prow = ~0ull;
-                    if (lane < kClusterCtas) {
-                        pm = load_remote(remote(&cand_mag[par], lane), T(0));
-                        prow = load_remote_u64(remote(&cand_row[par], lane));
-                    }
-                    warp_argmax(pm, prow);
-                    if (pm < T(0)) prow = row_j;  // no candidate (cannot happen for a valid pivot row)
-                    const unsigned prank = static_cast<unsigned>((prow - j0) / kPanelThreads);
-                    if (warp == 0 && lane < W) pivot_row[lane] = load_remote(remote(&cand_values[par][lane], prank), T(0));
-                    if (r == prow && prow != row_j) {
-                        // this row moves to the pivot's old place: it takes the displaced row's values
-#pragma unroll
-                        for (int k = 0; k < W; ++k) v[k] = load_remote(remote(&jbuf[par][k], 0), T(0));
-                    }
-                    __syncthreads();
-                    if (r == row_j) {
-#pragma unroll
-                        for (int k = 0; k < W; ++k) v[k] = pivot_row[k];
-                    }
-                    if (c == 0 && t == 0) piv[row_j] = static_cast<long long>(prow);
-                    // 3. eliminate below the pivot: l = a / pivot; a[k] -= l * pivot_row[k]
-                    const T diagonal = pivot_row[j];
-                    if (diagonal != T(0) && valid && r > row_j) {
-                        const T l = div(v[j], diagonal);
-                        v[j] = l;
-#pragma unroll
-                        for (int k = j + 1; k < W; ++k) v[k] = sub(v[k], mul(l, pivot_row[k]));
-                    }
+                    for (int k = 0; k < W; ++k) v[i][k] = (valid[i] && k < width) ? a[r[i] * n + j0 + k] : T(0);
                 }
             }
+
+#pragma unroll 1
+            for (int j = 0; j < width; ++j) {
+                const int par = j & 1;
+                const unsigned long long row_j = j0 + j;
+                // 1. candidacy; a NaN only stands at the pivot position itself, where the reference's
+                //    comparisons against it all fail (decompose.hpp:35-38).
+                T best = T(-1);
+                unsigned long long brow = r[0];
 #pragma unroll
-            for (int k = 0; k < W; ++k)
-                if (valid && k < width) a[r * n + j0 + k] = v[k];
+                for (int i = 0; i < R; ++i) {
+                    T mag = T(-1);
+                    if (valid[i] && r[i] >= row_j) {
+                        const T m = fabs(v[i][0]);
+                        mag = (m == m) ? m : (r[i] == row_j ? T(INFINITY) : T(-1));
+                    }
+                    if (better(mag, r[i], best, brow)) {
+                        best = mag;
+                        brow = r[i];
+                    }
+                }
+                warp_argmax(best, brow);
+                if (lane == 0) {
+                    warp_mag[warp] = best;
+                    warp_row[warp] = brow;
+                }
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+                    if (r[i] == brow) {
+#pragma unroll
+                        for (int k = 0; k < W; ++k) warp_values[warp][k] = v[i][k];
+                        warp_origin[warp] = origin[i];
+                    }
+                }
+                if (c == 0 && t == static_cast<unsigned>(j)) {  // row_j is row 0 of thread j in CTA 0
+#pragma unroll
+                    for (int k = 0; k < W; ++k) jbuf[par][k] = v[0][k];
+                    jbuf_origin[par] = origin[0];
+                }
+                if (warp == 0) {
+                    named_sync(1, TH);
+                    T m2 = lane < WARPS ? warp_mag[lane] : T(-1);
+                    unsigned long long r2 = lane < WARPS ? warp_row[lane] : ~0ull;
+                    warp_argmax(m2, r2);
+                    const unsigned source = static_cast<unsigned>((r2 - first) % TH) / 32;
+                    if (lane < W) cand_values[par][lane] = warp_values[source][lane];
+                    if (lane == 0) {
+                        cand_mag[par] = m2;
+                        cand_row[par] = r2;
+                        cand_origin[par] = warp_origin[source];
+                    }
+                } else {
+                    named_arrive(1, TH);
+                }
+                cluster_sync();  // the candidates and the pivot-position row are published
+                // 2. the pivot: warp 0 of every CTA reads all candidates in one round of loads
+                if (warp == 0) {
+                    T m = T(-1);
+                    unsigned long long row = ~0ull, org = 0;
+                    if (lane < kClusterCtas) {
+                        m = load_remote(remote(&cand_mag[par], lane), T(0));
+                        row = load_remote_u64(remote(&cand_row[par], lane));
+                        org = load_remote_u64(remote(&cand_origin[par], lane));
+                    }
+                    T values[kClusterCtas];
+#pragma unroll
+                    for (int q = 0; q < kClusterCtas; ++q)
+                        values[q] = lane < W ? load_remote(remote(&cand_values[par][lane], q), T(0)) : T(0);
+                    const T there = lane < W ? load_remote(remote(&jbuf[par][lane], 0), T(0)) : T(0);
+                    const unsigned long long there_origin = load_remote_u64(remote(&jbuf_origin[par], 0));
+                    unsigned q = lane;
+#pragma unroll
+                    for (int offset = kClusterCtas / 2; offset > 0; offset >>= 1) {
+                        const T om = __shfl_xor_sync(0xffffffffu, m, offset);
+                        const unsigned long long orow = __shfl_xor_sync(0xffffffffu, row, offset);
+                        const unsigned long long oorg = __shfl_xor_sync(0xffffffffu, org, offset);
+                        const unsigned oq = __shfl_xor_sync(0xffffffffu, q, offset);
+                        if (better(om, orow, m, row)) {
+                            m = om;
+                            row = orow;
+                            org = oorg;
+                            q = oq;
+                        }
+                    }
+                    m = __shfl_sync(0xffffffffu, m, 0);
+                    row = __shfl_sync(0xffffffffu, row, 0);
+                    org = __shfl_sync(0xffffffffu, org, 0);
+                    q = __shfl_sync(0xffffffffu, q, 0);
+                    const unsigned long long prow = m < T(0) ? row_j : row;  // row_j is always a candidate
+                    T value = values[0];
+#pragma unroll
+                    for (int s = 1; s < kClusterCtas; ++s)
+                        if (q == static_cast<unsigned>(s)) value = values[s];
+                    const bool exchange = (prow - j0) / kCtaRows == c && prow != row_j;
+                    if (lane < W) {
+                        pivot_row[lane] = value;
+                        if (exchange) displaced[lane] = there;
+                    }
+                    if (lane == 0) {
+                        pivot_at = prow;
+                        pivot_origin = org;
+                        if (exchange) displaced_origin = there_origin;
+                        if (c == 0) exchanges[j] = static_cast<long long>(prow);
+                    }
+                }
+                __syncthreads();
+                const unsigned long long prow = pivot_at;
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+                    if (r[i] == prow && prow != row_j) {
+                        // this row moves to the pivot's old place: it takes the displaced row's values
+#pragma unroll
+                        for (int k = 0; k < W; ++k) v[i][k] = displaced[k];
+                        origin[i] = displaced_origin;
+                    }
+                    if (r[i] == row_j) {
+                        // the pivot row is final: U's row j0 + j from column j0 + j on
+#pragma unroll
+                        for (int k = 0; k < W; ++k) v[i][k] = pivot_row[k];
+                        origin[i] = pivot_origin;
+#pragma unroll
+                        for (int k = 0; k < W; ++k)
+                            if (k < width - j) a[origin[i] * n + row_j + k] = v[i][k];
+                    }
+                    // 3. eliminate below the pivot: l = a / pivot; a[k] -= l * pivot_row[k]; a zero
+                    //    pivot leaves the column as it is (decompose.hpp:44-45)
+                    if (valid[i] && r[i] > row_j) {
+                        const T diagonal = pivot_row[0];
+                        if (diagonal != T(0)) {
+                            const T l = div(v[i][0], diagonal);
+                            v[i][0] = l;
+#pragma unroll
+                            for (int k = 1; k < W; ++k) v[i][k] = sub(v[i][k], mul(l, pivot_row[k]));
+                        }
+                        if (origin[i] == r[i]) {
+                            stage[j * P + static_cast<int>(r[i] - first)] = v[i][0];
+                            mask[i] |= 1u << j;
+                        } else {
+                            a[origin[i] * n + row_j] = v[i][0];
+                        }
+                    }
+#pragma unroll
+                    for (int k = 0; k + 1 < W; ++k) v[i][k] = v[i][k + 1];
+                    v[i][W - 1] = T(0);
+                }
+            }
+            // The staged multipliers, one row per warp store. Then every row's panel values sit at the
+            // position the row started in; move the rows the exchanges displaced: all reads, a
+            // cluster barrier, then all writes.
+#pragma unroll
+            for (int i = 0; i < R; ++i) home[r[i] - first] = mask[i];
+            __syncthreads();
+            for (int row = warp; row < kCtaRows; row += WARPS) {
+                const unsigned long long g = first + row;
+                if (g >= n) break;
+                if (lane < static_cast<unsigned>(width) && (home[row] >> lane & 1u)) a[g * n + j0 + lane] = stage[lane * P + row];
+            }
+            __threadfence();
+            cluster_sync();
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                if (valid[i] && origin[i] != r[i]) {
+#pragma unroll
+                    for (int k = 0; k < W; ++k) v[i][k] = k < width ? a[origin[i] * n + j0 + k] : T(0);
+                }
+            }
+            cluster_sync();  // also: no CTA leaves while another may still read its shared memory
+#pragma unroll
+            for (int i = 0; i < R; ++i) {
+                if (valid[i] && origin[i] != r[i]) {
+#pragma unroll
+                    for (int k = 0; k < W; ++k)
+                        if (k < width) a[r[i] * n + j0 + k] = v[i][k];
+                }
+            }
             if (c == 0 && warp == 0) {
                 // The net movement of rows: the exchanges applied in order to a table of the rows they
                 // touch (at most 2W), one warp, each lane holding two table entries.
@@ -215,8 +380,9 @@ namespace sci_cuda {
                 long long row_b = -1;
                 long long src_a = row_a, src_b = -1;
                 int count = width;
+                if (lane < static_cast<unsigned>(width)) piv[j0 + lane] = exchanges[lane];
                 for (int j = 0; j < width; ++j) {
-                    const long long p = piv[j0 + j];
+                    const long long p = exchanges[j];
                     // where p sits in the table: entry index, or -1
                     const unsigned in_a = __ballot_sync(0xffffffffu, row_a == p);
                     const unsigned in_b = __ballot_sync(0xffffffffu, row_b == p);
@@ -257,7 +423,6 @@ namespace sci_cuda {
                 }
                 if (lane == 0) moved->count = __popc(mask_a) + __popc(mask_b);
             }
-            cluster_sync();  // no CTA leaves while another may still read its shared memory
         }
 
         // Applies a panel's net row movement to every column outside [skip0, skip1): all reads first,
@@ -312,7 +477,7 @@ namespace sci_cuda {
                                                            const T *__restrict__ b, unsigned long long ldb, T *c,
                                                            unsigned long long ldc, unsigned long long m, unsigned long long n,
                                                            unsigned long long k) {
-            constexpr int BM = 64, BK = 32, TN = BN / 16;
+            constexpr int BM = 64, BK = 32, TN = BN / 16, LA = BM * BK / 256, LB = BK * BN / 256;
             __shared__ T as[BK][BM + 1];
             __shared__ T bs[BK][BN + 1];
             const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
@@ -322,18 +487,37 @@ namespace sci_cuda {
             for (int i = 0; i < 4; ++i)
 #pragma unroll
                 for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
-            for (unsigned long long k0 = 0; k0 < k; k0 += BK) {
-                for (int i = threadIdx.x; i < BM * BK; i += 256) {
-                    const int row = i / BK, q = i % BK;
+            // Each K slice is loaded into registers (all of a thread's loads in flight together) while
+            // the previous one is multiplied out of shared memory.
+            T ra[LA], rb[LB];
+            auto fetch = [&](unsigned long long k0) {
+#pragma unroll
+                for (int u = 0; u < LA; ++u) {
+                    const int i = threadIdx.x + u * 256, row = i / BK, q = i % BK;
                     const unsigned long long gr = m0 + row, gk = k0 + q;
-                    as[q][row] = (gr < m && gk < k) ? a[gr * lda + gk] : T(0);
+                    ra[u] = (gr < m && gk < k) ? a[gr * lda + gk] : T(0);
                 }
-                for (int i = threadIdx.x; i < BK * BN; i += 256) {
-                    const int q = i / BN, col = i % BN;
+#pragma unroll
+                for (int u = 0; u < LB; ++u) {
+                    const int i = threadIdx.x + u * 256, q = i / BN, col = i % BN;
                     const unsigned long long gk = k0 + q, gc = n0 + col;
-                    bs[q][col] = (gk < k && gc < n) ? b[gk * ldb + gc] : T(0);
+                    rb[u] = (gk < k && gc < n) ? b[gk * ldb + gc] : T(0);
+                }
+            };
+            fetch(0);
+            for (unsigned long long k0 = 0; k0 < k; k0 += BK) {
+#pragma unroll
+                for (int u = 0; u < LA; ++u) {
+                    const int i = threadIdx.x + u * 256;
+                    as[i % BK][i / BK] = ra[u];
+                }
+#pragma unroll
+                for (int u = 0; u < LB; ++u) {
+                    const int i = threadIdx.x + u * 256;
+                    bs[i / BN][i % BN] = rb[u];
                 }
                 __syncthreads();
+                if (k0 + BK < k) fetch(k0 + BK);
 #pragma unroll 8
                 for (int q = 0; q < BK; ++q) {
                     T av[4], bv[TN];
@@ -378,20 +562,28 @@ namespace sci_cuda {
         // Rows [j0, j0 + w) of columns [c0, c1) := L^-1 times themselves, L the unit lower triangle
         // of the panel's top w x w block. One thread per column, the column's w values in registers.
         template <typename T>
-        __global__ void trsm_rows(T *a, unsigned long long n, unsigned long long j0, int w, unsigned long long c0,
+        __global__ void __launch_bounds__(128) trsm_rows(T *a, unsigned long long n, unsigned long long j0, int w, unsigned long long c0,
                                   unsigned long long c1) {
             constexpr int W = PanelWidth<T>::value;
+            constexpr int threads = 128, L = W * W / threads;
             __shared__ T lower[W][W];
-            for (int i = threadIdx.x; i < W * W; i += blockDim.x) {
-                const int row = i / W, k = i % W;
-                lower[row][k] = (row < w && k < w) ? a[(j0 + row) * n + j0 + k] : T(0);
+            const unsigned long long col = c0 + blockIdx.x * 1ull * threads + threadIdx.x;
+            // every global load of the thread is issued before the first shared store
+            T staged[L], x[W];
+#pragma unroll
+            for (int u = 0; u < L; ++u) {
+                const int i = threadIdx.x + u * threads, row = i / W, k = i % W;
+                staged[u] = (row < w && k < w) ? a[(j0 + row) * n + j0 + k] : T(0);
+            }
+#pragma unroll
+            for (int i = 0; i < W; ++i) x[i] = (col < c1 && i < w) ? a[(j0 + i) * n + col] : T(0);
+#pragma unroll
+            for (int u = 0; u < L; ++u) {
+                const int i = threadIdx.x + u * threads;
+                lower[i / W][i % W] = staged[u];
             }
             __syncthreads();
-            const unsigned long long col = c0 + blockIdx.x * 1ull * blockDim.x + threadIdx.x;
             if (col >= c1) return;
-            T x[W];
-#pragma unroll
-            for (int i = 0; i < W; ++i) x[i] = i < w ? a[(j0 + i) * n + col] : T(0);
 #pragma unroll
             for (int i = 1; i < W; ++i) {
 #pragma unroll
@@ -411,9 +603,19 @@ namespace sci_cuda {
                                     unsigned long long width) {
             extern __shared__ __align__(16) unsigned char solve_shared[];
             T(*tri)[kSolveBlock + 1] = reinterpret_cast<T(*)[kSolveBlock + 1]>(solve_shared);
-            for (int i = threadIdx.x; i < size * size; i += blockDim.x) {
-                const int row = i / size, k = i % size;
-                tri[row][k] = lu[(s + row) * n + s + k];
+            {
+                constexpr int L = kSolveBlock * kSolveBlock / 1024;
+                T staged[L];
+#pragma unroll
+                for (int u = 0; u < L; ++u) {
+                    const int i = threadIdx.x + u * 1024, row = i / kSolveBlock, k = i % kSolveBlock;
+                    staged[u] = (row < size && k < size) ? lu[(s + row) * n + s + k] : T(0);
+                }
+#pragma unroll
+                for (int u = 0; u < L; ++u) {
+                    const int i = threadIdx.x + u * 1024;
+                    tri[i / kSolveBlock][i % kSolveBlock] = staged[u];
+                }
             }
             __syncthreads();
             const unsigned lane = threadIdx.x % 32, warp = threadIdx.x / 32;
@@ -481,35 +683,94 @@ namespace sci_cuda {
             }
         }
 
-        // x[s + r][col] := sum_k inv[r][k] x[s + k][col] for the `size` rows of one diagonal block, 32
-        // columns per CTA (blockIdx.y): the block's inverse and its rows of x are read whole into
-        // shared memory before any row is written. Warp w computes rows 4w .. 4w + 3, lane = column.
-        // inv is triangular: lower blocks sum over k <= r, upper ones over k >= r.
+        // y[s + r][col] := sum_k inv[r][k] x[s + k][col] for the `size` rows of one diagonal block, out
+        // of place: 16 rows (blockIdx.x) by 32 columns (blockIdx.y) per CTA of 512 threads, warp w
+        // computing row 16 blockIdx.x + w with lane = column. inv is zero padded to kSolveBlock
+        // square and triangular: lower blocks sum over k <= r, upper ones over k >= r.
+        constexpr int kApplyRows = 16;
+        template <typename T> constexpr size_t apply_shared_bytes() {
+            return sizeof(T) * (kApplyRows * kSolveBlock + kSolveBlock * 32);
+        }
         template <typename T, bool upper>
-        __global__ void __launch_bounds__(1024) apply_inverse(const T *inv, unsigned long long s, int size, T *x,
-                                                              unsigned long long width) {
-            constexpr int B = kSolveBlock;
+        __global__ void __launch_bounds__(kApplyRows * 32) apply_inverse(const T *inv, unsigned long long s, int size,
+                                                                         const T *x, T *y, unsigned long long width) {
+            constexpr int B = kSolveBlock, threads = kApplyRows * 32;
             extern __shared__ __align__(16) unsigned char apply_shared[];
-            T *ms = reinterpret_cast<T *>(apply_shared);  // [B][B]: the inverse
-            T *xs = ms + B * B;                           // [B][32]: the block of x
+            T *ms = reinterpret_cast<T *>(apply_shared);  // [kApplyRows][B]: this CTA's rows of inv
+            T *xs = ms + kApplyRows * B;                  // [B][32]: the block of x
+            const int r0 = blockIdx.x * kApplyRows;
             const unsigned long long c0 = blockIdx.y * 32ull;
-            for (int i = threadIdx.x; i < B * B; i += 1024) ms[i] = inv[i];
-            for (int i = threadIdx.x; i < B * 32; i += 1024) {
-                const int k = i / 32, col = i % 32;
-                xs[i] = (k < size && c0 + col < width) ? x[(s + k) * width + c0 + col] : T(0);
-            }
-            __syncthreads();
-            const int lane = threadIdx.x % 32, warp = threadIdx.x / 32;
-            const unsigned long long col = c0 + lane;
+            constexpr int LM = kApplyRows * B / threads, LX = B * 32 / threads;
+            T rm[LM], rx[LX];  // every global load of the thread is issued before the first shared store
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int r = warp * 4 + q;
-                if (r >= size) break;
-                const int k0 = upper ? r : 0, k1 = upper ? size : r + 1;
-                T acc = T(0);
-                for (int k = k0; k < k1; ++k) acc = fma_(ms[r * B + k], xs[k * 32 + lane], acc);
-                if (col < width) x[(s + r) * width + col] = acc;
+            for (int u = 0; u < LM; ++u) rm[u] = inv[r0 * B + threadIdx.x + u * threads];
+#pragma unroll
+            for (int u = 0; u < LX; ++u) {
+                const int i = threadIdx.x + u * threads, k = i / 32, col = i % 32;
+                rx[u] = (k < size && c0 + col < width) ? x[(s + k) * width + c0 + col] : T(0);
             }
+#pragma unroll
+            for (int u = 0; u < LM; ++u) ms[threadIdx.x + u * threads] = rm[u];
+#pragma unroll
+            for (int u = 0; u < LX; ++u) xs[threadIdx.x + u * threads] = rx[u];
+            __syncthreads();
+            const int lane = threadIdx.x % 32, row = threadIdx.x / 32, r = r0 + row;
+            if (r >= size) return;
+            const int k0 = upper ? r : 0, k1 = upper ? size : r + 1;
+            T acc = T(0);
+            for (int k = k0; k < k1; ++k) acc = fma_(ms[row * B + k], xs[k * 32 + lane], acc);
+            if (c0 + lane < width) y[(s + r) * width + c0 + lane] = acc;
+        }
+
+        // C (m x w, pitch ldc) -= A (m x k, pitch lda) * B (k x w, pitch ldb) for w <= 32 and
+        // k <= kSolveBlock: the substitution's update of the rows beyond a diagonal block. 32 rows per
+        // CTA; A's rows and all of B staged in shared memory; thread = (row, 4 columns).
+        constexpr int kSkinnyRows = 32;
+        template <typename T> constexpr size_t skinny_shared_bytes() {
+            return sizeof(T) * (kSkinnyRows * (kSolveBlock + 1) + kSolveBlock * 32);
+        }
+        template <typename T>
+        __global__ void __launch_bounds__(256) skinny_update(const T *a, unsigned long long lda, const T *b,
+                                                             unsigned long long ldb, T *c, unsigned long long ldc,
+                                                             unsigned long long m, int w, int k) {
+            constexpr int B = kSolveBlock, P = kSolveBlock + 1;
+            extern __shared__ __align__(16) unsigned char skinny_shared[];
+            T *as = reinterpret_cast<T *>(skinny_shared);  // [kSkinnyRows][P]
+            T *bs = as + kSkinnyRows * P;                  // [B][32]
+            const unsigned long long m0 = blockIdx.x * 1ull * kSkinnyRows;
+            constexpr int LA = kSkinnyRows * B / 256, LB = B * 32 / 256;
+            T ra[LA], rb[LB];  // every global load of the thread is issued before the first shared store
+#pragma unroll
+            for (int u = 0; u < LA; ++u) {
+                const int i = threadIdx.x + u * 256, row = i / B, q = i % B;
+                ra[u] = (m0 + row < m && q < k) ? a[(m0 + row) * lda + q] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < LB; ++u) {
+                const int i = threadIdx.x + u * 256, q = i / 32, col = i % 32;
+                rb[u] = (q < k && col < w) ? b[q * ldb + col] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < LA; ++u) {
+                const int i = threadIdx.x + u * 256;
+                as[(i / B) * P + i % B] = ra[u];
+            }
+#pragma unroll
+            for (int u = 0; u < LB; ++u) bs[threadIdx.x + u * 256] = rb[u];
+            __syncthreads();
+            const int row = threadIdx.x / 8, c4 = (threadIdx.x % 8) * 4;
+            if (c4 >= w) return;
+            T acc[4] = {T(0), T(0), T(0), T(0)};
+            for (int q = 0; q < k; ++q) {
+                const T av = as[row * P + q];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[j] = fma_(av, bs[q * 32 + c4 + j], acc[j]);
+            }
+            const unsigned long long gr = m0 + row;
+            if (gr >= m) return;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (c4 + j < w) c[gr * ldc + c4 + j] = sub(c[gr * ldc + c4 + j], acc[j]);
         }
 
         // ---- FP64 helpers of the refinement -----------------------------------------------------------
@@ -570,11 +831,16 @@ namespace sci_cuda {
                                          "reserving the trailing-update workspace"))
                     return code;
             }
+            if (int code = ctx.check(cudaFuncSetAttribute(reinterpret_cast<const void *>(&panel_factor<T>),
+                                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                          static_cast<int>(panel_shared_bytes<T>())),
+                                     "sizing the panel kernel's shared memory"))
+                return code;
             for (unsigned long long J0 = 0; J0 < n; J0 += kOuter) {
                 const unsigned long long ob = std::min<unsigned long long>(kOuter, n - J0);
                 for (unsigned long long j0 = J0; j0 < J0 + ob; j0 += W) {
                     const int w = static_cast<int>(std::min<unsigned long long>(W, J0 + ob - j0));
-                    panel_factor<T><<<kClusterCtas, kPanelThreads, 0, ctx.stream>>>(a, n, j0, w, piv, moved);
+                    panel_factor<T><<<kClusterCtas, kPanelBlock, panel_shared_bytes<T>(), ctx.stream>>>(a, n, j0, w, piv, moved);
                     if (int code = ctx.check(cudaGetLastError(), "launching the panel factorisation")) return code;
                     move_rows<T><<<static_cast<unsigned>((n + 255) / 256), 256, 0, ctx.stream>>>(a, n, moved, j0, j0 + w);
                     // Inside the outer block only: U rows of the panel, then the rows below it. Columns
@@ -639,28 +905,19 @@ namespace sci_cuda {
             return ctx.check(cudaGetLastError(), "inverting the diagonal blocks");
         }
 
-        // x (n x width, in place: holds P b on entry) := U^-1 L^-1 x. With inv (from invert_diagonal)
-        // each diagonal block is one small product; without it, a substitution in the reference's
-        // order inside the block (FP64 solves keep that form).
+        // x (n x width, in place: holds P b on entry) := U^-1 L^-1 x, a substitution in the
+        // reference's order inside each diagonal block (the FP64 form).
         template <typename T>
-        int substitute_device(Context &ctx, const T *lu, const T *inv, unsigned long long n, T *x, unsigned long long width) {
+        int substitute_device(Context &ctx, const T *lu, unsigned long long n, T *x, unsigned long long width) {
             const dim3 groups(1, static_cast<unsigned>((width + 31) / 32));
-            const size_t smem = inv ? sizeof(T) * (kSolveBlock * kSolveBlock + kSolveBlock * 32)
-                                    : sizeof(T) * kSolveBlock * (kSolveBlock + 1);
-            const void *forward = inv ? reinterpret_cast<const void *>(&apply_inverse<T, false>)
-                                      : reinterpret_cast<const void *>(&solve_block<T, false>);
-            const void *backward = inv ? reinterpret_cast<const void *>(&apply_inverse<T, true>)
-                                       : reinterpret_cast<const void *>(&solve_block<T, true>);
-            cudaFuncSetAttribute(forward, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-            cudaFuncSetAttribute(backward, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-            constexpr unsigned long long block_elements = 1ull * kSolveBlock * kSolveBlock;
+            const size_t smem = sizeof(T) * kSolveBlock * (kSolveBlock + 1);
+            cudaFuncSetAttribute(reinterpret_cast<const void *>(&solve_block<T, false>),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+            cudaFuncSetAttribute(reinterpret_cast<const void *>(&solve_block<T, true>),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
             for (unsigned long long s = 0; s < n; s += kSolveBlock) {
                 const int size = static_cast<int>(std::min<unsigned long long>(kSolveBlock, n - s));
-                if (inv)
-                    apply_inverse<T, false><<<groups, 1024, smem, ctx.stream>>>(inv + 2 * (s / kSolveBlock) * block_elements, s,
-                                                                                size, x, width);
-                else
-                    solve_block<T, false><<<groups, 1024, smem, ctx.stream>>>(lu, n, s, size, x, width);
+                solve_block<T, false><<<groups, 1024, smem, ctx.stream>>>(lu, n, s, size, x, width);
                 const unsigned long long below = s + size;
                 if (below < n) {
                     if (int code = update<T>(ctx, lu + below * n + s, n, x + s * width, width, x + below * width, width,
@@ -672,15 +929,60 @@ namespace sci_cuda {
             for (long long s = static_cast<long long>(last); s >= 0; s -= kSolveBlock) {
                 const unsigned long long us = static_cast<unsigned long long>(s);
                 const int size = static_cast<int>(std::min<unsigned long long>(kSolveBlock, n - us));
-                if (inv)
-                    apply_inverse<T, true><<<groups, 1024, smem, ctx.stream>>>(
-                            inv + (2 * (us / kSolveBlock) + 1) * block_elements, us, size, x, width);
-                else
-                    solve_block<T, true><<<groups, 1024, smem, ctx.stream>>>(lu, n, us, size, x, width);
+                solve_block<T, true><<<groups, 1024, smem, ctx.stream>>>(lu, n, us, size, x, width);
                 if (us > 0) {
                     if (int code = update<T>(ctx, lu + us, n, x + us * width, width, x, width, us, width, size))
                         return code;
                 }
+            }
+            return ctx.check(cudaGetLastError(), "launching the substitution");
+        }
+
+        // C -= A B for the substitution: the skinny kernel when B has at most 32 columns.
+        template <typename T>
+        int substitution_update(Context &ctx, const T *a, unsigned long long lda, const T *b, T *c, unsigned long long m,
+                                unsigned long long width, int k) {
+            if (m == 0) return SCI_CUDA_OK;
+            if (width > 32) return update<T>(ctx, a, lda, b, width, c, width, m, width, static_cast<unsigned long long>(k));
+            skinny_update<T><<<static_cast<unsigned>((m + kSkinnyRows - 1) / kSkinnyRows), 256, skinny_shared_bytes<T>(),
+                               ctx.stream>>>(a, lda, b, width, c, width, m, static_cast<int>(width), k);
+            return SCI_CUDA_OK;
+        }
+
+        // x (n x width; holds P b on entry) := U^-1 L^-1 x with the diagonal blocks' inverses (from
+        // invert_diagonal): each block is one small product, spread over 8 CTAs, and the rows beyond
+        // it are updated by the skinny kernel. y (n x width) is scratch: the forward sweep writes
+        // L^-1 P b there and the backward sweep writes the solution back into x.
+        template <typename T>
+        int substitute_inverse(Context &ctx, const T *lu, const T *inv, unsigned long long n, T *x, T *y,
+                               unsigned long long width) {
+            const unsigned column_groups = static_cast<unsigned>((width + 31) / 32);
+            const int apply_smem = static_cast<int>(apply_shared_bytes<T>());
+            cudaFuncSetAttribute(reinterpret_cast<const void *>(&apply_inverse<T, false>),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, apply_smem);
+            cudaFuncSetAttribute(reinterpret_cast<const void *>(&apply_inverse<T, true>),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, apply_smem);
+            cudaFuncSetAttribute(reinterpret_cast<const void *>(&skinny_update<T>), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(skinny_shared_bytes<T>()));
+            constexpr unsigned long long block_elements = 1ull * kSolveBlock * kSolveBlock;
+            for (unsigned long long s = 0; s < n; s += kSolveBlock) {
+                const int size = static_cast<int>(std::min<unsigned long long>(kSolveBlock, n - s));
+                const dim3 grid(static_cast<unsigned>((size + kApplyRows - 1) / kApplyRows), column_groups);
+                apply_inverse<T, false><<<grid, kApplyRows * 32, apply_smem, ctx.stream>>>(
+                        inv + 2 * (s / kSolveBlock) * block_elements, s, size, x, y, width);
+                const unsigned long long below = s + size;
+                if (int code = substitution_update<T>(ctx, lu + below * n + s, n, y + s * width, x + below * width, n - below,
+                                                      width, size))
+                    return code;
+            }
+            const unsigned long long last = (n - 1) / kSolveBlock * kSolveBlock;
+            for (long long s = static_cast<long long>(last); s >= 0; s -= kSolveBlock) {
+                const unsigned long long us = static_cast<unsigned long long>(s);
+                const int size = static_cast<int>(std::min<unsigned long long>(kSolveBlock, n - us));
+                const dim3 grid(static_cast<unsigned>((size + kApplyRows - 1) / kApplyRows), column_groups);
+                apply_inverse<T, true><<<grid, kApplyRows * 32, apply_smem, ctx.stream>>>(
+                        inv + (2 * (us / kSolveBlock) + 1) * block_elements, us, size, y, x, width);
+                if (int code = substitution_update<T>(ctx, lu + us, n, x + us * width, y, us, width, size)) return code;
             }
             return ctx.check(cudaGetLastError(), "launching the substitution");
         }
@@ -800,7 +1102,7 @@ extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uin
     const bool wide = precision == SCI_PRECISION_WIDE;
     const size_t element = (wide && refine == SCI_REFINE_NONE) ? 8 : 4;
     const unsigned long long need = n * n * element + n * 8 + sizeof(Movement) + n * 4 + nw * 12 + n * 8 + width * 16 +
-                                    inverse_elements(n) * 4 + 8192;
+                                    inverse_elements(n) * 4 + nw * 4 + 8192;
     if (int code = context->check(context->solver->reserve(need), "reserving the solver workspace")) return code;
     Carve carve{static_cast<unsigned char *>(context->solver->memory)};
     long long *piv = carve.take<long long>(n);
@@ -817,7 +1119,7 @@ extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uin
             if (!code) code = row_order(*context, piv, rows, n);
             if (!code) permute<double, double>(*context, static_cast<const double *>(right), static_cast<double *>(solution),
                                                rows, n, width);
-            if (!code) code = substitute_device<double>(*context, lu, nullptr, n, static_cast<double *>(solution), width);
+            if (!code) code = substitute_device<double>(*context, lu, n, static_cast<double *>(solution), width);
             if (!code && report) {
                 double *r = carve.take<double>(nw);
                 double *sums = carve.take<double>(n);
@@ -835,13 +1137,14 @@ extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uin
         } else {
             float *lu = carve.take<float>(n * n);
             float *inv = carve.take<float>(inverse_elements(n));
+            float *y = carve.take<float>(nw);
             cudaMemcpyAsync(lu, matrix, n * n * 4, cudaMemcpyDeviceToDevice, context->stream);
             code = factor_device<float>(*context, lu, n, piv, moved, true, true);
             if (!code) code = invert_diagonal<float>(*context, lu, n, inv);
             if (!code) code = row_order(*context, piv, rows, n);
             if (!code) permute<float, float>(*context, static_cast<const float *>(right), static_cast<float *>(solution), rows,
                                              n, width);
-            if (!code) code = substitute_device<float>(*context, lu, inv, n, static_cast<float *>(solution), width);
+            if (!code) code = substitute_inverse<float>(*context, lu, inv, n, static_cast<float *>(solution), y, width);
         }
         if (!code) code = context->drain();
         return code;
@@ -853,6 +1156,7 @@ extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uin
     double *x = static_cast<double *>(solution);
     float *lu = carve.take<float>(n * n);
     float *inv = carve.take<float>(inverse_elements(n));
+    float *y = carve.take<float>(nw);
     double *r = carve.take<double>(nw);
     float *d = carve.take<float>(nw);
     double *sums = carve.take<double>(n);
@@ -874,7 +1178,7 @@ extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uin
     const double *residual = b;  // the first correction solves for b itself
     while (iterations < kMaxIterations) {
         permute<double, float>(*context, residual, d, rows, n, width);
-        if (int code = substitute_device<float>(*context, lu, inv, n, d, width)) return code;
+        if (int code = substitute_inverse<float>(*context, lu, inv, n, d, y, width)) return code;
         widen_add<<<blocks_for(nw, sms), 256, 0, context->stream>>>(d, x, nw);
         ++iterations;
         if (int code = backward_error(*context, a, b, x, r, sums, norms, n, width, a_norm, b_norm.data(), berr)) return code;

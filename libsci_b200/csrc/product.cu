@@ -312,7 +312,7 @@ namespace sci_cuda {
                                                             const T *__restrict__ b, unsigned long long ldb, T *__restrict__ c,
                                                             unsigned long long ldc, unsigned long long m, unsigned long long n,
                                                             unsigned long long k, int subtract) {
-            constexpr int BM = 128, BN = 128, BK = 8, TM = 8, TN = 8;
+            constexpr int BM = 128, BN = 128, BK = 8, TM = 8, TN = 8, LA = BM * BK / 256, LB = BK * BN / 256;
             __shared__ T as[BK][BM + 4];
             __shared__ T bs[BK][BN + 4];
             const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
@@ -323,19 +323,38 @@ namespace sci_cuda {
             for (int i = 0; i < TM; ++i)
 #pragma unroll
                 for (int j = 0; j < TN; ++j) acc[i][j] = T(0);
-            for (unsigned long long k0 = 0; k0 < k; k0 += BK) {
-                // A tile: 128 rows x 8 columns, stored transposed; B tile: 8 rows x 128 columns.
-                for (int i = threadIdx.x; i < BM * BK; i += 256) {
-                    const int r = i / BK, q = i % BK;
+            // A tile: 128 rows x 8 columns, stored transposed; B tile: 8 rows x 128 columns. Each K
+            // slice is loaded into registers (all of a thread's loads in flight together) while the
+            // previous one is multiplied out of shared memory.
+            T ra[LA], rb[LB];
+            auto fetch = [&](unsigned long long k0) {
+#pragma unroll
+                for (int u = 0; u < LA; ++u) {
+                    const int i = threadIdx.x + u * 256, r = i / BK, q = i % BK;
                     const unsigned long long gr = m0 + r, gk = k0 + q;
-                    as[q][r] = (gr < m && gk < k) ? a[gr * lda + gk] : T(0);
+                    ra[u] = (gr < m && gk < k) ? a[gr * lda + gk] : T(0);
                 }
-                for (int i = threadIdx.x; i < BK * BN; i += 256) {
-                    const int q = i / BN, col = i % BN;
+#pragma unroll
+                for (int u = 0; u < LB; ++u) {
+                    const int i = threadIdx.x + u * 256, q = i / BN, col = i % BN;
                     const unsigned long long gk = k0 + q, gc = n0 + col;
-                    bs[q][col] = (gk < k && gc < n) ? b[gk * ldb + gc] : T(0);
+                    rb[u] = (gk < k && gc < n) ? b[gk * ldb + gc] : T(0);
+                }
+            };
+            fetch(0);
+            for (unsigned long long k0 = 0; k0 < k; k0 += BK) {
+#pragma unroll
+                for (int u = 0; u < LA; ++u) {
+                    const int i = threadIdx.x + u * 256;
+                    as[i % BK][i / BK] = ra[u];
+                }
+#pragma unroll
+                for (int u = 0; u < LB; ++u) {
+                    const int i = threadIdx.x + u * 256;
+                    bs[i / BN][i % BN] = rb[u];
                 }
                 __syncthreads();
+                if (k0 + BK < k) fetch(k0 + BK);
 #pragma unroll
                 for (int q = 0; q < BK; ++q) {
                     T av[TM], bv[TN];
