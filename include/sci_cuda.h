@@ -173,6 +173,25 @@ int sci_cuda_factor(sci_cuda_context *context, uint32_t precision, uint32_t mode
 int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uint32_t refine, const void *matrix, const void *right,
                    void *solution, uint64_t order, uint64_t width, sci_solve_report *report);
 
+/* ---- gradients ------------------------------------------------------------------------------- */
+/* No counterpart in the reference (sci::gradient is new; the reference has no differentiation).
+ * For L = seed * sum over count elements of the chunk's reduced value (the sum
+ * sci_cuda_reduce(SCI_FOLD_SUM) computes), writes dL/d(argument a) elementwise to gradients[a]
+ * (device memory, count elements of the chunk's element type; a null entry, or a null array, skips
+ * it) and, when `value` is not null, the sum itself to *value (double). The derivatives are those of
+ * the function the device computes: forward values are bit-identical to sci_cuda_execute's, partial
+ * derivatives are evaluated in double and adjoints accumulate in double before one rounding.
+ * Conventions: d|x| at 0 is 0; minimum / maximum pass the adjoint to the operand they returned;
+ * a zero adjoint passes nothing back. `form`: */
+enum {
+    SCI_GRADIENT_RECOMPUTE = 0, /* one pass: forward values recomputed in registers, reverse walk, no tape */
+    SCI_GRADIENT_STORED = 1     /* the plain comparison form: a forward pass stores every value of the chunk
+                                   on a device tape (nodes x count elements, kept by the context), and a
+                                   backward pass reads it */
+};
+int sci_cuda_gradient(sci_cuda_context *context, const sci_chunk *chunk, uint64_t count, double seed,
+                      void *const *gradients, double *value, uint32_t form);
+
 /* No counterpart in the reference. The same reduction for callers that may not allocate device
  * memory (a host framework that owns the GPU heap through its own pool, a plugin inside one, a
  * latency-critical thread where an allocation would synchronize the device). It needs no context:

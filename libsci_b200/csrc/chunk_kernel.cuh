@@ -432,14 +432,71 @@ namespace sci_cuda {
         else return L.arguments;
     }
 
+    // The grid-wide end of a single-pass fold: each thread's state folds across its warp (shuffle)
+    // and block, every block writes one partial, and the last block to take a ticket folds the
+    // partials in block order and writes the value to `destination`. Every thread of the block
+    // calls it.
+    template <typename T>
+    __device__ __forceinline__ void finish_fold(Fold fold, unsigned op, ReduceState *state, double *destination) {
+        __shared__ double block_total[32];
+        __shared__ unsigned block_magnitude[32];
+        __shared__ bool last_block;
+        const unsigned threads = blockDim.x, t = threadIdx.x;
+        // warp
+#pragma unroll
+        for (int offset = 16; offset > 0; offset >>= 1) {
+            const double other = __shfl_xor_sync(0xffffffffu, fold.total, offset);
+            fold.total = combine(op, fold.total, other);
+            fold.magnitude = max(fold.magnitude, __shfl_xor_sync(0xffffffffu, fold.magnitude, offset));
+        }
+        const unsigned warp = t / 32, warps = (threads + 31) / 32;
+        if ((t & 31) == 0) {
+            block_total[warp] = fold.total;
+            block_magnitude[warp] = fold.magnitude;
+        }
+        __syncthreads();
+        if (t == 0) {
+            double total = block_total[0];
+            unsigned magnitude = block_magnitude[0];
+            for (unsigned i = 1; i < warps; ++i) {
+                total = combine(op, total, block_total[i]);
+                magnitude = max(magnitude, block_magnitude[i]);
+            }
+            state->partial[blockIdx.x] = total;
+            state->poisoned[blockIdx.x] = magnitude > nan_floor<T>() ? 1 : 0;
+            __threadfence();
+            const unsigned ticket = atomicAdd(&state->ticket, 1u);
+            last_block = ticket == gridDim.x - 1;
+        }
+        __syncthreads();
+        if (last_block && t < 32) {
+            __threadfence();
+            // Fold the block partials in block order: lane l takes blocks l, l+32, ... then the
+            // lanes combine in a fixed tree, so the result depends only on the launch shape.
+            double total = op == 0 ? 0.0 : (op == 1 ? __longlong_as_double(0x7ff0000000000000ll)
+                                                    : __longlong_as_double((long long)0xfff0000000000000ull));
+            int poisoned = 0;
+            for (unsigned b = t; b < gridDim.x; b += 32) {
+                total = combine(op, total, __ldcg(&state->partial[b]));
+                poisoned |= __ldcg(&state->poisoned[b]);
+            }
+#pragma unroll
+            for (int offset = 16; offset > 0; offset >>= 1) {
+                total = combine(op, total, __shfl_xor_sync(0xffffffffu, total, offset));
+                poisoned |= __shfl_xor_sync(0xffffffffu, poisoned, offset);
+            }
+            if (t == 0) {
+                *destination = poisoned ? __longlong_as_double(0x7ff8000000000000ll) : total;
+                state->ticket = 0;
+            }
+        }
+    }
+
     // ---- the kernel -----------------------------------------------------------------------------------
     template <typename T, class Program, int MODE>
     __global__ void __launch_bounds__(256) chunk_stream(const __grid_constant__ Launch<T> L) {
         extern __shared__ __align__(128) unsigned char shared[];
         __shared__ unsigned long long bars[kMaxStages];
-        __shared__ double block_total[32];
-        __shared__ unsigned block_magnitude[32];
-        __shared__ bool last_block;
         constexpr int N = Lanes<T>::count;
 
         const unsigned threads = blockDim.x, t = threadIdx.x;
@@ -525,56 +582,7 @@ namespace sci_cuda {
             if constexpr (MODE != kEvaluate) fold_tile<T, MODE>(fold, op, value, second, w, false);
         }
 
-        if constexpr (MODE != kEvaluate) {
-            // warp
-#pragma unroll
-            for (int offset = 16; offset > 0; offset >>= 1) {
-                const double other = __shfl_xor_sync(0xffffffffu, fold.total, offset);
-                fold.total = combine(op, fold.total, other);
-                fold.magnitude = max(fold.magnitude, __shfl_xor_sync(0xffffffffu, fold.magnitude, offset));
-            }
-            const unsigned warp = t / 32, warps = (threads + 31) / 32;
-            if ((t & 31) == 0) {
-                block_total[warp] = fold.total;
-                block_magnitude[warp] = fold.magnitude;
-            }
-            __syncthreads();
-            if (t == 0) {
-                double total = block_total[0];
-                unsigned magnitude = block_magnitude[0];
-                for (unsigned i = 1; i < warps; ++i) {
-                    total = combine(op, total, block_total[i]);
-                    magnitude = max(magnitude, block_magnitude[i]);
-                }
-                L.state->partial[blockIdx.x] = total;
-                L.state->poisoned[blockIdx.x] = magnitude > nan_floor<T>() ? 1 : 0;
-                __threadfence();
-                const unsigned ticket = atomicAdd(&L.state->ticket, 1u);
-                last_block = ticket == gridDim.x - 1;
-            }
-            __syncthreads();
-            if (last_block && t < 32) {
-                __threadfence();
-                // Fold the block partials in block order: lane l takes blocks l, l+32, ... then the
-                // lanes combine in a fixed tree, so the result depends only on the launch shape.
-                double total = op == 0 ? 0.0 : (op == 1 ? __longlong_as_double(0x7ff0000000000000ll)
-                                                        : __longlong_as_double((long long)0xfff0000000000000ull));
-                int poisoned = 0;
-                for (unsigned b = t; b < gridDim.x; b += 32) {
-                    total = combine(op, total, __ldcg(&L.state->partial[b]));
-                    poisoned |= __ldcg(&L.state->poisoned[b]);
-                }
-#pragma unroll
-                for (int offset = 16; offset > 0; offset >>= 1) {
-                    total = combine(op, total, __shfl_xor_sync(0xffffffffu, total, offset));
-                    poisoned |= __shfl_xor_sync(0xffffffffu, poisoned, offset);
-                }
-                if (t == 0) {
-                    *L.destination = poisoned ? __longlong_as_double(0x7ff8000000000000ll) : total;
-                    L.state->ticket = 0;
-                }
-            }
-        }
+        if constexpr (MODE != kEvaluate) finish_fold<T>(fold, op, L.state, L.destination);
     }
 
 } // namespace sci_cuda

@@ -87,6 +87,7 @@ namespace sci_cuda {
         std::unique_ptr<Specializer> specializer;
         std::unique_ptr<Workspace> workspace;  // product / trailing-update operands
         std::unique_ptr<Workspace> solver;     // LU copies, pivots, residuals
+        std::unique_ptr<Workspace> tape;       // the stored-form gradient's forward values
         int jit_mode{1};  // 0 off, 1 background, 2 synchronous (SCI_CUDA_JIT)
         bool jit_trace{false};
 
@@ -143,6 +144,10 @@ namespace sci_cuda {
 
     // Validates a chunk before anything is launched: counts, codes, and every value id in range.
     int validate(Context &ctx, const sci_chunk *chunk, bool reducing);
+
+    // Whether a pointer is memory this context's GPU reads directly (device memory of its GPU, or
+    // managed memory).
+    bool reachable(Context &ctx, const void *pointer);
 
 } // namespace sci_cuda
 

@@ -97,7 +97,7 @@ namespace sci_cuda {
 
     // Whether a pointer is memory this context's GPU reads directly (the reference's
     // Allocator::locate, src/core/drivers/vulkan/allocator.cpp:81-89).
-    static bool reachable(Context &ctx, const void *pointer) {
+    bool reachable(Context &ctx, const void *pointer) {
         cudaPointerAttributes attributes{};
         if (cudaPointerGetAttributes(&attributes, pointer) != cudaSuccess) {
             cudaGetLastError();
@@ -279,6 +279,7 @@ int sci_cuda_open(uint32_t ordinal, sci_cuda_context **context) {
     ctx->specializer = make_specializer(*ctx);
     ctx->workspace = std::make_unique<Workspace>();
     ctx->solver = std::make_unique<Workspace>();
+    ctx->tape = std::make_unique<Workspace>();
     *context = ctx.release();
     return SCI_CUDA_OK;
 }
@@ -292,6 +293,7 @@ int sci_cuda_close(sci_cuda_context *context) {
         context->specializer.reset();
         if (context->workspace) context->workspace->release();
         if (context->solver) context->solver->release();
+        if (context->tape) context->tape->release();
         for (auto &r : context->retired) {
             cudaEventDestroy(r.done);
             cudaFree(r.memory);

@@ -9,6 +9,7 @@
 // temporaries become registers. SCI_CUDA_JIT=0 turns it off, =sync compiles before the first
 // launch, =trace reports every compile on stderr.
 #include "specialize.hpp"
+#include "gradient_kernel.cuh"
 
 #include <cuda.h>
 #include <nvrtc.h>
@@ -22,9 +23,11 @@
 #include <unordered_map>
 #include <vector>
 
-// Generated at build time from sci_math.cuh and chunk_kernel.cuh (libsci_b200/build.py).
+// Generated at build time from sci_math.cuh, chunk_kernel.cuh and gradient_kernel.cuh
+// (libsci_b200/build.py).
 extern const char *const sci_embedded_math;
 extern const char *const sci_embedded_kernel;
+extern const char *const sci_embedded_gradient;
 
 namespace sci_cuda {
 
@@ -65,8 +68,10 @@ namespace sci_cuda {
             return key;
         }
 
-        // The instantiation of chunk_stream<T, Baked<SciBaked>, MODE> for one chunk.
+        // The instantiation of chunk_stream<T, Baked<SciBaked>, MODE> for one chunk, or of
+        // gradient_stream<T, Baked<SciBaked>, MODE> for a chunk in value form (the gradient modes).
         std::string program_of(const sci_chunk &chunk, int mode, std::string &name) {
+            const bool gradient = mode == kGradRecompute || mode == kGradRecord || mode == kGradReplay;
             const bool contract = mode == kDot;
             const int length = contract ? chunk.length - 1 : chunk.length;
             int dot_left = kNone, dot_right = kNone;
@@ -74,7 +79,8 @@ namespace sci_cuda {
                 dot_left = chunk.instructions[chunk.length - 1].sources[0];
                 dot_right = chunk.instructions[chunk.length - 1].sources[1];
             }
-            std::string src = "#include \"chunk_kernel.cuh\"\nstruct SciBaked {\n";
+            std::string src = gradient ? "#include \"gradient_kernel.cuh\"\nstruct SciBaked {\n"
+                                       : "#include \"chunk_kernel.cuh\"\nstruct SciBaked {\n";
             char line[256];
             std::snprintf(line, sizeof(line),
                           "  static constexpr int length = %d, arguments = %d, temporaries = %d, result = %d,"
@@ -92,8 +98,8 @@ namespace sci_cuda {
             if (stored == 0) src += "{0, 255, 255, 255, 255}";
             src += "};\n};\n";
             const char *type = chunk.precision == SCI_PRECISION_WIDE ? "double" : "float";
-            name = std::string("&sci_cuda::chunk_stream<") + type + ", sci_cuda::Baked<SciBaked>, " +
-                   std::to_string(mode) + ">";
+            name = std::string(gradient ? "&sci_cuda::gradient_stream<" : "&sci_cuda::chunk_stream<") + type +
+                   ", sci_cuda::Baked<SciBaked>, " + std::to_string(mode) + ">";
             return src;
         }
 
@@ -174,10 +180,10 @@ namespace sci_cuda {
                 entry.state = Entry::kFailed;
                 std::string name;
                 const std::string source = program_of(job.chunk, job.mode, name);
-                const char *headers[] = {sci_embedded_math, sci_embedded_kernel};
-                const char *names[] = {"sci_math.cuh", "chunk_kernel.cuh"};
+                const char *headers[] = {sci_embedded_math, sci_embedded_kernel, sci_embedded_gradient};
+                const char *names[] = {"sci_math.cuh", "chunk_kernel.cuh", "gradient_kernel.cuh"};
                 nvrtcProgram program;
-                if (nvrtcCreateProgram(&program, source.c_str(), "sci_specialized.cu", 2, headers, names) != NVRTC_SUCCESS)
+                if (nvrtcCreateProgram(&program, source.c_str(), "sci_specialized.cu", 3, headers, names) != NVRTC_SUCCESS)
                     return entry;
                 nvrtcAddNameExpression(program, name.c_str());
                 const char *options[] = {"-default-device", "-arch=sm_100a", "-std=c++17", "-lineinfo",

@@ -148,6 +148,30 @@ class Device:
         return float(expr.dtype.type(value))  # static_cast<element>(device->reduce(...)) (expression.hpp:198)
 
 
+    def gradient(self, expression, wrt, seed: float = 1.0, stored: bool = False):
+        """sci::gradient (new; the reference has none): for L = seed * sum(expression), returns
+        (sum, [dL/dw for w in wrt]) with each gradient a DeviceArray shaped like w. stored=True runs
+        the temporary-storing comparison form instead of the recomputing adjoint."""
+        expr = C._operand(expression, None)
+        chunk = C.record_reduce(expr)
+        if not chunk.valid():
+            raise SciCudaError(1, "expression outgrew the 64-entry chunk")
+        wanted = {int(w.pointer): i for i, w in enumerate(wrt)}
+        grads = [self.empty(w.count, w.dtype) for w in wrt]
+        slots = (ctypes.c_void_p * max(1, chunk.arguments))()
+        for a in range(chunk.arguments):
+            pointer = int(chunk.inputs[a] or 0)
+            if pointer in wanted:
+                slots[a] = grads[wanted[pointer]].pointer
+        for i, w in enumerate(wrt):
+            if not any(int(chunk.inputs[a] or 0) == int(w.pointer) for a in range(chunk.arguments)):
+                grads[i].upload(np.zeros(w.count, w.dtype))  # L does not depend on w
+        value = ctypes.c_double()
+        check(lib.sci_cuda_gradient(self.handle, ctypes.byref(chunk), expr.count, seed, slots, ctypes.byref(value),
+                                    1 if stored else 0), self.handle)
+        return value.value, grads
+
+
 class DeviceArray:
     """A one-dimensional array in this device's memory."""
 

@@ -58,6 +58,8 @@ def _load() -> ctypes.CDLL:
         "sci_cuda_product": (ctypes.c_int, [c_ctx, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64]),
     }
+    sig["sci_cuda_gradient"] = (ctypes.c_int, [c_ctx, P(ChunkStruct), ctypes.c_uint64, ctypes.c_double,
+                                               P(ctypes.c_void_p), P(ctypes.c_double), ctypes.c_uint32])
     optional = {}
     sig["sci_cuda_factor"] = (ctypes.c_int, [c_ctx, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_uint64])
