@@ -182,7 +182,7 @@ int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uint32_t refin
  * the function the device computes: forward values are bit-identical to sci_cuda_execute's, partial
  * derivatives are evaluated in double and adjoints accumulate in double before one rounding.
  * Conventions: d|x| at 0 is 0; minimum / maximum pass the adjoint to the operand they returned;
- * a zero adjoint passes nothing back. `form`: */
+ * a zero adjoint passes nothing back. Waits. `form`: */
 enum {
     SCI_GRADIENT_RECOMPUTE = 0, /* one pass: forward values recomputed in registers, reverse walk, no tape */
     SCI_GRADIENT_STORED = 1     /* the plain comparison form: a forward pass stores every value of the chunk
@@ -191,6 +191,24 @@ enum {
 };
 int sci_cuda_gradient(sci_cuda_context *context, const sci_chunk *chunk, uint64_t count, double seed,
                       void *const *gradients, double *value, uint32_t form);
+/* No counterpart in the reference. The adjoints of sci_cuda_product (linear::product): for
+ * C = left * right (rows x depth times depth x columns) and upstream = dL/dC (rows x columns),
+ * left_gradient = upstream * right^T (rows x depth) and right_gradient = left^T * upstream
+ * (depth x columns), two products in `mode` with the transposed operands read in place. Either
+ * gradient may be null. Queued. */
+int sci_cuda_product_gradient(sci_cuda_context *context, uint32_t precision, uint32_t mode, const void *left,
+                              const void *right, const void *upstream, void *left_gradient, void *right_gradient,
+                              uint64_t rows, uint64_t columns, uint64_t depth);
+/* No counterpart in the reference. The adjoints of sci_cuda_solve (linear::solve): for
+ * X = matrix^-1 right and upstream = dL/dX (order x width), right_gradient = lambda = matrix^-T upstream
+ * and matrix_gradient = -lambda X^T (order x order). One factorisation serves both solves: the
+ * transposed solve runs the substitutions through U^T and L^T of the same factors, then P^T. X is
+ * written to `solution` when it is not null; either gradient may be null. `refine` as for
+ * sci_cuda_solve, applied to both solves; `report` receives the larger of the two backward errors and
+ * the iterations of both. Waits. order <= 8192. */
+int sci_cuda_solve_gradient(sci_cuda_context *context, uint32_t precision, uint32_t refine, const void *matrix,
+                            const void *right, const void *upstream, void *solution, void *matrix_gradient,
+                            void *right_gradient, uint64_t order, uint64_t width, sci_solve_report *report);
 
 /* No counterpart in the reference. The same reduction for callers that may not allocate device
  * memory (a host framework that owns the GPU heap through its own pool, a plugin inside one, a

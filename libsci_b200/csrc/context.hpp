@@ -141,6 +141,15 @@ namespace sci_cuda {
     template <typename T>
     int simt_gemm(Context &ctx, const T *a, unsigned long long lda, const T *b, unsigned long long ldb, T *c,
                   unsigned long long ldc, unsigned long long m, unsigned long long n, unsigned long long k, bool subtract);
+    // The same with transposed operands read in place: a_t means A is stored k x m (pitch lda), b_t
+    // that B is stored n x k (pitch ldb).
+    int tensor_gemm_t(Context &ctx, int terms, const float *a, unsigned long long lda, bool a_t, const float *b,
+                      unsigned long long ldb, bool b_t, float *c, unsigned long long ldc, unsigned long long m,
+                      unsigned long long n, unsigned long long k, bool subtract);
+    template <typename T>
+    int simt_gemm_t(Context &ctx, const T *a, unsigned long long lda, bool a_t, const T *b, unsigned long long ldb, bool b_t,
+                    T *c, unsigned long long ldc, unsigned long long m, unsigned long long n, unsigned long long k,
+                    bool subtract);
 
     // Validates a chunk before anything is launched: counts, codes, and every value id in range.
     int validate(Context &ctx, const sci_chunk *chunk, bool reducing);

@@ -691,7 +691,8 @@ namespace sci_cuda {
         template <typename T> constexpr size_t apply_shared_bytes() {
             return sizeof(T) * (kApplyRows * kSolveBlock + kSolveBlock * 32);
         }
-        template <typename T, bool upper>
+        // transposed: apply inv^T instead (the blocks of U^T and L^T in the transposed solve).
+        template <typename T, bool upper, bool transposed = false>
         __global__ void __launch_bounds__(kApplyRows * 32) apply_inverse(const T *inv, unsigned long long s, int size,
                                                                          const T *x, T *y, unsigned long long width) {
             constexpr int B = kSolveBlock, threads = kApplyRows * 32;
@@ -703,7 +704,10 @@ namespace sci_cuda {
             constexpr int LM = kApplyRows * B / threads, LX = B * 32 / threads;
             T rm[LM], rx[LX];  // every global load of the thread is issued before the first shared store
 #pragma unroll
-            for (int u = 0; u < LM; ++u) rm[u] = inv[r0 * B + threadIdx.x + u * threads];
+            for (int u = 0; u < LM; ++u) {
+                const int i = threadIdx.x + u * threads, row = i / B, k = i % B;
+                rm[u] = transposed ? inv[k * B + r0 + row] : inv[(r0 + row) * B + k];
+            }
 #pragma unroll
             for (int u = 0; u < LX; ++u) {
                 const int i = threadIdx.x + u * threads, k = i / 32, col = i % 32;
@@ -729,7 +733,8 @@ namespace sci_cuda {
         template <typename T> constexpr size_t skinny_shared_bytes() {
             return sizeof(T) * (kSkinnyRows * (kSolveBlock + 1) + kSolveBlock * 32);
         }
-        template <typename T>
+        // transposed: A is stored k x m (pitch lda) and read in place.
+        template <typename T, bool transposed = false>
         __global__ void __launch_bounds__(256) skinny_update(const T *a, unsigned long long lda, const T *b,
                                                              unsigned long long ldb, T *c, unsigned long long ldc,
                                                              unsigned long long m, int w, int k) {
@@ -742,8 +747,9 @@ namespace sci_cuda {
             T ra[LA], rb[LB];  // every global load of the thread is issued before the first shared store
 #pragma unroll
             for (int u = 0; u < LA; ++u) {
-                const int i = threadIdx.x + u * 256, row = i / B, q = i % B;
-                ra[u] = (m0 + row < m && q < k) ? a[(m0 + row) * lda + q] : T(0);
+                const int i = threadIdx.x + u * 256;
+                const int row = transposed ? i % kSkinnyRows : i / B, q = transposed ? i / kSkinnyRows : i % B;
+                ra[u] = (m0 + row < m && q < k) ? (transposed ? a[q * lda + m0 + row] : a[(m0 + row) * lda + q]) : T(0);
             }
 #pragma unroll
             for (int u = 0; u < LB; ++u) {
@@ -753,7 +759,8 @@ namespace sci_cuda {
 #pragma unroll
             for (int u = 0; u < LA; ++u) {
                 const int i = threadIdx.x + u * 256;
-                as[(i / B) * P + i % B] = ra[u];
+                const int row = transposed ? i % kSkinnyRows : i / B, q = transposed ? i / kSkinnyRows : i % B;
+                as[row * P + q] = ra[u];
             }
 #pragma unroll
             for (int u = 0; u < LB; ++u) bs[threadIdx.x + u * 256] = rb[u];
@@ -938,14 +945,18 @@ namespace sci_cuda {
             return ctx.check(cudaGetLastError(), "launching the substitution");
         }
 
-        // C -= A B for the substitution: the skinny kernel when B has at most 32 columns.
-        template <typename T>
+        // C -= A B for the substitution (k <= kSolveBlock), 32 columns of B per launch of the skinny
+        // kernel; transposed: A is stored k x m (pitch lda).
+        template <typename T, bool transposed = false>
         int substitution_update(Context &ctx, const T *a, unsigned long long lda, const T *b, T *c, unsigned long long m,
                                 unsigned long long width, int k) {
             if (m == 0) return SCI_CUDA_OK;
-            if (width > 32) return update<T>(ctx, a, lda, b, width, c, width, m, width, static_cast<unsigned long long>(k));
-            skinny_update<T><<<static_cast<unsigned>((m + kSkinnyRows - 1) / kSkinnyRows), 256, skinny_shared_bytes<T>(),
-                               ctx.stream>>>(a, lda, b, width, c, width, m, static_cast<int>(width), k);
+            for (unsigned long long c0 = 0; c0 < width; c0 += 32) {
+                const int w = static_cast<int>(std::min<unsigned long long>(32, width - c0));
+                skinny_update<T, transposed><<<static_cast<unsigned>((m + kSkinnyRows - 1) / kSkinnyRows), 256,
+                                               skinny_shared_bytes<T>(), ctx.stream>>>(a, lda, b + c0, width, c + c0, width,
+                                                                                       m, w, k);
+            }
             return SCI_CUDA_OK;
         }
 
@@ -962,8 +973,8 @@ namespace sci_cuda {
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, apply_smem);
             cudaFuncSetAttribute(reinterpret_cast<const void *>(&apply_inverse<T, true>),
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, apply_smem);
-            cudaFuncSetAttribute(reinterpret_cast<const void *>(&skinny_update<T>), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(skinny_shared_bytes<T>()));
+            cudaFuncSetAttribute(reinterpret_cast<const void *>(&skinny_update<T, false>),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(skinny_shared_bytes<T>()));
             constexpr unsigned long long block_elements = 1ull * kSolveBlock * kSolveBlock;
             for (unsigned long long s = 0; s < n; s += kSolveBlock) {
                 const int size = static_cast<int>(std::min<unsigned long long>(kSolveBlock, n - s));
@@ -985,6 +996,76 @@ namespace sci_cuda {
                 if (int code = substitution_update<T>(ctx, lu + us, n, x + us * width, y, us, width, size)) return code;
             }
             return ctx.check(cudaGetLastError(), "launching the substitution");
+        }
+
+        // x (n x width; holds the right-hand side on entry) := L^-T U^-T x, the transposed system's
+        // substitutions with the same factors and inverses: forward through U^T (the transposed
+        // inverses of U's diagonal blocks, the updates reading U's rows in place), then back through L^T.
+        // P^T is left to the caller (A^T = U^T L^T P). y (n x width) is scratch.
+        template <typename T>
+        int substitute_inverse_transposed(Context &ctx, const T *lu, const T *inv, unsigned long long n, T *x, T *y,
+                                          unsigned long long width) {
+            const unsigned column_groups = static_cast<unsigned>((width + 31) / 32);
+            const int apply_smem = static_cast<int>(apply_shared_bytes<T>());
+            cudaFuncSetAttribute(reinterpret_cast<const void *>(&apply_inverse<T, false, true>),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, apply_smem);
+            cudaFuncSetAttribute(reinterpret_cast<const void *>(&apply_inverse<T, true, true>),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, apply_smem);
+            cudaFuncSetAttribute(reinterpret_cast<const void *>(&skinny_update<T, true>),
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(skinny_shared_bytes<T>()));
+            constexpr unsigned long long block_elements = 1ull * kSolveBlock * kSolveBlock;
+            for (unsigned long long s = 0; s < n; s += kSolveBlock) {
+                const int size = static_cast<int>(std::min<unsigned long long>(kSolveBlock, n - s));
+                const dim3 grid(static_cast<unsigned>((size + kApplyRows - 1) / kApplyRows), column_groups);
+                // (U_ss^-1)^T is lower triangular
+                apply_inverse<T, false, true><<<grid, kApplyRows * 32, apply_smem, ctx.stream>>>(
+                        inv + (2 * (s / kSolveBlock) + 1) * block_elements, s, size, x, y, width);
+                const unsigned long long below = s + size;
+                // x[below] -= U[s, below]^T y[s]
+                if (int code = substitution_update<T, true>(ctx, lu + s * n + below, n, y + s * width, x + below * width,
+                                                            n - below, width, size))
+                    return code;
+            }
+            const unsigned long long last = (n - 1) / kSolveBlock * kSolveBlock;
+            for (long long s = static_cast<long long>(last); s >= 0; s -= kSolveBlock) {
+                const unsigned long long us = static_cast<unsigned long long>(s);
+                const int size = static_cast<int>(std::min<unsigned long long>(kSolveBlock, n - us));
+                const dim3 grid(static_cast<unsigned>((size + kApplyRows - 1) / kApplyRows), column_groups);
+                // (L_ss^-1)^T is upper triangular
+                apply_inverse<T, true, true><<<grid, kApplyRows * 32, apply_smem, ctx.stream>>>(
+                        inv + 2 * (us / kSolveBlock) * block_elements, us, size, y, x, width);
+                // y[0, us) -= L[us, 0:us)^T x[us]
+                if (int code = substitution_update<T, true>(ctx, lu + us * n, n, x + us * width, y, us, width, size))
+                    return code;
+            }
+            return ctx.check(cudaGetLastError(), "launching the transposed substitution");
+        }
+
+        // x[rows[i]][:] (+)= z[i][:]: P^T z, added into a double accumulator or stored.
+        template <typename S, typename D, bool accumulate>
+        __global__ void scatter_rows(const S *z, D *x, const unsigned *rows, unsigned long long n, unsigned long long width) {
+            const unsigned long long total = n * width;
+            for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < total; i += 256ull * gridDim.x) {
+                const unsigned long long row = i / width, column = i % width;
+                D &out = x[static_cast<unsigned long long>(rows[row]) * width + column];
+                if (accumulate) out += static_cast<D>(z[i]);
+                else out = static_cast<D>(z[i]);
+            }
+        }
+
+        // out (n x n) = in^T, 32 x 32 tiles through shared memory.
+        template <typename T> __global__ void transpose_square(const T *in, T *out, unsigned long long n) {
+            __shared__ T tile[32][33];
+            const unsigned long long r0 = blockIdx.y * 32ull, c0 = blockIdx.x * 32ull;
+            for (unsigned j = threadIdx.y; j < 32; j += 8) {
+                const unsigned long long r = r0 + j, c = c0 + threadIdx.x;
+                if (r < n && c < n) tile[j][threadIdx.x] = in[r * n + c];
+            }
+            __syncthreads();
+            for (unsigned j = threadIdx.y; j < 32; j += 8) {
+                const unsigned long long r = c0 + j, c = r0 + threadIdx.x;
+                if (r < n && c < n) out[r * n + c] = tile[threadIdx.x][j];
+            }
         }
 
         // rows[] (device) from the exchanges of factor_device.
@@ -1082,6 +1163,32 @@ namespace {
         return SCI_CUDA_OK;
     }
 
+    // The refinement loop for a x = b (a n x n, b and x n x width, double): x = 0, r = b; repeat
+    // { x += correct(r); r = b - a x in FP64 } until the normwise backward error is at most 1e-15 or
+    // stops halving, at most 30 corrections. correct(r, x) adds the FP32 correction for residual r into x.
+    template <class Correct>
+    int refine_loop(Context &ctx, const double *a, const double *b, double *x, double *r, double *sums, double *norms,
+                    unsigned long long n, unsigned long long width, Correct correct, double &berr, int &iterations) {
+        double a_norm = 0.0;
+        std::vector<double> b_norm;
+        if (int code = norms_of(ctx, a, b, sums, norms, n, width, a_norm, b_norm)) return code;
+        cudaMemsetAsync(x, 0, n * width * 8, ctx.stream);
+        constexpr int kMaxIterations = 30;
+        double previous = INFINITY;
+        berr = INFINITY;
+        iterations = 0;
+        const double *residual = b;  // the first correction solves for b itself
+        while (iterations < kMaxIterations) {
+            if (int code = correct(residual, x)) return code;
+            ++iterations;
+            if (int code = backward_error(ctx, a, b, x, r, sums, norms, n, width, a_norm, b_norm.data(), berr)) return code;
+            residual = r;
+            if (!(berr > 1e-15) || !(berr < 0.5 * previous)) break;
+            previous = berr;
+        }
+        return SCI_CUDA_OK;
+    }
+
 } // namespace
 
 extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uint32_t refine, const void *matrix,
@@ -1167,28 +1274,151 @@ extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uin
     if (int code = factor_device<float>(*context, lu, n, piv, moved, true, true)) return code;
     if (int code = invert_diagonal<float>(*context, lu, n, inv)) return code;
     if (int code = row_order(*context, piv, rows, n)) return code;
-    double a_norm = 0.0;
-    std::vector<double> b_norm;
-    if (int code = norms_of(*context, a, b, sums, norms, n, width, a_norm, b_norm)) return code;
-    cudaMemsetAsync(x, 0, nw * 8, context->stream);
-
-    double previous = INFINITY, berr = INFINITY;
-    int iterations = 0;
-    constexpr int kMaxIterations = 30;
-    const double *residual = b;  // the first correction solves for b itself
-    while (iterations < kMaxIterations) {
+    auto correct = [&](const double *residual, double *xx) -> int {
         permute<double, float>(*context, residual, d, rows, n, width);
         if (int code = substitute_inverse<float>(*context, lu, inv, n, d, y, width)) return code;
-        widen_add<<<blocks_for(nw, sms), 256, 0, context->stream>>>(d, x, nw);
-        ++iterations;
-        if (int code = backward_error(*context, a, b, x, r, sums, norms, n, width, a_norm, b_norm.data(), berr)) return code;
-        residual = r;
-        if (!(berr > 1e-15) || !(berr < 0.5 * previous)) break;
-        previous = berr;
-    }
+        widen_add<<<blocks_for(nw, sms), 256, 0, context->stream>>>(d, xx, nw);
+        return SCI_CUDA_OK;
+    };
+    double berr = 0.0;
+    int iterations = 0;
+    if (int code = refine_loop(*context, a, b, x, r, sums, norms, n, width, correct, berr, iterations)) return code;
     if (report) {
         report->backward_error = berr;
         report->iterations = iterations;
+    }
+    return SCI_CUDA_OK;
+}
+
+namespace {
+
+    // The plain form of the solve adjoint in the element type T: factor a copy of A, X = A^-1 B, then
+    // lambda = A^-T G with the same factors (substitutions through U^T and L^T, then P^T), and
+    // d A = -lambda X^T.
+    template <typename T>
+    int solve_gradient_plain(Context &ctx, Carve &carve, const T *a, const T *b, const T *g, T *x, T *dA, T *dB,
+                             long long *piv, Movement *moved, unsigned *rows, unsigned long long n, unsigned long long width) {
+        const unsigned long long nw = n * width;
+        T *lu = carve.take<T>(n * n);
+        T *inv = carve.take<T>(inverse_elements(n));
+        T *y = carve.take<T>(nw);
+        T *z = carve.take<T>(nw);
+        T *lambda = dB ? dB : carve.take<T>(nw);
+        cudaMemcpyAsync(lu, a, n * n * sizeof(T), cudaMemcpyDeviceToDevice, ctx.stream);
+        if (int code = factor_device<T>(ctx, lu, n, piv, moved, sizeof(T) == 4, sizeof(T) == 4)) return code;
+        if (int code = invert_diagonal<T>(ctx, lu, n, inv)) return code;
+        if (int code = row_order(ctx, piv, rows, n)) return code;
+        permute<T, T>(ctx, b, x, rows, n, width);
+        if constexpr (sizeof(T) == 8) {
+            if (int code = substitute_device<T>(ctx, lu, n, x, width)) return code;
+        } else {
+            if (int code = substitute_inverse<T>(ctx, lu, inv, n, x, y, width)) return code;
+        }
+        cudaMemcpyAsync(z, g, nw * sizeof(T), cudaMemcpyDeviceToDevice, ctx.stream);
+        if (int code = substitute_inverse_transposed<T>(ctx, lu, inv, n, z, y, width)) return code;
+        scatter_rows<T, T, false><<<blocks_for(nw, ctx.sms), 256, 0, ctx.stream>>>(z, lambda, rows, n, width);
+        if (dA) {
+            cudaMemsetAsync(dA, 0, n * n * sizeof(T), ctx.stream);
+            if (int code = simt_gemm_t<T>(ctx, lambda, width, false, x, width, true, dA, n, n, n, width, true)) return code;
+        }
+        return ctx.check(cudaGetLastError(), "launching the solve adjoint");
+    }
+
+} // namespace
+
+extern "C" int sci_cuda_solve_gradient(sci_cuda_context *context, uint32_t precision, uint32_t refine, const void *matrix,
+                                       const void *right, const void *upstream, void *solution, void *matrix_gradient,
+                                       void *right_gradient, uint64_t order, uint64_t width, sci_solve_report *report) {
+    if (!context) return SCI_CUDA_ERROR_INVALID;
+    std::lock_guard<std::recursive_mutex> lock(context->guard);
+    if (precision > SCI_PRECISION_WIDE || refine > SCI_REFINE_FP64)
+        return context->fail(SCI_CUDA_ERROR_INVALID, "unknown precision %u or refinement %u", precision, refine);
+    if (refine == SCI_REFINE_FP64 && precision != SCI_PRECISION_WIDE)
+        return context->fail(SCI_CUDA_ERROR_INVALID, "FP64 refinement needs double operands");
+    if (report) std::memset(report, 0, sizeof(*report));
+    if (order == 0 || width == 0) return SCI_CUDA_OK;
+    if (!matrix || !right || !upstream) return context->fail(SCI_CUDA_ERROR_INVALID, "null operand");
+    if (order > kPanelRows) return context->fail(SCI_CUDA_ERROR_UNSUPPORTED, "solve: order %llu above %llu",
+                                                 static_cast<unsigned long long>(order), kPanelRows);
+    cudaSetDevice(context->device);
+    const unsigned long long n = order, nw = order * width;
+    const size_t element = precision == SCI_PRECISION_WIDE ? 8 : 4;
+    // everything either form carves, generously: matrices, inverses, right-hand-side blocks, norms
+    const unsigned long long need = n * n * (8 + element) + inverse_elements(n) * element + nw * 8 * 10 + n * 32 +
+                                    sizeof(Movement) + width * 16 + 16384;
+    if (int code = context->check(context->solver->reserve(need), "reserving the solver workspace")) return code;
+    Carve carve{static_cast<unsigned char *>(context->solver->memory)};
+    long long *piv = carve.take<long long>(n);
+    Movement *moved = carve.take<Movement>(1);
+    unsigned *rows = carve.take<unsigned>(n);
+
+    if (refine == SCI_REFINE_NONE) {
+        int code;
+        if (precision == SCI_PRECISION_WIDE) {
+            double *x = solution ? static_cast<double *>(solution) : carve.take<double>(nw);
+            code = solve_gradient_plain<double>(*context, carve, static_cast<const double *>(matrix),
+                                                static_cast<const double *>(right), static_cast<const double *>(upstream), x,
+                                                static_cast<double *>(matrix_gradient), static_cast<double *>(right_gradient),
+                                                piv, moved, rows, n, width);
+        } else {
+            float *x = solution ? static_cast<float *>(solution) : carve.take<float>(nw);
+            code = solve_gradient_plain<float>(*context, carve, static_cast<const float *>(matrix),
+                                               static_cast<const float *>(right), static_cast<const float *>(upstream), x,
+                                               static_cast<float *>(matrix_gradient), static_cast<float *>(right_gradient),
+                                               piv, moved, rows, n, width);
+        }
+        if (!code) code = context->drain();
+        return code;
+    }
+
+    // FP32 factorisation shared by both solves; FP64 residuals and updates.
+    const double *a = static_cast<const double *>(matrix);
+    const double *b = static_cast<const double *>(right);
+    const double *g = static_cast<const double *>(upstream);
+    double *x = solution ? static_cast<double *>(solution) : carve.take<double>(nw);
+    double *lambda = right_gradient ? static_cast<double *>(right_gradient) : carve.take<double>(nw);
+    float *lu = carve.take<float>(n * n);
+    float *inv = carve.take<float>(inverse_elements(n));
+    double *at = carve.take<double>(n * n);
+    float *y = carve.take<float>(nw);
+    float *d = carve.take<float>(nw);
+    double *r = carve.take<double>(nw);
+    double *sums = carve.take<double>(n);
+    double *norms = carve.take<double>(2 * width);
+    const int sms = context->sms;
+
+    narrow<<<blocks_for(n * n, sms), 256, 0, context->stream>>>(a, lu, n * n);
+    if (int code = factor_device<float>(*context, lu, n, piv, moved, true, true)) return code;
+    if (int code = invert_diagonal<float>(*context, lu, n, inv)) return code;
+    if (int code = row_order(*context, piv, rows, n)) return code;
+    auto forward = [&](const double *residual, double *xx) -> int {
+        permute<double, float>(*context, residual, d, rows, n, width);
+        if (int code = substitute_inverse<float>(*context, lu, inv, n, d, y, width)) return code;
+        widen_add<<<blocks_for(nw, sms), 256, 0, context->stream>>>(d, xx, nw);
+        return SCI_CUDA_OK;
+    };
+    // A^T lambda = G: A^T = U^T L^T P, so lambda = P^T (L^-T U^-T G), with the same factors
+    auto transposed = [&](const double *residual, double *xx) -> int {
+        narrow<<<blocks_for(nw, sms), 256, 0, context->stream>>>(residual, d, nw);
+        if (int code = substitute_inverse_transposed<float>(*context, lu, inv, n, d, y, width)) return code;
+        scatter_rows<float, double, true><<<blocks_for(nw, sms), 256, 0, context->stream>>>(d, xx, rows, n, width);
+        return SCI_CUDA_OK;
+    };
+    double berr_x = 0.0, berr_l = 0.0;
+    int it_x = 0, it_l = 0;
+    if (int code = refine_loop(*context, a, b, x, r, sums, norms, n, width, forward, berr_x, it_x)) return code;
+    transpose_square<double><<<dim3(static_cast<unsigned>((n + 31) / 32), static_cast<unsigned>((n + 31) / 32)), dim3(32, 8), 0,
+                               context->stream>>>(a, at, n);
+    if (int code = refine_loop(*context, at, g, lambda, r, sums, norms, n, width, transposed, berr_l, it_l)) return code;
+    if (matrix_gradient) {
+        double *dA = static_cast<double *>(matrix_gradient);
+        cudaMemsetAsync(dA, 0, n * n * 8, context->stream);
+        if (int code = simt_gemm_t<double>(*context, lambda, width, false, x, width, true, dA, n, n, n, width, true)) return code;
+    }
+    if (int code = context->drain()) return code;
+    if (report) {
+        report->backward_error = std::max(berr_x, berr_l);
+        report->iterations = it_x + it_l;
     }
     return SCI_CUDA_OK;
 }

@@ -307,11 +307,14 @@ namespace sci_cuda {
         // 128 x 128 output tile per 256-thread block, 8 x 8 per thread, K slices of 8 through shared
         // memory. T = float accumulates in float, T = double in double (the reference's
         // multiply<type> accumulates in the element type, dispatch.cpp:171-224).
+        // Element (r, q) of A is a[r * a_row + q * a_col] and element (q, j) of B is b[q * b_row + j * b_col],
+        // so a transposed operand is read in place.
         template <typename T>
-        __global__ void __launch_bounds__(256) simt_product(const T *__restrict__ a, unsigned long long lda,
-                                                            const T *__restrict__ b, unsigned long long ldb, T *__restrict__ c,
-                                                            unsigned long long ldc, unsigned long long m, unsigned long long n,
-                                                            unsigned long long k, int subtract) {
+        __global__ void __launch_bounds__(256) simt_product(const T *__restrict__ a, unsigned long long a_row,
+                                                            unsigned long long a_col, const T *__restrict__ b,
+                                                            unsigned long long b_row, unsigned long long b_col,
+                                                            T *__restrict__ c, unsigned long long ldc, unsigned long long m,
+                                                            unsigned long long n, unsigned long long k, int subtract) {
             constexpr int BM = 128, BN = 128, BK = 8, TM = 8, TN = 8, LA = BM * BK / 256, LB = BK * BN / 256;
             __shared__ T as[BK][BM + 4];
             __shared__ T bs[BK][BN + 4];
@@ -332,13 +335,13 @@ namespace sci_cuda {
                 for (int u = 0; u < LA; ++u) {
                     const int i = threadIdx.x + u * 256, r = i / BK, q = i % BK;
                     const unsigned long long gr = m0 + r, gk = k0 + q;
-                    ra[u] = (gr < m && gk < k) ? a[gr * lda + gk] : T(0);
+                    ra[u] = (gr < m && gk < k) ? a[gr * a_row + gk * a_col] : T(0);
                 }
 #pragma unroll
                 for (int u = 0; u < LB; ++u) {
                     const int i = threadIdx.x + u * 256, q = i / BN, col = i % BN;
                     const unsigned long long gk = k0 + q, gc = n0 + col;
-                    rb[u] = (gk < k && gc < n) ? b[gk * ldb + gc] : T(0);
+                    rb[u] = (gk < k && gc < n) ? b[gk * b_row + gc * b_col] : T(0);
                 }
             };
             fetch(0);
@@ -415,10 +418,18 @@ namespace sci_cuda {
     } // namespace
 
     // C (m x n, row pitch ldc) = or -= A (m x k, pitch lda) * B (k x n, pitch ldb) on the tensor cores, each
-    // operand split into `terms` bf16 parts (1, 2 or 3).
+    // operand split into `terms` bf16 parts (1, 2 or 3). a_t: A is stored transposed (k x m, pitch lda);
+    // b_t: B is stored transposed (n x k, pitch ldb). The conversion to K-major bf16 terms absorbs the
+    // transposition, so the tensor-core kernel is the same either way.
     int tensor_gemm(Context &ctx, int terms, const float *a, unsigned long long lda, const float *b,
                     unsigned long long ldb, float *c, unsigned long long ldc, unsigned long long m, unsigned long long n,
                     unsigned long long k, bool subtract) {
+        return tensor_gemm_t(ctx, terms, a, lda, false, b, ldb, false, c, ldc, m, n, k, subtract);
+    }
+
+    int tensor_gemm_t(Context &ctx, int terms, const float *a, unsigned long long lda, bool a_t, const float *b,
+                      unsigned long long ldb, bool b_t, float *c, unsigned long long ldc, unsigned long long m,
+                      unsigned long long n, unsigned long long k, bool subtract) {
         if (terms < 1 || terms > 3) return ctx.fail(SCI_CUDA_ERROR_INVALID, "bf16 terms %d", terms);
         const unsigned long long kp = (k + kBK - 1) / kBK * kBK;
         if (kp > (1ull << 31) || m > (1ull << 31) || n > (1ull << 31))
@@ -432,10 +443,18 @@ namespace sci_cuda {
             at.t[q] = reinterpret_cast<__nv_bfloat16 *>(base + q * a_bytes);
             bt.t[q] = reinterpret_cast<__nv_bfloat16 *>(base + terms * a_bytes + q * b_bytes);
         }
-        const unsigned grid = static_cast<unsigned>(std::min<unsigned long long>((m * kp + 255) / 256, ctx.sms * 16ull));
-        split_rows<<<grid, 256, 0, ctx.stream>>>(a, lda, at, terms, m, k, kp);
-        const dim3 tgrid(static_cast<unsigned>((n + 31) / 32), static_cast<unsigned>((kp + 31) / 32));
-        split_transpose<<<tgrid, dim3(32, 8), 0, ctx.stream>>>(b, ldb, bt, terms, k, n, kp);
+        auto rows_of = [&](const float *x, unsigned long long ld, Terms out, unsigned long long rows) {
+            const unsigned grid = static_cast<unsigned>(std::min<unsigned long long>((rows * kp + 255) / 256, ctx.sms * 16ull));
+            split_rows<<<grid, 256, 0, ctx.stream>>>(x, ld, out, terms, rows, k, kp);
+        };
+        auto columns_of = [&](const float *x, unsigned long long ld, Terms out, unsigned long long columns) {
+            const dim3 tgrid(static_cast<unsigned>((columns + 31) / 32), static_cast<unsigned>((kp + 31) / 32));
+            split_transpose<<<tgrid, dim3(32, 8), 0, ctx.stream>>>(x, ld, out, terms, k, columns, kp);
+        };
+        if (a_t) columns_of(a, lda, at, m);
+        else rows_of(a, lda, at, m);
+        if (b_t) rows_of(b, ldb, bt, n);
+        else columns_of(b, ldb, bt, n);
         if (int code = ctx.check(cudaGetLastError(), "launching the bf16 conversion")) return code;
 
         const unsigned bn = terms == 3 ? 128u : 256u;
@@ -460,16 +479,30 @@ namespace sci_cuda {
         return ctx.check(cudaLaunchKernel(kernel, pgrid, dim3(192), params, smem, ctx.stream), "launching the tensor product");
     }
 
-    // C (pitch ldc) = or -= A (pitch lda) * B (pitch ldb) with the plain SIMT kernel.
+    // C (pitch ldc) = or -= A (pitch lda) * B (pitch ldb) with the plain SIMT kernel; a_t / b_t as for
+    // tensor_gemm_t.
     template <typename T>
-    int simt_gemm(Context &ctx, const T *a, unsigned long long lda, const T *b, unsigned long long ldb, T *c,
-                  unsigned long long ldc, unsigned long long m, unsigned long long n, unsigned long long k, bool subtract) {
+    int simt_gemm_t(Context &ctx, const T *a, unsigned long long lda, bool a_t, const T *b, unsigned long long ldb, bool b_t,
+                    T *c, unsigned long long ldc, unsigned long long m, unsigned long long n, unsigned long long k,
+                    bool subtract) {
         const dim3 grid(static_cast<unsigned>((n + 127) / 128), static_cast<unsigned>((m + 127) / 128));
         if (grid.y > 65535) return ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "too many rows for one launch");
         if (m == 0 || n == 0) return SCI_CUDA_OK;
-        simt_product<T><<<grid, 256, 0, ctx.stream>>>(a, lda, b, ldb, c, ldc, m, n, k, subtract ? 1 : 0);
+        simt_product<T><<<grid, 256, 0, ctx.stream>>>(a, a_t ? 1ull : lda, a_t ? lda : 1ull, b, b_t ? 1ull : ldb,
+                                                      b_t ? ldb : 1ull, c, ldc, m, n, k, subtract ? 1 : 0);
         return ctx.check(cudaGetLastError(), "launching the SIMT product");
     }
+    template <typename T>
+    int simt_gemm(Context &ctx, const T *a, unsigned long long lda, const T *b, unsigned long long ldb, T *c,
+                  unsigned long long ldc, unsigned long long m, unsigned long long n, unsigned long long k, bool subtract) {
+        return simt_gemm_t<T>(ctx, a, lda, false, b, ldb, false, c, ldc, m, n, k, subtract);
+    }
+    template int simt_gemm_t<float>(Context &, const float *, unsigned long long, bool, const float *, unsigned long long,
+                                    bool, float *, unsigned long long, unsigned long long, unsigned long long,
+                                    unsigned long long, bool);
+    template int simt_gemm_t<double>(Context &, const double *, unsigned long long, bool, const double *,
+                                     unsigned long long, bool, double *, unsigned long long, unsigned long long,
+                                     unsigned long long, unsigned long long, bool);
     template int simt_gemm<float>(Context &, const float *, unsigned long long, const float *, unsigned long long, float *,
                                   unsigned long long, unsigned long long, unsigned long long, unsigned long long, bool);
     template int simt_gemm<double>(Context &, const double *, unsigned long long, const double *, unsigned long long,
@@ -505,4 +538,35 @@ extern "C" int sci_cuda_product(sci_cuda_context *context, uint32_t precision, u
                        static_cast<const float *>(left), depth,
                        static_cast<const float *>(right), columns, static_cast<float *>(output), columns, rows, columns,
                        depth, false);
+}
+
+extern "C" int sci_cuda_product_gradient(sci_cuda_context *context, uint32_t precision, uint32_t mode, const void *left,
+                                         const void *right, const void *upstream, void *left_gradient, void *right_gradient,
+                                         uint64_t rows, uint64_t columns, uint64_t depth) {
+    if (!context) return SCI_CUDA_ERROR_INVALID;
+    std::lock_guard<std::recursive_mutex> lock(context->guard);
+    if (precision > SCI_PRECISION_WIDE || mode > SCI_PRODUCT_SPLIT3_BF16)
+        return context->fail(SCI_CUDA_ERROR_INVALID, "unknown precision %u or mode %u", precision, mode);
+    if (!upstream || (left_gradient && !right) || (right_gradient && !left))
+        return context->fail(SCI_CUDA_ERROR_INVALID, "null matrix");
+    cudaSetDevice(context->device);
+    const size_t element = precision == SCI_PRECISION_WIDE ? 8 : 4;
+    // d left (rows x depth) = G (rows x columns) * right^T; d right (depth x columns) = left^T * G.
+    // An empty inner dimension (columns for d left, rows for d right) gives zeros.
+    auto one = [&](void *out, const void *a, uint64_t lda, bool a_t, const void *b, uint64_t ldb, bool b_t, uint64_t m,
+                   uint64_t n, uint64_t k) -> int {
+        if (!out || m == 0 || n == 0) return SCI_CUDA_OK;
+        if (k == 0) return context->check(cudaMemsetAsync(out, 0, m * n * element, context->stream), "zeroing a gradient");
+        if (precision == SCI_PRECISION_WIDE)
+            return simt_gemm_t<double>(*context, static_cast<const double *>(a), lda, a_t, static_cast<const double *>(b), ldb,
+                                       b_t, static_cast<double *>(out), n, m, n, k, false);
+        if (mode == SCI_PRODUCT_FP32)
+            return simt_gemm_t<float>(*context, static_cast<const float *>(a), lda, a_t, static_cast<const float *>(b), ldb,
+                                      b_t, static_cast<float *>(out), n, m, n, k, false);
+        return tensor_gemm_t(*context, mode == SCI_PRODUCT_SPLIT3_BF16 ? 3 : (mode == SCI_PRODUCT_SPLIT_BF16 ? 2 : 1),
+                             static_cast<const float *>(a), lda, a_t, static_cast<const float *>(b), ldb, b_t,
+                             static_cast<float *>(out), n, m, n, k, false);
+    };
+    if (int code = one(left_gradient, upstream, columns, false, right, columns, true, rows, depth, columns)) return code;
+    return one(right_gradient, left, depth, true, upstream, columns, false, depth, columns, rows);
 }

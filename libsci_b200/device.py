@@ -172,6 +172,31 @@ class Device:
         return value.value, grads
 
 
+    def product_gradient(self, left: "DeviceArray", right: "DeviceArray", upstream: "DeviceArray", rows: int,
+                         columns: int, depth: int, mode: int = 0):
+        """Adjoints of product (new): (upstream @ right.T, left.T @ upstream) as DeviceArrays."""
+        dtype = left.dtype
+        dl, dr = self.empty(rows * depth, dtype), self.empty(depth * columns, dtype)
+        precision = C.WIDE if dtype == np.float64 else C.SINGLE
+        check(lib.sci_cuda_product_gradient(self.handle, precision, mode, left.pointer, right.pointer, upstream.pointer,
+                                            dl.pointer, dr.pointer, rows, columns, depth), self.handle)
+        return dl, dr
+
+    def solve_gradient(self, matrix: "DeviceArray", right: "DeviceArray", upstream: "DeviceArray", order: int,
+                       width: int, refine: bool = False):
+        """Adjoints of solve (new): returns (X, dL/dmatrix, dL/dright, backward_error, iterations)."""
+        from .native import SolveReport
+
+        dtype = matrix.dtype
+        x, dm, db = self.empty(order * width, dtype), self.empty(order * order, dtype), self.empty(order * width, dtype)
+        precision = C.WIDE if dtype == np.float64 else C.SINGLE
+        report = SolveReport()
+        check(lib.sci_cuda_solve_gradient(self.handle, precision, 1 if refine else 0, matrix.pointer, right.pointer,
+                                          upstream.pointer, x.pointer, dm.pointer, db.pointer, order, width,
+                                          ctypes.byref(report)), self.handle)
+        return x, dm, db, report.backward_error, report.iterations
+
+
 class DeviceArray:
     """A one-dimensional array in this device's memory."""
 

@@ -60,6 +60,10 @@ def _load() -> ctypes.CDLL:
     }
     sig["sci_cuda_gradient"] = (ctypes.c_int, [c_ctx, P(ChunkStruct), ctypes.c_uint64, ctypes.c_double,
                                                P(ctypes.c_void_p), P(ctypes.c_double), ctypes.c_uint32])
+    sig["sci_cuda_product_gradient"] = (ctypes.c_int, [c_ctx, ctypes.c_uint32, ctypes.c_uint32] + [ctypes.c_void_p] * 5 +
+                                        [ctypes.c_uint64] * 3)
+    sig["sci_cuda_solve_gradient"] = (ctypes.c_int, [c_ctx, ctypes.c_uint32, ctypes.c_uint32] + [ctypes.c_void_p] * 6 +
+                                      [ctypes.c_uint64, ctypes.c_uint64, P(SolveReport)])
     optional = {}
     sig["sci_cuda_factor"] = (ctypes.c_int, [c_ctx, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_uint64])
