@@ -327,9 +327,161 @@ def run_solve(args) -> int:
     return 0
 
 
+def run_gradient(args) -> int:
+    """sci::gradient workloads. Chunk: L = sum(exponential(-a*a)*sin(b) + logarithm(1+c*c)), float32,
+    n = 2^26 per array, a,b,c ~ N(0,1): the recomputing adjoint against the temporary-storing one,
+    each timed on the device (inputs 256 MiB each, above L2), gradients checked against the closed
+    form in FP64. Solve: L = sum(solve(A, B)), A = G + 4096 I (4096^2, fp64), B 4096 x 64: the
+    adjoint with FP32 LU + FP64 refinement (one factorisation for the forward and the transposed
+    solve) against the plain FP64 form, both checked against numpy FP64."""
+    import torch
+
+    from libsci_b200 import chunk as C
+    from libsci_b200.device import Device
+    from libsci_b200.native import check, lib
+
+    n = 1 << 26
+    device = Device(0)
+    stream = torch.cuda.ExternalStream(device.stream)
+    rng = np.random.default_rng(0)
+    hosts = [rng.standard_normal(n, dtype=np.float32) for _ in range(3)]
+    arrays = [device.array(h) for h in hosts]
+    grads = [device.empty(n) for _ in range(3)]
+    expr = C.unary("exponential", -arrays[0].expression() * arrays[0].expression()) * C.unary("sin", arrays[1].expression()) \
+        + C.unary("logarithm", 1 + arrays[2].expression() * arrays[2].expression())
+    chunk = C.record_reduce(expr)
+    slots = (ctypes.c_void_p * 3)(*[g.pointer for g in grads])
+    peak, peak_source = measured_peaks()
+
+    def time_form(form):
+        for _ in range(args.warmup):
+            check(lib.sci_cuda_gradient(device.handle, ctypes.byref(chunk), n, 1.0, slots, None, form), device.handle)
+        device.jit_wait()
+        check(lib.sci_cuda_gradient(device.handle, ctypes.byref(chunk), n, 1.0, slots, None, form), device.handle)
+        device.synchronize()
+        times = []
+        for _ in range(args.steps):
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            check(lib.sci_cuda_gradient(device.handle, ctypes.byref(chunk), n, 1.0, slots, None, form), device.handle)
+            stop.record(stream)
+            stop.synchronize()
+            times.append(start.elapsed_time(stop))
+        return statistics.median(times)
+
+    with ClockSampler(0) as clocks:
+        ms_recompute = time_form(0)
+        ms_stored = time_form(1)
+    value = ctypes.c_double()
+    check(lib.sci_cuda_gradient(device.handle, ctypes.byref(chunk), n, 1.0, slots, ctypes.byref(value), 0), device.handle)
+    got = [g.numpy().astype(np.float64) for g in grads]
+    a64, b64, c64 = (h.astype(np.float64) for h in hosts)
+    e = np.exp(-a64 * a64)
+    want = [-2.0 * a64 * e * np.sin(b64), e * np.cos(b64), 2.0 * c64 / (1.0 + c64 * c64)]
+    errors = []
+    for g, w in zip(got, want):
+        scale = np.maximum(np.abs(w), 1e-3 * np.abs(w).max())
+        errors.append(float((np.abs(g - w) / scale).max()))
+    want_value = float(np.sum(e * np.sin(b64) + np.log1p(c64 * c64)))
+    bytes_recompute = 24.0 * n  # read a, b, c; write three gradients
+    nodes = 8
+    bytes_stored = (12.0 + 4 * nodes + 4 * nodes + 12.0 + 12.0) * n  # forward + tape out, tape + inputs in, grads out
+    chunk_result = {
+        "elements": n,
+        "recompute": {"ms": ms_recompute, "GB/s": bytes_recompute / (ms_recompute * 1e-3) / 1e9,
+                      "frac_of_peak": bytes_recompute / (ms_recompute * 1e-3) / 1e9 / peak},
+        "stored": {"ms": ms_stored, "GB/s_moved": bytes_stored / (ms_stored * 1e-3) / 1e9,
+                   "bytes_per_element": bytes_stored / n},
+        "speedup_recompute_vs_stored": ms_stored / ms_recompute,
+        "max_rel_error_vs_fp64": max(errors),
+        "value": value.value, "value_rel_error": abs(value.value - want_value) / abs(want_value),
+    }
+    for x in arrays + grads:
+        x.free()
+
+    # the solve adjoint
+    m, width = 4096, 64
+    rng = np.random.default_rng(1)
+    a = rng.standard_normal((m, m)) + m * np.eye(m)
+    b = rng.standard_normal((m, width))
+    g = np.ones((m, width))
+    da, db, dg = device.array(a.ravel()), device.array(b.ravel()), device.array(g.ravel())
+    x_out, dA_out, dB_out = device.empty(m * width, np.float64), device.empty(m * m, np.float64), device.empty(m * width, np.float64)
+    from libsci_b200.native import SolveReport
+
+    def solve_adjoint(refine):
+        report = SolveReport()
+        check(lib.sci_cuda_solve_gradient(device.handle, 1, 1 if refine else 0, da.pointer, db.pointer, dg.pointer,
+                                          x_out.pointer, dA_out.pointer, dB_out.pointer, m, width, ctypes.byref(report)),
+              device.handle)
+        return report
+
+    solve_result = {}
+    want_x = np.linalg.solve(a, b)
+    want_l = np.linalg.solve(a.T, g)
+    want_dA = -want_l @ want_x.T
+    for label, refine in (("fp32_lu_fp64_refine", True), ("fp64_plain", False)):
+        for _ in range(args.warmup):
+            solve_adjoint(refine)
+        times = []
+        for _ in range(max(3, args.steps // 4)):
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            report = solve_adjoint(refine)
+            stop.record(stream)
+            stop.synchronize()
+            times.append(start.elapsed_time(stop))
+        dA = dA_out.numpy().reshape(m, m)
+        dB = dB_out.numpy().reshape(m, width)
+        solve_result[label] = {
+            "ms": statistics.median(times), "backward_error": report.backward_error, "iterations": report.iterations,
+            "dA_rel_error": float(np.abs(dA - want_dA).max() / np.abs(want_dA).max()),
+            "dB_rel_error": float(np.abs(dB - want_l).max() / np.abs(want_l).max()),
+        }
+    solve_result["speedup_refined_vs_fp64"] = solve_result["fp64_plain"]["ms"] / solve_result["fp32_lu_fp64_refine"]["ms"]
+
+    from tests import _oracle
+
+    cpu = None
+    ref = None if args.no_cpu else _oracle.reference()
+    if ref is not None:
+        # What the reference offers for gradients: central differences through its CPU path, two
+        # Precision::wide evaluations of the chunk per input, on a 2^22-element sample.
+        sample = 1 << 22
+        base = [h[:sample].astype(np.float64) for h in hosts]
+        start = time.perf_counter()
+        for index in range(3):
+            for sign in (1.0, -1.0):
+                moved = [x.copy() for x in base]
+                moved[index] += sign * 1e-5 * np.maximum(1.0, np.abs(base[index]))
+                refs = [C.Reference(x.ctypes.data, sample, np.float64) for x in moved]
+                wide = C.record_output(C.unary("exponential", -refs[0] * refs[0]) * C.unary("sin", refs[1])
+                                       + C.unary("logarithm", 1 + refs[2] * refs[2]))
+                _oracle.execute(ref, wide, sample, np.float64)
+        seconds = time.perf_counter() - start
+        cpu = {"value": sample / seconds, "unit": "gradient elements/s", "cores": int(ref.sci_ref_threads()),
+               "kind": "reference", "sample": "central differences on libsci's CPU path: 6 Precision::wide chunk "
+                                              "evaluations over 2^22 elements"}
+    line = {"metric": "gradient speedup: recomputing adjoint vs temporary-storing adjoint", "unit": "x",
+            "value": chunk_result["speedup_recompute_vs_stored"], "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_recompute, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (adjoints in f64)", "data": "synthetic",
+            "config": {"workload": "gradient of sum(exp(-a*a)*sin(b)+log(1+c*c)), n=2^26 float32; "
+                                   "gradient of sum(solve(A,B)), A=G+4096I 4096^2 fp64, B 4096x64",
+                       "l2": "inputs 256 MiB each, above L2"},
+            "chunk": chunk_result, "solve": solve_result,
+            "roofline": {"bound": "hbm", "achieved": chunk_result["recompute"]["GB/s"], "peak": peak, "unit": "GB/s",
+                         "frac": chunk_result["recompute"]["frac_of_peak"], "traffic": None,
+                         "peak_source": peak_source},
+            "cpu_baseline": cpu, "gpu_launches": args.steps, "clocks": clocks.summary()}
+    print(json.dumps(line))
+    device.close()
+    return 0
+
+
 def main() -> int:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--workload", default="chunks", choices=["chunks", "product", "solve"])
+    parser.add_argument("--workload", default="chunks", choices=["chunks", "product", "solve", "gradient"])
     parser.add_argument("--size", type=int, default=8192)
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=20)
@@ -350,6 +502,8 @@ def main() -> int:
         return run_product(args)
     if args.workload == "solve":
         return run_solve(args)
+    if args.workload == "gradient":
+        return run_gradient(args)
 
     import torch
 

@@ -182,7 +182,8 @@ int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uint32_t refin
  * the function the device computes: forward values are bit-identical to sci_cuda_execute's, partial
  * derivatives are evaluated in double and adjoints accumulate in double before one rounding.
  * Conventions: d|x| at 0 is 0; minimum / maximum pass the adjoint to the operand they returned;
- * a zero adjoint passes nothing back. Waits. `form`: */
+ * a zero adjoint passes nothing back. Waits for the sum when `value` is not null; without it the
+ * call is only queued (errors a kernel records surface at the next sci_cuda_synchronize). `form`: */
 enum {
     SCI_GRADIENT_RECOMPUTE = 0, /* one pass: forward values recomputed in registers, reverse walk, no tape */
     SCI_GRADIENT_STORED = 1     /* the plain comparison form: a forward pass stores every value of the chunk

@@ -200,14 +200,12 @@ extern "C" int sci_cuda_gradient(sci_cuda_context *context, const sci_chunk *chu
     const int code = chunk->precision == SCI_PRECISION_WIDE
                              ? gradient<double>(*context, program, count, seed, gradients, device_value, form)
                              : gradient<float>(*context, program, count, seed, gradients, device_value, form);
-    if (code) return code;
-    if (value) {
-        if (int c = context->check(cudaMemcpyAsync(context->host_result, context->result, sizeof(double),
-                                                   cudaMemcpyDeviceToHost, context->stream),
-                                   "reading the sum"))
-            return c;
-    }
+    if (code || !value) return code;  // without a value the call is only queued
+    if (int c = context->check(cudaMemcpyAsync(context->host_result, context->result, sizeof(double),
+                                               cudaMemcpyDeviceToHost, context->stream),
+                               "reading the sum"))
+        return c;
     if (int c = context->drain()) return c;
-    if (value) *value = *context->host_result;
+    *value = *context->host_result;
     return SCI_CUDA_OK;
 }
