@@ -211,6 +211,37 @@ int sci_cuda_solve_gradient(sci_cuda_context *context, uint32_t precision, uint3
                             const void *right, const void *upstream, void *solution, void *matrix_gradient,
                             void *right_gradient, uint64_t order, uint64_t width, sci_solve_report *report);
 
+/* ---- batches ---------------------------------------------------------------------------------- */
+/* Many instances ("items") of one chunk in one persistent launch, replayed from a CUDA graph. No
+ * counterpart in the reference's API; it stands where the reference batches its dispatches into a
+ * Vulkan command buffer (src/core/drivers/vulkan/stream.cpp:71-106). Every item supplies its own
+ * inputs, output and element count; the chunk's own inputs[] are ignored. Tables are host arrays,
+ * read once at creation; the pointers in them are device memory of the context's GPU. */
+typedef struct sci_batch_items {
+    uint32_t items;
+    const void *const *inputs; /* items x chunk->arguments pointers, one row per item             */
+    void *const *outputs;      /* items pointers receiving the chunk's stored output, or null      */
+    const uint64_t *counts;    /* items element counts (0 allowed)                                  */
+    void *results;             /* device memory, items doubles: each item's reduced value (the fold
+                                  of the chunk's result), or null when the batch only stores       */
+} sci_batch_items;
+typedef struct sci_cuda_batch sci_cuda_batch;
+/* Prepares a batch: checks every item, compiles the chunk's batch kernel (NVRTC, synchronously),
+ * tunes the unit span of each item-size bucket (< 4096, < 65536, larger; cached per device, chunk
+ * signature and bucket in SCI_CUDA_TUNE_CACHE, default $HOME/.cache/sci_cuda/batch_tune.txt;
+ * SCI_CUDA_TUNE=0 skips tuning), uploads the item tables and captures the launch into a CUDA graph.
+ * The tuning launches run the batch, so outputs and results are written. A chunk may both store
+ * an output and reduce a result. Stored outputs are bit-identical to sci_cuda_execute on each item;
+ * results are folded in double like sci_cuda_reduce (in a fixed, per-item order). Waits. */
+int sci_cuda_batch_create(sci_cuda_context *context, const sci_chunk *chunk, uint32_t fold,
+                          const sci_batch_items *items, sci_cuda_batch **batch);
+/* Replays the batch's graph on the context's stream (queued). */
+int sci_cuda_batch_launch(sci_cuda_batch *batch);
+/* The unit span chosen for each of the three buckets and whether the kernel is the NVRTC instance. */
+int sci_cuda_batch_spans(const sci_cuda_batch *batch, uint32_t *spans, int32_t *specialized);
+/* Waits for the context's queued work, then frees the batch. */
+int sci_cuda_batch_destroy(sci_cuda_batch *batch);
+
 /* No counterpart in the reference. The same reduction for callers that may not allocate device
  * memory (a host framework that owns the GPU heap through its own pool, a plugin inside one, a
  * latency-critical thread where an allocation would synchronize the device). It needs no context:

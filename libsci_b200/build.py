@@ -54,10 +54,12 @@ def build(jobs: int | None = None, verbose: bool = False) -> Path:
 
     # The kernel source NVRTC specialises at run time, embedded in the library (specialize.cu).
     embedded = OBJECTS / "embedded_sources.cu"
-    embedded_sources = [SOURCES / "sci_math.cuh", SOURCES / "chunk_kernel.cuh", SOURCES / "gradient_kernel.cuh"]
+    embedded_sources = [SOURCES / "sci_math.cuh", SOURCES / "chunk_kernel.cuh", SOURCES / "gradient_kernel.cuh",
+                        SOURCES / "batch_kernel.cuh"]
     if _stale(embedded, embedded_sources):
         text = "// Generated by libsci_b200/build.py: the chunk kernel source NVRTC specialises.\n"
-        for symbol, path in zip(("sci_embedded_math", "sci_embedded_kernel", "sci_embedded_gradient"), embedded_sources):
+        symbols = ("sci_embedded_math", "sci_embedded_kernel", "sci_embedded_gradient", "sci_embedded_batch")
+        for symbol, path in zip(symbols, embedded_sources):
             body = path.read_text()
             assert ")SCIEMBED\"" not in body
             text += f'extern const char *const {symbol} = R"SCIEMBED({body})SCIEMBED";\n'

@@ -134,6 +134,22 @@ namespace sci_cuda {
         }
     }
 
+    // One code on one element, dispatched at run time.
+    template <typename T> __device__ __forceinline__ T apply_one(int code, T a, T b, T c, bool tail) {
+        switch (code) {
+#define SCI_CASE(N) \
+    case N: return apply<N>(a, b, c, tail);
+            SCI_CASE(0) SCI_CASE(1) SCI_CASE(2) SCI_CASE(3) SCI_CASE(4) SCI_CASE(5) SCI_CASE(6) SCI_CASE(7)
+            SCI_CASE(8) SCI_CASE(9) SCI_CASE(10) SCI_CASE(11) SCI_CASE(12) SCI_CASE(13) SCI_CASE(14) SCI_CASE(15)
+            SCI_CASE(16) SCI_CASE(17) SCI_CASE(18) SCI_CASE(19) SCI_CASE(20) SCI_CASE(21) SCI_CASE(22) SCI_CASE(23)
+            SCI_CASE(24) SCI_CASE(25) SCI_CASE(26) SCI_CASE(27) SCI_CASE(28) SCI_CASE(29) SCI_CASE(30) SCI_CASE(31)
+            SCI_CASE(32) SCI_CASE(33) SCI_CASE(34) SCI_CASE(35) SCI_CASE(36)
+#undef SCI_CASE
+        default:
+            return T(0);
+        }
+    }
+
     // ---- mbarrier and bulk-copy primitives (PTX ISA 8.x, sm_90+) -------------------------------
     __device__ __forceinline__ unsigned smem_address(const void *p) {
         return static_cast<unsigned>(__cvta_generic_to_shared(p));

@@ -9,6 +9,7 @@
 // temporaries become registers. SCI_CUDA_JIT=0 turns it off, =sync compiles before the first
 // launch, =trace reports every compile on stderr.
 #include "specialize.hpp"
+#include "batch_kernel.cuh"
 #include "gradient_kernel.cuh"
 
 #include <cuda.h>
@@ -23,11 +24,12 @@
 #include <unordered_map>
 #include <vector>
 
-// Generated at build time from sci_math.cuh, chunk_kernel.cuh and gradient_kernel.cuh
-// (libsci_b200/build.py).
+// Generated at build time from sci_math.cuh, chunk_kernel.cuh, gradient_kernel.cuh and
+// batch_kernel.cuh (libsci_b200/build.py).
 extern const char *const sci_embedded_math;
 extern const char *const sci_embedded_kernel;
 extern const char *const sci_embedded_gradient;
+extern const char *const sci_embedded_batch;
 
 namespace sci_cuda {
 
@@ -79,7 +81,9 @@ namespace sci_cuda {
                 dot_left = chunk.instructions[chunk.length - 1].sources[0];
                 dot_right = chunk.instructions[chunk.length - 1].sources[1];
             }
+            const bool batch = mode == kBatchMode;
             std::string src = gradient ? "#include \"gradient_kernel.cuh\"\nstruct SciBaked {\n"
+                              : batch  ? "#include \"batch_kernel.cuh\"\nstruct SciBaked {\n"
                                        : "#include \"chunk_kernel.cuh\"\nstruct SciBaked {\n";
             char line[256];
             std::snprintf(line, sizeof(line),
@@ -98,8 +102,12 @@ namespace sci_cuda {
             if (stored == 0) src += "{0, 255, 255, 255, 255}";
             src += "};\n};\n";
             const char *type = chunk.precision == SCI_PRECISION_WIDE ? "double" : "float";
-            name = std::string(gradient ? "&sci_cuda::gradient_stream<" : "&sci_cuda::chunk_stream<") + type +
-                   ", sci_cuda::Baked<SciBaked>, " + std::to_string(mode) + ">";
+            if (batch) {
+                name = std::string("&sci_cuda::batch_stream<") + type + ", sci_cuda::Baked<SciBaked>>";
+            } else {
+                name = std::string(gradient ? "&sci_cuda::gradient_stream<" : "&sci_cuda::chunk_stream<") + type +
+                       ", sci_cuda::Baked<SciBaked>, " + std::to_string(mode) + ">";
+            }
             return src;
         }
 
@@ -180,10 +188,10 @@ namespace sci_cuda {
                 entry.state = Entry::kFailed;
                 std::string name;
                 const std::string source = program_of(job.chunk, job.mode, name);
-                const char *headers[] = {sci_embedded_math, sci_embedded_kernel, sci_embedded_gradient};
-                const char *names[] = {"sci_math.cuh", "chunk_kernel.cuh", "gradient_kernel.cuh"};
+                const char *headers[] = {sci_embedded_math, sci_embedded_kernel, sci_embedded_gradient, sci_embedded_batch};
+                const char *names[] = {"sci_math.cuh", "chunk_kernel.cuh", "gradient_kernel.cuh", "batch_kernel.cuh"};
                 nvrtcProgram program;
-                if (nvrtcCreateProgram(&program, source.c_str(), "sci_specialized.cu", 3, headers, names) != NVRTC_SUCCESS)
+                if (nvrtcCreateProgram(&program, source.c_str(), "sci_specialized.cu", 4, headers, names) != NVRTC_SUCCESS)
                     return entry;
                 nvrtcAddNameExpression(program, name.c_str());
                 const char *options[] = {"-default-device", "-arch=sm_100a", "-std=c++17", "-lineinfo",

@@ -197,6 +197,47 @@ class Device:
         return x, dm, db, report.backward_error, report.iterations
 
 
+    def batch(self, chunk: C.Chunk, fold: int, inputs: np.ndarray, counts: np.ndarray, outputs=None,
+              results: "DeviceArray | None" = None) -> "Batch":
+        """Many instances of one chunk in one graph-captured launch (new; the reference batches
+        dispatches into Vulkan command buffers). inputs: items x arguments device pointers; counts:
+        items element counts; outputs: items device pointers or None; results: a float64
+        DeviceArray of items values, or None."""
+        return Batch(self, chunk, fold, inputs, counts, outputs, results)
+
+
+class Batch:
+    """A prepared batch (sci_cuda_batch_*): launch() replays its CUDA graph on the device stream."""
+
+    def __init__(self, device: Device, chunk: C.Chunk, fold: int, inputs, counts, outputs, results):
+        from .native import BatchItems
+
+        self.device = device
+        self._inputs = np.ascontiguousarray(inputs, np.uint64)
+        self._counts = np.ascontiguousarray(counts, np.uint64)
+        self._outputs = None if outputs is None else np.ascontiguousarray(outputs, np.uint64)
+        items = BatchItems(len(self._counts), self._inputs.ctypes.data,
+                           None if self._outputs is None else self._outputs.ctypes.data, self._counts.ctypes.data,
+                           None if results is None else results.pointer)
+        self.handle = ctypes.c_void_p()
+        check(lib.sci_cuda_batch_create(device.handle, ctypes.byref(chunk), fold, ctypes.byref(items),
+                                        ctypes.byref(self.handle)), device.handle)
+
+    def launch(self) -> None:
+        check(lib.sci_cuda_batch_launch(self.handle), self.device.handle)
+
+    def spans(self):
+        spans = (ctypes.c_uint32 * 3)()
+        specialized = ctypes.c_int32()
+        check(lib.sci_cuda_batch_spans(self.handle, spans, ctypes.byref(specialized)), self.device.handle)
+        return list(spans), bool(specialized.value)
+
+    def close(self) -> None:
+        if self.handle:
+            lib.sci_cuda_batch_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+
 class DeviceArray:
     """A one-dimensional array in this device's memory."""
 

@@ -34,6 +34,13 @@ class SolveReport(ctypes.Structure):
     _fields_ = [("backward_error", ctypes.c_double), ("iterations", ctypes.c_int)]
 
 
+class BatchItems(ctypes.Structure):
+    """sci_batch_items (include/sci_cuda.h)."""
+
+    _fields_ = [("items", ctypes.c_uint32), ("inputs", ctypes.c_void_p), ("outputs", ctypes.c_void_p),
+                ("counts", ctypes.c_void_p), ("results", ctypes.c_void_p)]
+
+
 def _load() -> ctypes.CDLL:
     if not LIBRARY.exists():
         raise ImportError(f"{LIBRARY} is not built; run `python -m libsci_b200.build` (needs nvcc)")
@@ -64,6 +71,11 @@ def _load() -> ctypes.CDLL:
                                         [ctypes.c_uint64] * 3)
     sig["sci_cuda_solve_gradient"] = (ctypes.c_int, [c_ctx, ctypes.c_uint32, ctypes.c_uint32] + [ctypes.c_void_p] * 6 +
                                       [ctypes.c_uint64, ctypes.c_uint64, P(SolveReport)])
+    sig["sci_cuda_batch_create"] = (ctypes.c_int, [c_ctx, P(ChunkStruct), ctypes.c_uint32, P(BatchItems),
+                                                   P(ctypes.c_void_p)])
+    sig["sci_cuda_batch_launch"] = (ctypes.c_int, [ctypes.c_void_p])
+    sig["sci_cuda_batch_spans"] = (ctypes.c_int, [ctypes.c_void_p, P(ctypes.c_uint32), P(ctypes.c_int32)])
+    sig["sci_cuda_batch_destroy"] = (ctypes.c_int, [ctypes.c_void_p])
     optional = {}
     sig["sci_cuda_factor"] = (ctypes.c_int, [c_ctx, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_uint64])
