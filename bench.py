@@ -340,7 +340,7 @@ def run_gradient(args) -> int:
     from libsci_b200.device import Device
     from libsci_b200.native import check, lib
 
-    n = 1 << 26
+    n = args.gradient_elements
     device = Device(0)
     stream = torch.cuda.ExternalStream(device.stream)
     rng = np.random.default_rng(0)
@@ -466,7 +466,7 @@ def run_gradient(args) -> int:
             "value": chunk_result["speedup_recompute_vs_stored"], "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_recompute, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (adjoints in f64)", "data": "synthetic",
-            "config": {"workload": "gradient of sum(exp(-a*a)*sin(b)+log(1+c*c)), n=2^26 float32; "
+            "config": {"workload": f"gradient of sum(exp(-a*a)*sin(b)+log(1+c*c)), n={n} float32; "
                                    "gradient of sum(solve(A,B)), A=G+4096I 4096^2 fp64, B 4096x64",
                        "l2": "inputs 256 MiB each, above L2"},
             "chunk": chunk_result, "solve": solve_result,
@@ -479,9 +479,162 @@ def run_gradient(args) -> int:
     return 0
 
 
+def batch_chunk(C, precision=0):
+    """t = a*b + c stored and tanh(t) reduced in one chunk: fuse(in0, in1, in2) -> T0; copy(T0) ->
+    output; tanh(T0) -> T1; result T1."""
+    chunk = C.Chunk(precision)
+    chunk.arguments, chunk.temporaries, chunk.length = 3, 2, 3
+    program = ((C.CODE["fuse"], C.TEMPORARY | 0, (0, 1, 2)),
+               (C.CODE["copy"], C.OUTPUT, (C.TEMPORARY | 0, C.NONE, C.NONE)),
+               (C.CODE["tanh"], C.TEMPORARY | 1, (C.TEMPORARY | 0, C.NONE, C.NONE)))
+    for index, (code, target, sources) in enumerate(program):
+        ins = chunk.instructions[index]
+        ins.code, ins.target = code, target
+        ins.sources[0], ins.sources[1], ins.sources[2] = sources
+    chunk.result = C.TEMPORARY | 1
+    return chunk
+
+
+def run_batch(args) -> int:
+    """Batching: 8192 float32 instances of t = a*b + c, r = sum(tanh(t)), lengths log-uniform in
+    [256, 2^20] (seeded), a, b, c ~ N(0,1), in one persistent launch replayed from a CUDA graph.
+    Beside it: the plain form, a loop of single calls through the C ABI (execute t, reduce
+    tanh(t), per item) on the same GPU, and libsci's CPU path on a sample of items."""
+    import torch
+
+    from libsci_b200 import chunk as C
+    from libsci_b200.device import Device
+    from libsci_b200.native import check, lib
+    from tests import _oracle
+
+    items = args.items
+    rng = np.random.default_rng(0)
+    counts = np.exp(rng.uniform(np.log(256), np.log(1 << 20), items)).astype(np.int64)
+    offsets = np.concatenate([[0], np.cumsum((counts + 63) // 64 * 64)])
+    total = int(offsets[-1])
+    elements = int(counts.sum())
+    device = Device(0)
+    stream = torch.cuda.ExternalStream(device.stream)
+    generator = torch.Generator(device="cuda").manual_seed(0)
+    inputs = [torch.randn(total, generator=generator, device="cuda", dtype=torch.float32) for _ in range(3)]
+    t_out = torch.empty(total, device="cuda", dtype=torch.float32)
+    results = torch.zeros(items, device="cuda", dtype=torch.float64)
+    pointers = np.array([[x.data_ptr() + 4 * int(o) for x in inputs] for o in offsets[:-1]], np.uint64)
+    outputs = np.array([t_out.data_ptr() + 4 * int(o) for o in offsets[:-1]], np.uint64)
+
+    class Results:  # the DeviceArray face of the torch buffer
+        pointer = results.data_ptr()
+
+    chunk = batch_chunk(C)
+    torch.cuda.synchronize()
+    created = time.perf_counter()
+    batch = device.batch(chunk, C.SUM, pointers, counts, outputs, Results)
+    created = time.perf_counter() - created
+    spans, specialized = batch.spans()
+    for _ in range(args.warmup):
+        batch.launch()
+    device.synchronize()
+    times = []
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            batch.launch()
+            stop.record(stream)
+            stop.synchronize()
+            times.append(start.elapsed_time(stop))
+    ms = statistics.median(times)
+    bytes_moved = 16.0 * elements  # read a, b, c; write t; r folds from registers
+    peak, peak_source = measured_peaks()
+    got = results.cpu().numpy()
+
+    # the plain form: one execute and one reduce per item through the C ABI
+    single_t = C.Chunk(0)
+    single_r = C.Chunk(0)
+    for ch, program, result in ((single_t, ((C.CODE["fuse"], C.OUTPUT, (0, 1, 2)),), C.OUTPUT),
+                                (single_r, ((C.CODE["tanh"], C.TEMPORARY | 0, (0, C.NONE, C.NONE)),), C.TEMPORARY | 0)):
+        ch.length, ch.temporaries = 1, (1 if ch is single_r else 0)
+        ch.arguments = 3 if ch is single_t else 1
+        ins = ch.instructions[0]
+        ins.code, ins.target = program[0][0], program[0][1]
+        ins.sources[0], ins.sources[1], ins.sources[2] = program[0][2]
+        ch.result = result
+
+    def loop():
+        for k in range(items):
+            for a in range(3):
+                single_t.inputs[a] = int(pointers[k, a])
+            check(lib.sci_cuda_execute(device.handle, ctypes.byref(single_t), int(outputs[k]), int(counts[k])), device.handle)
+            single_r.inputs[0] = int(outputs[k])
+            check(lib.sci_cuda_reduce_async(device.handle, ctypes.byref(single_r), C.SUM, int(counts[k]),
+                                            results.data_ptr() + 8 * k), device.handle)
+
+    loop()
+    device.jit_wait()
+    loop()
+    device.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    loop()
+    stop.record(stream)
+    stop.synchronize()
+    loop_ms = start.elapsed_time(stop)
+    loop_results = results.cpu().numpy()
+
+    # spot checks against libsci's CPU path on 16 items: t bit for bit, r to 1e-6 of sum |tanh t|
+    ref = _oracle.reference()
+    checked, t_mismatch, r_error = 0, 0, 0.0
+    if ref is not None:
+        t_host = t_out.cpu().numpy()
+        host = [x.cpu().numpy() for x in inputs]
+        for k in rng.choice(items, 16, replace=False):
+            o, n = int(offsets[k]), int(counts[k])
+            a, b, c = (np.ascontiguousarray(h[o:o + n]) for h in host)
+            refs = [C.Reference(x.ctypes.data, n, np.float32) for x in (a, b, c)]
+            t = _oracle.execute(ref, C.record_output(refs[0] * refs[1] + refs[2]), n, np.float32)
+            values = _oracle.execute(ref, C.record_output(C.unary("tanh", C.Reference(t.ctypes.data, n, np.float32))), n,
+                                     np.float32).astype(np.float64)
+            t_mismatch += int(_oracle.mismatches(t_host[o:o + n], t).size)
+            r_error = max(r_error, abs(got[k] - values.sum()) / np.abs(values).sum())
+            checked += 1
+
+    cpu = None
+    if ref is not None and not args.no_cpu:
+        sample = rng.choice(items, 256, replace=False)
+        host = [x.cpu().numpy() for x in inputs]
+        start_cpu = time.perf_counter()
+        done = 0
+        for k in sample:
+            o, n = int(offsets[k]), int(counts[k])
+            refs = [C.Reference(h[o:o + n].ctypes.data, n, np.float32) for h in host]
+            t = _oracle.execute(ref, C.record_output(refs[0] * refs[1] + refs[2]), n, np.float32)
+            _oracle.reduce(ref, C.record_reduce(C.unary("tanh", C.Reference(t.ctypes.data, n, np.float32))), C.SUM, n)
+            done += n
+        seconds = time.perf_counter() - start_cpu
+        cpu = {"value": 16.0 * done / seconds / 1e9, "unit": "GB/s", "cores": int(ref.sci_ref_threads()),
+               "kind": "reference", "sample": f"{len(sample)} of the {items} items ({done} elements): one assign and "
+                                               "one reduce per item on libsci's CPU path"}
+    line = {"metric": "batched chunk GB/s (one graph launch over all items)", "value": bytes_moved / (ms * 1e-3) / 1e9,
+            "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{items} instances of t=a*b+c, r=sum(tanh(t)), lengths log-uniform in [256, 2^20]",
+                       "elements": elements, "bytes_per_element": 16, "l2": f"{16 * elements / 1e9:.1f} GB of operands, above L2"},
+            "batch": {"spans": spans, "specialized": specialized, "create_s": created,
+                      "plain_loop_ms": loop_ms, "speedup_vs_plain_loop": loop_ms / ms,
+                      "loop_max_rel_diff": float(np.max(np.abs(loop_results - got) / np.maximum(np.abs(got), 1e-30))),
+                      "checked_items": checked, "t_mismatches": t_mismatch, "r_rel_error": r_error},
+            "roofline": {"bound": "hbm", "achieved": bytes_moved / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": bytes_moved / (ms * 1e-3) / 1e9 / peak, "traffic": None, "peak_source": peak_source},
+            "cpu_baseline": cpu, "gpu_launches": args.steps, "clocks": clocks.summary()}
+    print(json.dumps(line))
+    batch.close()
+    device.close()
+    return 0
+
+
 def main() -> int:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--workload", default="chunks", choices=["chunks", "product", "solve", "gradient"])
+    parser.add_argument("--workload", default="chunks", choices=["chunks", "product", "solve", "gradient", "batch"])
     parser.add_argument("--size", type=int, default=8192)
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=20)
@@ -490,6 +643,8 @@ def main() -> int:
     parser.add_argument("--elements", type=int, default=1 << 28)
     parser.add_argument("--e2e-steps", type=int, default=3)
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    parser.add_argument("--items", type=int, default=8192, help="batch workload: instances")
+    parser.add_argument("--gradient-elements", type=int, default=1 << 26, help="gradient workload: elements per array")
     args = parser.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -504,6 +659,8 @@ def main() -> int:
         return run_solve(args)
     if args.workload == "gradient":
         return run_gradient(args)
+    if args.workload == "batch":
+        return run_batch(args)
 
     import torch
 
