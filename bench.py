@@ -21,7 +21,8 @@ the timed region. `roofline` is the dominant kernel's achieved GB/s over the mea
 
 `--impl reference` times only that CPU path (the reference arm), on rank 0.
 With N > 1 GPUs (torchrun), every rank runs its own 2^28-element shard (weak scaling) and the
-three reductions are combined across ranks with one NCCL all-reduce per step.
+three reductions are combined across ranks each step (libsci_b200/shards.py: four small NCCL
+all-reduces that keep the rule that a NaN on any rank wins).
 """
 from __future__ import annotations
 
@@ -675,6 +676,7 @@ def main() -> int:
 
     from libsci_b200 import chunk as C
     from libsci_b200.device import Device
+    from libsci_b200.shards import combine
 
     n = args.elements
     device = Device(local)
@@ -711,10 +713,7 @@ def main() -> int:
             events[len(names)].record(stream)
         if dist is not None:
             with torch.cuda.stream(stream):
-                sums = results[[0, 2]].clone()
-                peak = results[1:2].clone()
-                dist.all_reduce(sums)
-                dist.all_reduce(peak, op=dist.ReduceOp.MAX)
+                results.copy_(combine(results, (C.SUM, C.MAXIMUM, C.SUM)))  # mean, peak, dot of the whole array
 
     # warm-up (also lets any specialised kernels compile and load)
     for _ in range(args.warmup):
