@@ -633,9 +633,113 @@ def run_batch(args) -> int:
     return 0
 
 
+def run_solves(args) -> int:
+    """Batching of solves: 4096 independent systems, n ~ U[8, 256] (seeded), A = G + n I (G ~ N(0,1)),
+    one right-hand side ~ N(0,1), FP32 LU + FP64 refinement, one graph replay (block size tuned per
+    order bucket). Beside it: a loop of single sci_cuda_solve calls (the plain form, sampled) and
+    libsci's CPU solve<double> per system (sampled)."""
+    import torch
+
+    from libsci_b200.device import Device
+    from libsci_b200.native import SolveReport, check, lib
+    from tests import _oracle
+
+    count = args.items if args.items != 8192 else 4096
+    rng = np.random.default_rng(0)
+    orders = rng.integers(8, 257, count)
+    device = Device(0)
+    stream = torch.cuda.ExternalStream(device.stream)
+    mats = [rng.standard_normal((n, n)) + n * np.eye(n) for n in orders]
+    rhs = [rng.standard_normal(n) for n in orders]
+    offsets_a = np.concatenate([[0], np.cumsum(orders * orders)])
+    offsets_b = np.concatenate([[0], np.cumsum(orders)])
+    flat_a = device.array(np.concatenate([m.ravel() for m in mats]))
+    flat_b = device.array(np.concatenate(rhs))
+    flat_x = device.empty(int(offsets_b[-1]), np.float64)
+    errors = device.empty(count, np.float64)
+    iterations = device.empty(count, np.int32)
+    pa = [flat_a.pointer + 8 * int(o) for o in offsets_a[:-1]]
+    pb = [flat_b.pointer + 8 * int(o) for o in offsets_b[:-1]]
+    px = [flat_x.pointer + 8 * int(o) for o in offsets_b[:-1]]
+    created = time.perf_counter()
+    batch = device.solve_batch(orders, pa, pb, px, errors, iterations)
+    created = time.perf_counter() - created
+    for _ in range(args.warmup):
+        batch.launch()
+    device.synchronize()
+    times = []
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            batch.launch()
+            stop.record(stream)
+            stop.synchronize()
+            times.append(start.elapsed_time(stop))
+    ms = statistics.median(times)
+    flops = float(np.sum(2.0 / 3.0 * orders.astype(np.float64) ** 3 + 2.0 * orders.astype(np.float64) ** 2))
+    berr, its = errors.numpy(), iterations.numpy()
+    x = flat_x.numpy()
+    sample = rng.choice(count, 64, replace=False)
+    mine = max(float(np.abs(rhs[k] - mats[k] @ x[offsets_b[k]:offsets_b[k + 1]]).max()
+                     / (np.abs(mats[k]).sum(axis=1).max() * np.abs(x[offsets_b[k]:offsets_b[k + 1]]).max()
+                        + np.abs(rhs[k]).max())) for k in sample)
+
+    # the plain form: one sci_cuda_solve (FP32 LU + FP64 refinement) per system, sampled
+    loop_sample = rng.choice(count, 128, replace=False)
+    report = SolveReport()
+    for k in loop_sample[:4]:
+        check(lib.sci_cuda_solve(device.handle, 1, 1, pa[k], pb[k], px[k], int(orders[k]), 1, ctypes.byref(report)),
+              device.handle)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for k in loop_sample:
+        check(lib.sci_cuda_solve(device.handle, 1, 1, pa[k], pb[k], px[k], int(orders[k]), 1, ctypes.byref(report)),
+              device.handle)
+    stop.record(stream)
+    stop.synchronize()
+    loop_flops = float(np.sum(2.0 / 3.0 * orders[loop_sample].astype(np.float64) ** 3
+                              + 2.0 * orders[loop_sample].astype(np.float64) ** 2))
+    loop_gflops = loop_flops / (start.elapsed_time(stop) * 1e-3) / 1e9
+
+    ref = None if args.no_cpu else _oracle.reference()
+    cpu = None
+    if ref is not None:
+        cpu_sample = rng.choice(count, 256, replace=False)
+        done = 0.0
+        out = np.empty(257)
+        started = time.perf_counter()
+        for k in cpu_sample:
+            n = int(orders[k])
+            ref.sci_ref_solve_f64(mats[k].ctypes.data, rhs[k].ctypes.data, out.ctypes.data, n, 1)
+            done += 2.0 / 3.0 * n ** 3 + 2.0 * n * n
+        seconds = time.perf_counter() - started
+        cpu = {"value": done / seconds / 1e9, "unit": "GFLOP/s", "cores": int(ref.sci_ref_threads()), "kind": "reference",
+               "sample": "256 of the systems, one solve<double> call each on libsci's CPU path"}
+    line = {"metric": "batched small solves GFLOP/s (one graph launch)", "value": flops / (ms * 1e-3) / 1e9,
+            "unit": "GFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 LU + f64 refinement",
+            "data": "synthetic",
+            "config": {"workload": f"{count} solves, n ~ U[8,256], A = G + nI, 1 RHS", "flop": flops,
+                       "matrix_bytes": int(offsets_a[-1]) * 8},
+            "solves": {"threads_per_bucket": batch.shapes(), "create_s": created, "max_backward_error": float(np.nanmax(berr)),
+                       "mean_iterations": float(its.mean()), "max_backward_error_numpy_sample": mine,
+                       "plain_loop_GFLOP/s": loop_gflops,
+                       "speedup_vs_plain_loop": (flops / (ms * 1e-3) / 1e9) / loop_gflops},
+            "roofline": {"bound": "latency (per-column barriers)", "achieved": flops / (ms * 1e-3) / 1e12,
+                         "peak": None, "unit": "TFLOP/s", "frac": None, "traffic": None,
+                         "note": "A is read twice (FP32 copy + FP64 residuals from L2): "
+                                 f"{2 * int(offsets_a[-1]) * 8 / (ms * 1e-3) / 1e9:.0f} GB/s of HBM for A"},
+            "cpu_baseline": cpu, "gpu_launches": 4 * args.steps, "clocks": clocks.summary()}
+    print(json.dumps(line))
+    batch.close()
+    device.close()
+    return 0
+
+
 def main() -> int:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--workload", default="chunks", choices=["chunks", "product", "solve", "gradient", "batch"])
+    parser.add_argument("--workload", default="chunks", choices=["chunks", "product", "solve", "gradient", "batch", "solves"])
     parser.add_argument("--size", type=int, default=8192)
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=20)
@@ -662,6 +766,8 @@ def main() -> int:
         return run_gradient(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "solves":
+        return run_solves(args)
 
     import torch
 

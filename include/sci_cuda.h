@@ -242,6 +242,32 @@ int sci_cuda_batch_spans(const sci_cuda_batch *batch, uint32_t *spans, int32_t *
 /* Waits for the context's queued work, then frees the batch. */
 int sci_cuda_batch_destroy(sci_cuda_batch *batch);
 
+/* Thousands of small independent solves (linear::solve, include/linear/solve.hpp:60-76, one
+ * right-hand side each, double operands, order 1..256) in one graph replay: FP32 LU with the
+ * reference's pivoting rules and FP64 refinement, one CTA per system (no counterpart in the
+ * reference's API). Tables are host arrays read once at creation; the pointers in them, and
+ * `errors` / `iterations` (systems entries each, may be null), are device memory. */
+typedef struct sci_solve_items {
+    uint32_t systems;
+    const uint32_t *orders;        /* order of each system                                  */
+    const void *const *matrices;   /* n x n row-major doubles per system                    */
+    const void *const *rights;     /* n doubles per system                                  */
+    void *const *solutions;        /* n doubles per system, written                         */
+    double *errors;                /* normwise backward error per system, or null          */
+    int32_t *iterations;           /* refinement iterations per system, or null            */
+} sci_solve_items;
+typedef struct sci_cuda_solve_batch sci_cuda_solve_batch;
+/* Checks every system, tunes the block size of each order bucket (<= 32, <= 64, <= 128, <= 256;
+ * cached like the chunk batches), and captures one launch per bucket into a CUDA graph. The tuning
+ * launches solve the systems. Waits. */
+int sci_cuda_solve_batch_create(sci_cuda_context *context, const sci_solve_items *items, sci_cuda_solve_batch **batch);
+/* Replays the graph on the context's stream (queued). */
+int sci_cuda_solve_batch_launch(sci_cuda_solve_batch *batch);
+/* Threads per CTA chosen for each bucket (0: the bucket is empty). */
+int sci_cuda_solve_batch_shapes(const sci_cuda_solve_batch *batch, uint32_t *threads);
+/* Waits for the context's queued work, then frees the batch. */
+int sci_cuda_solve_batch_destroy(sci_cuda_solve_batch *batch);
+
 /* No counterpart in the reference. The same reduction for callers that may not allocate device
  * memory (a host framework that owns the GPU heap through its own pool, a plugin inside one, a
  * latency-critical thread where an allocation would synchronize the device). It needs no context:

@@ -14,6 +14,7 @@
 // $HOME/.cache/sci_cuda/batch_tune.txt) that later processes read; SCI_CUDA_TUNE=0 skips tuning.
 #include "batch_kernel.cuh"
 #include "context.hpp"
+#include "solve_batch_kernel.cuh"
 #include "specialize.hpp"
 
 #include <cuda_runtime.h>
@@ -397,6 +398,242 @@ extern "C" int sci_cuda_batch_destroy(sci_cuda_batch *batch) {
         cudaStreamSynchronize(context->stream);
         if (batch->exec) cudaGraphExecDestroy(batch->exec);
         if (batch->graph) cudaGraphDestroy(batch->graph);
+        if (batch->memory) cudaFree(batch->memory);
+    }
+    delete batch;
+    return SCI_CUDA_OK;
+}
+
+// ---- batched small solves ---------------------------------------------------------------------
+// Thousands of independent systems (n <= 256, one right-hand side, double operands), FP32 LU and
+// FP64 refinement inside one CTA per system (solve_batch_kernel.cuh). Systems are grouped into four
+// buckets by order (<= 32, <= 64, <= 128, <= 256); each bucket is one launch whose block size the
+// autotuner picks among the variants that fit it (timed on the bucket's own systems, cached like
+// the chunk batches' spans). The four launches are captured into one CUDA graph on parallel
+// branches, so small buckets fill the gaps of the large one.
+
+struct sci_cuda_solve_batch {
+    sci_cuda_context *context{nullptr};
+    void *memory{nullptr};
+    unsigned threads[4]{};
+    cudaStream_t branches[4]{};
+    cudaEvent_t fork{nullptr}, joins[4]{};
+    cudaGraph_t graph{nullptr};
+    cudaGraphExec_t exec{nullptr};
+};
+
+namespace {
+
+    struct Variant {
+        int threads, rc;
+        const void *kernel;
+    };
+    const Variant kVariants[] = {
+            {32, 0, reinterpret_cast<const void *>(&small_solve<32, 0>)},
+            {64, 0, reinterpret_cast<const void *>(&small_solve<64, 0>)},
+            {128, 0, reinterpret_cast<const void *>(&small_solve<128, 0>)},
+            {256, 0, reinterpret_cast<const void *>(&small_solve<256, 0>)},
+            {256, kSmallRegisters, reinterpret_cast<const void *>(&small_solve<256, kSmallRegisters>)},
+            {512, kSmallRegisters, reinterpret_cast<const void *>(&small_solve<512, kSmallRegisters>)},
+    };
+
+    int solve_bucket(unsigned n) { return n <= 32 ? 0 : (n <= 64 ? 1 : (n <= 128 ? 2 : 3)); }
+
+    // The variants that may run a bucket whose largest order is `most`.
+    std::vector<const Variant *> candidates(int bucket, unsigned most) {
+        std::vector<const Variant *> out;
+        for (const Variant &v : kVariants) {
+            const bool registers = v.rc > 0;
+            if (bucket < 3 && registers) continue;
+            if (bucket == 3 && most > kSmallShared && !registers) continue;  // only the register form fits
+            if (registers && static_cast<unsigned>(v.threads) < most) continue;
+            if (bucket == 0 && v.threads > 128) continue;
+            if (bucket >= 2 && v.threads < 64) continue;
+            out.push_back(&v);
+        }
+        return out;
+    }
+
+} // namespace
+
+extern "C" int sci_cuda_solve_batch_create(sci_cuda_context *context, const sci_solve_items *items,
+                                           sci_cuda_solve_batch **batch) {
+    if (!context || !batch) return SCI_CUDA_ERROR_INVALID;
+    *batch = nullptr;
+    std::lock_guard<std::recursive_mutex> lock(context->guard);
+    Context &ctx = *context;
+    if (!items || (items->systems && (!items->orders || !items->matrices || !items->rights || !items->solutions)))
+        return ctx.fail(SCI_CUDA_ERROR_INVALID, "null system tables");
+    cudaSetDevice(ctx.device);
+    const unsigned count = items->systems;
+    std::vector<SmallSystem> systems(count);
+    std::vector<unsigned> lists[4];
+    unsigned most[4] = {};
+    for (unsigned s = 0; s < count; ++s) {
+        const unsigned n = items->orders[s];
+        if (n == 0 || n > static_cast<unsigned>(kSmallMax))
+            return ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "system %u: order %u outside 1..%d", s, n, kSmallMax);
+        const void *a = items->matrices[s], *b = items->rights[s];
+        void *x = items->solutions[s];
+        if (!a || !b || !x || !reachable(ctx, a) || !reachable(ctx, b) || !reachable(ctx, x))
+            return ctx.fail(SCI_CUDA_ERROR_INVALID, "system %u: an operand is not memory of this device", s);
+        systems[s] = SmallSystem{static_cast<const double *>(a), static_cast<const double *>(b), static_cast<double *>(x), n, 0};
+        const int b_ = solve_bucket(n);
+        lists[b_].push_back(s);
+        most[b_] = std::max(most[b_], n);
+    }
+    if ((items->errors && !reachable(ctx, items->errors)) || (items->iterations && !reachable(ctx, items->iterations)))
+        return ctx.fail(SCI_CUDA_ERROR_INVALID, "errors / iterations are not memory of this device");
+    for (auto &list : lists)
+        std::stable_sort(list.begin(), list.end(), [&](unsigned x, unsigned y) { return systems[x].n > systems[y].n; });
+
+    auto *made = new sci_cuda_solve_batch;
+    made->context = context;
+    const size_t table = (count * sizeof(SmallSystem) + 255) / 256 * 256;
+    if (int code = ctx.check(cudaMalloc(&made->memory, table + 4ull * count + 256), "allocating the system tables")) {
+        delete made;
+        return code;
+    }
+    auto fail = [&](int code) {
+        sci_cuda_solve_batch_destroy(made);
+        return code;
+    };
+    auto *device_systems = static_cast<SmallSystem *>(made->memory);
+    auto *device_order = reinterpret_cast<unsigned *>(static_cast<unsigned char *>(made->memory) + table);
+    unsigned offsets[4] = {};
+    std::vector<unsigned> flat;
+    for (int b = 0; b < 4; ++b) {
+        offsets[b] = static_cast<unsigned>(flat.size());
+        flat.insert(flat.end(), lists[b].begin(), lists[b].end());
+    }
+    cudaMemcpyAsync(device_systems, systems.data(), count * sizeof(SmallSystem), cudaMemcpyHostToDevice, ctx.stream);
+    cudaMemcpyAsync(device_order, flat.data(), flat.size() * 4, cudaMemcpyHostToDevice, ctx.stream);
+    if (int code = ctx.check(cudaStreamSynchronize(ctx.stream), "uploading the system tables")) return fail(code);
+
+    double *errors = items->errors;
+    int *iterations = items->iterations;
+    auto launch = [&](int b, const Variant &v, cudaStream_t stream) -> int {
+        const unsigned long long smem = small_shared_bytes(most[b], v.rc);
+        if (smem > ctx.shared_limit) return ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "bucket %d needs %llu bytes of shared memory", b, smem);
+        cudaFuncSetAttribute(v.kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        const unsigned *order = device_order + offsets[b];
+        void *args[] = {&device_systems, &order, &errors, &iterations};
+        return ctx.check(cudaLaunchKernel(v.kernel, dim3(static_cast<unsigned>(lists[b].size())), dim3(v.threads), args, smem, stream),
+                         "launching a batch of small solves");
+    };
+
+    // tune each bucket's block size
+    const char *tune = std::getenv("SCI_CUDA_TUNE");
+    const bool tuning = !(tune && tune[0] == '0');
+    {
+        std::lock_guard<std::mutex> guard(cache_guard);
+        load_cache();
+    }
+    const Variant *chosen[4] = {};
+    for (int b = 0; b < 4; ++b) {
+        if (lists[b].empty()) continue;
+        const auto options = candidates(b, most[b]);
+        if (options.empty()) return fail(ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "no variant for bucket %d", b));
+        chosen[b] = options.back();
+        std::string key;
+        for (char ch : ctx.name) key += (ch == ' ' ? '_' : ch);
+        key += "|solve|" + std::to_string(b);
+        if (!tuning) continue;
+        {
+            std::lock_guard<std::mutex> guard(cache_guard);
+            auto hit = cache.find(key);
+            if (hit != cache.end()) {
+                for (const Variant *v : options)
+                    if (static_cast<unsigned>(v->threads) == hit->second) chosen[b] = v;
+                continue;
+            }
+        }
+        float best = -1.0f;
+        for (const Variant *v : options) {
+            cudaEvent_t start, stop;
+            cudaEventCreate(&start);
+            cudaEventCreate(&stop);
+            std::vector<float> times;
+            for (int rep = 0; rep < 4; ++rep) {
+                cudaEventRecord(start, ctx.stream);
+                if (int code = launch(b, *v, ctx.stream)) return fail(code);
+                cudaEventRecord(stop, ctx.stream);
+                if (int code = ctx.check(cudaEventSynchronize(stop), "timing a solve variant")) return fail(code);
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, start, stop);
+                if (rep > 0) times.push_back(ms);
+            }
+            cudaEventDestroy(start);
+            cudaEventDestroy(stop);
+            std::sort(times.begin(), times.end());
+            if (best < 0.0f || times[1] < best) {
+                best = times[1];
+                chosen[b] = v;
+            }
+        }
+        std::lock_guard<std::mutex> guard(cache_guard);
+        store_cache(key, static_cast<unsigned>(chosen[b]->threads));
+    }
+    for (int b = 0; b < 4; ++b) made->threads[b] = chosen[b] ? static_cast<unsigned>(chosen[b]->threads) : 0u;
+
+    // capture: fork to one branch per bucket, join back
+    cudaEventCreateWithFlags(&made->fork, cudaEventDisableTiming);
+    for (int b = 0; b < 4; ++b) {
+        cudaStreamCreateWithFlags(&made->branches[b], cudaStreamNonBlocking);
+        cudaEventCreateWithFlags(&made->joins[b], cudaEventDisableTiming);
+    }
+    if (int code = ctx.check(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal), "capturing the solves"))
+        return fail(code);
+    int launched = SCI_CUDA_OK;
+    cudaEventRecord(made->fork, ctx.stream);
+    for (int b = 3; b >= 0 && !launched; --b) {
+        if (!chosen[b]) continue;
+        cudaStreamWaitEvent(made->branches[b], made->fork, 0);
+        launched = launch(b, *chosen[b], made->branches[b]);
+        cudaEventRecord(made->joins[b], made->branches[b]);
+        cudaStreamWaitEvent(ctx.stream, made->joins[b], 0);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ended = cudaStreamEndCapture(ctx.stream, &graph);
+    if (launched) {
+        if (graph) cudaGraphDestroy(graph);
+        return fail(launched);
+    }
+    if (int code = ctx.check(ended, "ending the solve capture")) return fail(code);
+    made->graph = graph;
+    if (int code = ctx.check(cudaGraphInstantiate(&made->exec, graph, 0), "instantiating the solve graph")) return fail(code);
+    *batch = made;
+    return SCI_CUDA_OK;
+}
+
+extern "C" int sci_cuda_solve_batch_launch(sci_cuda_solve_batch *batch) {
+    if (!batch || !batch->exec) return SCI_CUDA_ERROR_INVALID;
+    sci_cuda_context *context = batch->context;
+    std::lock_guard<std::recursive_mutex> lock(context->guard);
+    cudaSetDevice(context->device);
+    return context->check(cudaGraphLaunch(batch->exec, context->stream), "launching the solve graph");
+}
+
+extern "C" int sci_cuda_solve_batch_shapes(const sci_cuda_solve_batch *batch, uint32_t *threads) {
+    if (!batch || !threads) return SCI_CUDA_ERROR_INVALID;
+    for (int b = 0; b < 4; ++b) threads[b] = batch->threads[b];
+    return SCI_CUDA_OK;
+}
+
+extern "C" int sci_cuda_solve_batch_destroy(sci_cuda_solve_batch *batch) {
+    if (!batch) return SCI_CUDA_OK;
+    sci_cuda_context *context = batch->context;
+    {
+        std::lock_guard<std::recursive_mutex> lock(context->guard);
+        cudaSetDevice(context->device);
+        cudaStreamSynchronize(context->stream);
+        if (batch->exec) cudaGraphExecDestroy(batch->exec);
+        if (batch->graph) cudaGraphDestroy(batch->graph);
+        for (int b = 0; b < 4; ++b) {
+            if (batch->branches[b]) cudaStreamDestroy(batch->branches[b]);
+            if (batch->joins[b]) cudaEventDestroy(batch->joins[b]);
+        }
+        if (batch->fork) cudaEventDestroy(batch->fork);
         if (batch->memory) cudaFree(batch->memory);
     }
     delete batch;

@@ -206,6 +206,43 @@ class Device:
         return Batch(self, chunk, fold, inputs, counts, outputs, results)
 
 
+    def solve_batch(self, orders, matrices, rights, solutions, errors: "DeviceArray | None" = None,
+                    iterations: "DeviceArray | None" = None) -> "SolveBatch":
+        """Many small solves (n <= 256, one right-hand side, double) in one graph replay: FP32 LU +
+        FP64 refinement per system. matrices / rights / solutions: device pointers per system."""
+        return SolveBatch(self, orders, matrices, rights, solutions, errors, iterations)
+
+
+class SolveBatch:
+    """A prepared batch of small solves (sci_cuda_solve_batch_*)."""
+
+    def __init__(self, device: Device, orders, matrices, rights, solutions, errors, iterations):
+        from .native import SolveItems
+
+        self.device = device
+        self._keep = [np.ascontiguousarray(orders, np.uint32)] + [np.ascontiguousarray(t, np.uint64)
+                                                                  for t in (matrices, rights, solutions)]
+        items = SolveItems(len(self._keep[0]), *[k.ctypes.data for k in self._keep],
+                           None if errors is None else errors.pointer,
+                           None if iterations is None else iterations.pointer)
+        self.handle = ctypes.c_void_p()
+        check(lib.sci_cuda_solve_batch_create(device.handle, ctypes.byref(items), ctypes.byref(self.handle)),
+              device.handle)
+
+    def launch(self) -> None:
+        check(lib.sci_cuda_solve_batch_launch(self.handle), self.device.handle)
+
+    def shapes(self):
+        threads = (ctypes.c_uint32 * 4)()
+        check(lib.sci_cuda_solve_batch_shapes(self.handle, threads), self.device.handle)
+        return list(threads)
+
+    def close(self) -> None:
+        if self.handle:
+            lib.sci_cuda_solve_batch_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+
 class Batch:
     """A prepared batch (sci_cuda_batch_*): launch() replays its CUDA graph on the device stream."""
 

@@ -41,6 +41,14 @@ class BatchItems(ctypes.Structure):
                 ("counts", ctypes.c_void_p), ("results", ctypes.c_void_p)]
 
 
+class SolveItems(ctypes.Structure):
+    """sci_solve_items (include/sci_cuda.h)."""
+
+    _fields_ = [("systems", ctypes.c_uint32), ("orders", ctypes.c_void_p), ("matrices", ctypes.c_void_p),
+                ("rights", ctypes.c_void_p), ("solutions", ctypes.c_void_p), ("errors", ctypes.c_void_p),
+                ("iterations", ctypes.c_void_p)]
+
+
 def _load() -> ctypes.CDLL:
     if not LIBRARY.exists():
         raise ImportError(f"{LIBRARY} is not built; run `python -m libsci_b200.build` (needs nvcc)")
@@ -76,6 +84,10 @@ def _load() -> ctypes.CDLL:
     sig["sci_cuda_batch_launch"] = (ctypes.c_int, [ctypes.c_void_p])
     sig["sci_cuda_batch_spans"] = (ctypes.c_int, [ctypes.c_void_p, P(ctypes.c_uint32), P(ctypes.c_int32)])
     sig["sci_cuda_batch_destroy"] = (ctypes.c_int, [ctypes.c_void_p])
+    sig["sci_cuda_solve_batch_create"] = (ctypes.c_int, [c_ctx, P(SolveItems), P(ctypes.c_void_p)])
+    sig["sci_cuda_solve_batch_launch"] = (ctypes.c_int, [ctypes.c_void_p])
+    sig["sci_cuda_solve_batch_shapes"] = (ctypes.c_int, [ctypes.c_void_p, P(ctypes.c_uint32)])
+    sig["sci_cuda_solve_batch_destroy"] = (ctypes.c_int, [ctypes.c_void_p])
     optional = {}
     sig["sci_cuda_factor"] = (ctypes.c_int, [c_ctx, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_uint64])
