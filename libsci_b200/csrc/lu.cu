@@ -79,29 +79,58 @@ namespace sci_cuda {
             return v;
         }
 
-        // (magnitude, row) pairs: larger magnitude wins, equal magnitudes go to the lower row -- the
-        // row the reference's "first strictly larger" scan keeps.
-        template <typename T> __device__ __forceinline__ bool better(T m1, unsigned long long r1, T m2, unsigned long long r2) {
-            return m1 > m2 || (m1 == m2 && r1 < r2);
-        }
-        template <typename T> __device__ __forceinline__ void warp_argmax(T &m, unsigned long long &r) {
-#pragma unroll
-            for (int offset = 16; offset > 0; offset >>= 1) {
-                const T om = __shfl_xor_sync(0xffffffffu, m, offset);
-                const unsigned long long orow = __shfl_xor_sync(0xffffffffu, r, offset);
-                if (better(om, orow, m, r)) {
-                    m = om;
-                    r = orow;
-                }
-            }
-        }
-
         // The panel's net row movement: after its exchanges, row rows[i] holds what row src[i] held.
         // Only rows the panel touched appear (at most twice its width).
         struct Movement {
             long long count;
             long long rows[64];
             long long src[64];
+        };
+
+        // ---- pivot search keys ---------------------------------------------------------------------
+        // A candidate's |value| as an unsigned key that orders like the value (non-negative floats
+        // order like their bits), plus one so that a candidate of magnitude 0 still beats "no
+        // candidate" (key 0). Rows are offsets from the panel's first row; kNoRow marks none. The
+        // pivot is the largest key and, among equal keys, the lowest row: the reference's "first
+        // strictly larger" scan (decompose.hpp:35-38).
+        constexpr unsigned kNoRow = 0xFFFFFFFFu;
+        template <typename T> struct MagnitudeKey;
+        template <> struct MagnitudeKey<float> {
+            using type = unsigned;
+        };
+        template <> struct MagnitudeKey<double> {
+            using type = unsigned long long;
+        };
+        __device__ __forceinline__ unsigned magnitude_key(float m) { return __float_as_uint(m) + 1u; }
+        __device__ __forceinline__ unsigned long long magnitude_key(double m) {
+            return static_cast<unsigned long long>(__double_as_longlong(m)) + 1ull;
+        }
+        // Every lane of the warp ends with the warp's best (key, row): warp reductions of the key,
+        // then of the row among the lanes that hold the best key.
+        __device__ __forceinline__ void best_of_warp(unsigned &key, unsigned &rel) {
+            const unsigned top = __reduce_max_sync(0xffffffffu, key);
+            rel = __reduce_min_sync(0xffffffffu, key == top ? rel : kNoRow);
+            key = top;
+        }
+        __device__ __forceinline__ void best_of_warp(unsigned long long &key, unsigned &rel) {
+            const unsigned hi = static_cast<unsigned>(key >> 32), lo = static_cast<unsigned>(key);
+            const unsigned top_hi = __reduce_max_sync(0xffffffffu, hi);
+            const unsigned top_lo = __reduce_max_sync(0xffffffffu, hi == top_hi ? lo : 0u);
+            const bool tie = hi == top_hi && lo == top_lo;
+            rel = __reduce_min_sync(0xffffffffu, tie ? rel : kNoRow);
+            key = (static_cast<unsigned long long>(top_hi) << 32) | top_lo;
+        }
+        __device__ __forceinline__ unsigned load_remote_u32(unsigned address) {
+            unsigned v;
+            asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(address) : "memory");
+            return v;
+        }
+        __device__ __forceinline__ unsigned load_remote_key(unsigned address, unsigned) { return load_remote_u32(address); }
+        __device__ __forceinline__ unsigned long long load_remote_key(unsigned address, unsigned long long) {
+            return load_remote_u64(address);
+        }
+        template <int N> struct Span {
+            static constexpr int value = N;
         };
 
         constexpr int kRowsPerThread = 2;
@@ -164,11 +193,14 @@ namespace sci_cuda {
             extern __shared__ __align__(16) unsigned char panel_shared[];
             T *stage = reinterpret_cast<T *>(panel_shared);  // stage[k * P + local row]
             __shared__ unsigned home[kCtaRows];          // bit k: stage holds column k of the row
-            __shared__ T warp_mag[WARPS];
-            __shared__ unsigned long long warp_row[WARPS], warp_origin[WARPS];
+            using Key = typename MagnitudeKey<T>::type;
+            __shared__ Key warp_key[WARPS];
+            __shared__ unsigned warp_rel[WARPS];
+            __shared__ unsigned long long warp_origin[WARPS];
             __shared__ __align__(16) T warp_values[WARPS][W];
-            __shared__ T cand_mag[2];
-            __shared__ unsigned long long cand_row[2], cand_origin[2];
+            __shared__ Key cand_key[2];
+            __shared__ unsigned cand_rel[2];
+            __shared__ unsigned long long cand_origin[2];
             __shared__ __align__(16) T cand_values[2][W];
             __shared__ __align__(16) T jbuf[2][W];  // CTA 0: the row at the pivot position
             __shared__ unsigned long long jbuf_origin[2];
@@ -198,54 +230,57 @@ namespace sci_cuda {
                 }
             }
 
-#pragma unroll 1
-            for (int j = 0; j < width; ++j) {
+            // One column step, specialised on Q >= width - j: after j shifts only v[i][0, width - j)
+            // is live (the rest is zero), so publication, elimination and the shift stop at Q.
+            auto column = [&](auto span, const int j) {
+                constexpr int Q = decltype(span)::value;
                 const int par = j & 1;
                 const unsigned long long row_j = j0 + j;
                 // 1. candidacy; a NaN only stands at the pivot position itself, where the reference's
                 //    comparisons against it all fail (decompose.hpp:35-38).
-                T best = T(-1);
-                unsigned long long brow = r[0];
+                Key key = 0;
+                unsigned rel = kNoRow;
 #pragma unroll
                 for (int i = 0; i < R; ++i) {
-                    T mag = T(-1);
                     if (valid[i] && r[i] >= row_j) {
                         const T m = fabs(v[i][0]);
-                        mag = (m == m) ? m : (r[i] == row_j ? T(INFINITY) : T(-1));
-                    }
-                    if (better(mag, r[i], best, brow)) {
-                        best = mag;
-                        brow = r[i];
+                        const bool candidate = m == m || r[i] == row_j;
+                        const Key k = candidate ? magnitude_key(m == m ? m : T(INFINITY)) : Key(0);
+                        const unsigned at = static_cast<unsigned>(r[i] - j0);
+                        if (k > key || (k == key && k != 0 && at < rel)) {
+                            key = k;
+                            rel = at;
+                        }
                     }
                 }
-                warp_argmax(best, brow);
+                best_of_warp(key, rel);
                 if (lane == 0) {
-                    warp_mag[warp] = best;
-                    warp_row[warp] = brow;
+                    warp_key[warp] = key;
+                    warp_rel[warp] = rel;
                 }
 #pragma unroll
                 for (int i = 0; i < R; ++i) {
-                    if (r[i] == brow) {
+                    if (rel != kNoRow && r[i] - j0 == rel) {
 #pragma unroll
-                        for (int k = 0; k < W; ++k) warp_values[warp][k] = v[i][k];
+                        for (int k = 0; k < Q; ++k) warp_values[warp][k] = v[i][k];
                         warp_origin[warp] = origin[i];
                     }
                 }
                 if (c == 0 && t == static_cast<unsigned>(j)) {  // row_j is row 0 of thread j in CTA 0
 #pragma unroll
-                    for (int k = 0; k < W; ++k) jbuf[par][k] = v[0][k];
+                    for (int k = 0; k < Q; ++k) jbuf[par][k] = v[0][k];
                     jbuf_origin[par] = origin[0];
                 }
                 if (warp == 0) {
                     named_sync(1, TH);
-                    T m2 = lane < WARPS ? warp_mag[lane] : T(-1);
-                    unsigned long long r2 = lane < WARPS ? warp_row[lane] : ~0ull;
-                    warp_argmax(m2, r2);
-                    const unsigned source = static_cast<unsigned>((r2 - first) % TH) / 32;
-                    if (lane < W) cand_values[par][lane] = warp_values[source][lane];
+                    Key k2 = lane < WARPS ? warp_key[lane] : Key(0);
+                    unsigned r2 = lane < WARPS ? warp_rel[lane] : kNoRow;
+                    best_of_warp(k2, r2);
+                    const unsigned source = r2 == kNoRow ? 0u : ((r2 - c * kCtaRows) % TH) / 32;
+                    if (lane < Q) cand_values[par][lane] = warp_values[source][lane];
                     if (lane == 0) {
-                        cand_mag[par] = m2;
-                        cand_row[par] = r2;
+                        cand_key[par] = k2;
+                        cand_rel[par] = r2;
                         cand_origin[par] = warp_origin[source];
                     }
                 } else {
@@ -254,44 +289,31 @@ namespace sci_cuda {
                 cluster_sync();  // the candidates and the pivot-position row are published
                 // 2. the pivot: warp 0 of every CTA reads all candidates in one round of loads
                 if (warp == 0) {
-                    T m = T(-1);
-                    unsigned long long row = ~0ull, org = 0;
+                    Key k3 = 0;
+                    unsigned r3 = kNoRow;
+                    unsigned long long org = 0;
                     if (lane < kClusterCtas) {
-                        m = load_remote(remote(&cand_mag[par], lane), T(0));
-                        row = load_remote_u64(remote(&cand_row[par], lane));
+                        k3 = load_remote_key(remote(&cand_key[par], lane), Key(0));
+                        r3 = load_remote_u32(remote(&cand_rel[par], lane));
                         org = load_remote_u64(remote(&cand_origin[par], lane));
                     }
                     T values[kClusterCtas];
 #pragma unroll
                     for (int q = 0; q < kClusterCtas; ++q)
-                        values[q] = lane < W ? load_remote(remote(&cand_values[par][lane], q), T(0)) : T(0);
-                    const T there = lane < W ? load_remote(remote(&jbuf[par][lane], 0), T(0)) : T(0);
+                        values[q] = lane < Q ? load_remote(remote(&cand_values[par][lane], q), T(0)) : T(0);
+                    const T there = lane < Q ? load_remote(remote(&jbuf[par][lane], 0), T(0)) : T(0);
                     const unsigned long long there_origin = load_remote_u64(remote(&jbuf_origin[par], 0));
-                    unsigned q = lane;
-#pragma unroll
-                    for (int offset = kClusterCtas / 2; offset > 0; offset >>= 1) {
-                        const T om = __shfl_xor_sync(0xffffffffu, m, offset);
-                        const unsigned long long orow = __shfl_xor_sync(0xffffffffu, row, offset);
-                        const unsigned long long oorg = __shfl_xor_sync(0xffffffffu, org, offset);
-                        const unsigned oq = __shfl_xor_sync(0xffffffffu, q, offset);
-                        if (better(om, orow, m, row)) {
-                            m = om;
-                            row = orow;
-                            org = oorg;
-                            q = oq;
-                        }
-                    }
-                    m = __shfl_sync(0xffffffffu, m, 0);
-                    row = __shfl_sync(0xffffffffu, row, 0);
-                    org = __shfl_sync(0xffffffffu, org, 0);
-                    q = __shfl_sync(0xffffffffu, q, 0);
-                    const unsigned long long prow = m < T(0) ? row_j : row;  // row_j is always a candidate
+                    best_of_warp(k3, r3);
+                    // the winner's CTA owns its row; no candidate cannot happen (row_j is one)
+                    const unsigned q = r3 == kNoRow ? 0u : r3 / kCtaRows;
+                    org = __shfl_sync(0xffffffffu, org, q);
+                    const unsigned long long prow = r3 == kNoRow ? row_j : j0 + r3;
                     T value = values[0];
 #pragma unroll
                     for (int s = 1; s < kClusterCtas; ++s)
                         if (q == static_cast<unsigned>(s)) value = values[s];
                     const bool exchange = (prow - j0) / kCtaRows == c && prow != row_j;
-                    if (lane < W) {
+                    if (lane < Q) {
                         pivot_row[lane] = value;
                         if (exchange) displaced[lane] = there;
                     }
@@ -309,16 +331,16 @@ namespace sci_cuda {
                     if (r[i] == prow && prow != row_j) {
                         // this row moves to the pivot's old place: it takes the displaced row's values
 #pragma unroll
-                        for (int k = 0; k < W; ++k) v[i][k] = displaced[k];
+                        for (int k = 0; k < Q; ++k) v[i][k] = displaced[k];
                         origin[i] = displaced_origin;
                     }
                     if (r[i] == row_j) {
                         // the pivot row is final: U's row j0 + j from column j0 + j on
 #pragma unroll
-                        for (int k = 0; k < W; ++k) v[i][k] = pivot_row[k];
+                        for (int k = 0; k < Q; ++k) v[i][k] = pivot_row[k];
                         origin[i] = pivot_origin;
 #pragma unroll
-                        for (int k = 0; k < W; ++k)
+                        for (int k = 0; k < Q; ++k)
                             if (k < width - j) a[origin[i] * n + row_j + k] = v[i][k];
                     }
                     // 3. eliminate below the pivot: l = a / pivot; a[k] -= l * pivot_row[k]; a zero
@@ -329,7 +351,7 @@ namespace sci_cuda {
                             const T l = div(v[i][0], diagonal);
                             v[i][0] = l;
 #pragma unroll
-                            for (int k = 1; k < W; ++k) v[i][k] = sub(v[i][k], mul(l, pivot_row[k]));
+                            for (int k = 1; k < Q; ++k) v[i][k] = sub(v[i][k], mul(l, pivot_row[k]));
                         }
                         if (origin[i] == r[i]) {
                             stage[j * P + static_cast<int>(r[i] - first)] = v[i][0];
@@ -339,9 +361,17 @@ namespace sci_cuda {
                         }
                     }
 #pragma unroll
-                    for (int k = 0; k + 1 < W; ++k) v[i][k] = v[i][k + 1];
-                    v[i][W - 1] = T(0);
+                    for (int k = 0; k + 1 < Q; ++k) v[i][k] = v[i][k + 1];
+                    v[i][Q - 1] = T(0);
                 }
+            };
+#pragma unroll 1
+            for (int j = 0; j < width; ++j) {
+                const int live = width - j;
+                if (live > 3 * W / 4) column(Span<W>{}, j);
+                else if (live > W / 2) column(Span<3 * W / 4>{}, j);
+                else if (live > W / 4) column(Span<W / 2>{}, j);
+                else column(Span<W / 4>{}, j);
             }
             // The staged multipliers, one row per warp store. Then every row's panel values sit at the
             // position the row started in; move the rows the exchanges displaced: all reads, a
