@@ -31,6 +31,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -38,9 +39,7 @@ namespace sci_cuda {
 
     namespace {
 
-        constexpr int kClusterCtas = 8;
-        constexpr int kCtaRows = 1024;
-        constexpr unsigned long long kPanelRows = 1ull * kClusterCtas * kCtaRows;
+        constexpr unsigned long long kPanelRows = 8192;  // the panel cluster holds every row in registers
         constexpr unsigned long long kOuter = 256;
         constexpr int kSolveBlock = 128;
 
@@ -133,11 +132,17 @@ namespace sci_cuda {
             static constexpr int value = N;
         };
 
-        constexpr int kRowsPerThread = 2;
-        constexpr int kPanelBlock = kCtaRows / kRowsPerThread;  // threads per panel CTA
-        // Dynamic shared memory of panel_factor: the staged multipliers, W x (1024 + 1).
-        template <typename T> constexpr size_t panel_shared_bytes() {
-            return sizeof(T) * PanelWidth<T>::value * (kCtaRows + 1);
+        // The panel runs on one thread-block cluster of CL CTAs (8, the portable size, or 16 where the
+        // GPU can co-schedule them) of 512 threads; CTA c holds rows [8192 c / CL, 8192 (c + 1) / CL)
+        // of the panel, 8192 / (512 CL) rows per thread.
+        constexpr int kPanelBlock = 512;
+        template <int CL> struct PanelShape {
+            static constexpr int rows = static_cast<int>(kPanelRows) / CL;  // rows per CTA
+            static constexpr int per_thread = rows / kPanelBlock;
+        };
+        // Dynamic shared memory of panel_factor: the staged multipliers, W x (rows per CTA + 1).
+        template <typename T, int CL> constexpr size_t panel_shared_bytes() {
+            return sizeof(T) * PanelWidth<T>::value * (PanelShape<CL>::rows + 1);
         }
 
         __device__ __forceinline__ void named_sync(unsigned id, unsigned count) {
@@ -185,10 +190,11 @@ namespace sci_cuda {
         // picks the pivot, and one CTA barrier hands it to every thread. Buffers read across the
         // cluster alternate by column parity, so one is rewritten only after a later cluster barrier
         // every reader has passed.
-        template <typename T>
-        __global__ void __cluster_dims__(kClusterCtas, 1, 1) __launch_bounds__(kPanelBlock, 1)
+        template <typename T, int CL>
+        __global__ void __launch_bounds__(kPanelBlock, 1)
                 panel_factor(T *a, unsigned long long n, unsigned long long j0, int width, long long *piv, Movement *moved) {
-            constexpr int W = PanelWidth<T>::value, R = kRowsPerThread, TH = kPanelBlock, WARPS = TH / 32;
+            constexpr int kClusterCtas = CL, kCtaRows = PanelShape<CL>::rows;
+            constexpr int W = PanelWidth<T>::value, R = PanelShape<CL>::per_thread, TH = kPanelBlock, WARPS = TH / 32;
             constexpr int P = kCtaRows + 1;  // pitch of the staged multipliers
             extern __shared__ __align__(16) unsigned char panel_shared[];
             T *stage = reinterpret_cast<T *>(panel_shared);  // stage[k * P + local row]
@@ -453,6 +459,66 @@ namespace sci_cuda {
                 }
                 if (lane == 0) moved->count = __popc(mask_a) + __popc(mask_b);
             }
+        }
+
+        // Launches panel_factor<T, CL> as one cluster of CL CTAs.
+        template <typename T, int CL>
+        cudaError_t launch_panel(cudaStream_t stream, T *a, unsigned long long n, unsigned long long j0, int w, long long *piv,
+                                 Movement *moved) {
+            cudaLaunchConfig_t config{};
+            config.gridDim = dim3(CL);
+            config.blockDim = dim3(kPanelBlock);
+            config.dynamicSmemBytes = panel_shared_bytes<T, CL>();
+            config.stream = stream;
+            cudaLaunchAttribute attribute[1];
+            attribute[0].id = cudaLaunchAttributeClusterDimension;
+            attribute[0].val.clusterDim.x = CL;
+            attribute[0].val.clusterDim.y = 1;
+            attribute[0].val.clusterDim.z = 1;
+            config.attrs = attribute;
+            config.numAttrs = 1;
+            return cudaLaunchKernelEx(&config, panel_factor<T, CL>, a, n, j0, w, piv, moved);
+        }
+
+        // The panel's cluster size for this process: 16 CTAs (half the rows per SM, a non-portable
+        // cluster size) when the GPU can schedule such a cluster, else 8; SCI_CUDA_PANEL_CLUSTER=8 or
+        // 16 asks for one. 0 when neither can run. Decided once per element type.
+        template <typename T> int panel_cluster() {
+            static const int chosen = [] {
+                const int smem8 = static_cast<int>(panel_shared_bytes<T, 8>()), smem16 = static_cast<int>(panel_shared_bytes<T, 16>());
+                cudaFuncSetAttribute(reinterpret_cast<const void *>(&panel_factor<T, 8>),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem8);
+                cudaFuncSetAttribute(reinterpret_cast<const void *>(&panel_factor<T, 16>),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem16);
+                cudaFuncSetAttribute(reinterpret_cast<const void *>(&panel_factor<T, 16>),
+                                     cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+                auto schedulable = [](const void *kernel, int cl, int smem) {
+                    cudaLaunchConfig_t config{};
+                    config.gridDim = dim3(cl);
+                    config.blockDim = dim3(kPanelBlock);
+                    config.dynamicSmemBytes = smem;
+                    cudaLaunchAttribute attribute[1];
+                    attribute[0].id = cudaLaunchAttributeClusterDimension;
+                    attribute[0].val.clusterDim.x = cl;
+                    attribute[0].val.clusterDim.y = 1;
+                    attribute[0].val.clusterDim.z = 1;
+                    config.attrs = attribute;
+                    config.numAttrs = 1;
+                    int clusters = 0;
+                    if (cudaOccupancyMaxActiveClusters(&clusters, kernel, &config) != cudaSuccess) {
+                        cudaGetLastError();
+                        return false;
+                    }
+                    return clusters >= 1;
+                };
+                const bool can16 = schedulable(reinterpret_cast<const void *>(&panel_factor<T, 16>), 16, smem16);
+                const bool can8 = schedulable(reinterpret_cast<const void *>(&panel_factor<T, 8>), 8, smem8);
+                const char *asked = std::getenv("SCI_CUDA_PANEL_CLUSTER");
+                if (asked && std::atoi(asked) == 8 && can8) return 8;
+                if (can16) return 16;
+                return can8 ? 8 : 0;
+            }();
+            return chosen;
         }
 
         // Applies a panel's net row movement to every column outside [skip0, skip1): all reads first,
@@ -868,17 +934,15 @@ namespace sci_cuda {
                                          "reserving the trailing-update workspace"))
                     return code;
             }
-            if (int code = ctx.check(cudaFuncSetAttribute(reinterpret_cast<const void *>(&panel_factor<T>),
-                                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                          static_cast<int>(panel_shared_bytes<T>())),
-                                     "sizing the panel kernel's shared memory"))
-                return code;
+            const int cluster = panel_cluster<T>();
+            if (cluster == 0) return ctx.fail(SCI_CUDA_ERROR_LAUNCH, "the panel kernel's cluster cannot be scheduled");
             for (unsigned long long J0 = 0; J0 < n; J0 += kOuter) {
                 const unsigned long long ob = std::min<unsigned long long>(kOuter, n - J0);
                 for (unsigned long long j0 = J0; j0 < J0 + ob; j0 += W) {
                     const int w = static_cast<int>(std::min<unsigned long long>(W, J0 + ob - j0));
-                    panel_factor<T><<<kClusterCtas, kPanelBlock, panel_shared_bytes<T>(), ctx.stream>>>(a, n, j0, w, piv, moved);
-                    if (int code = ctx.check(cudaGetLastError(), "launching the panel factorisation")) return code;
+                    const cudaError_t launched = cluster == 16 ? launch_panel<T, 16>(ctx.stream, a, n, j0, w, piv, moved)
+                                                               : launch_panel<T, 8>(ctx.stream, a, n, j0, w, piv, moved);
+                    if (int code = ctx.check(launched, "launching the panel factorisation")) return code;
                     move_rows<T><<<static_cast<unsigned>((n + 255) / 256), 256, 0, ctx.stream>>>(a, n, moved, j0, j0 + w);
                     // Inside the outer block only: U rows of the panel, then the rows below it. Columns
                     // beyond the block wait until the block's pivots are all known (a later pivot of
