@@ -3,7 +3,7 @@
 // Each system (n <= 256, one right-hand side, double operands) is factored in FP32 and refined in
 // FP64 inside one CTA, with nothing but its matrix, right-hand side and solution in global memory:
 //  - the FP32 copy of A lives in shared memory: columns [0, sc) of every row, sc = min(n, S), pitch
-//    sc + 1; for n > S (the 256-thread variant, S = 208) thread r also holds columns [S, n) of row r
+//    sc + 1; for n > S (the register variants, S = 192) thread r also holds columns [S, n) of row r
 //    in registers (RC of them), so a 256 x 256 system fits one SM;
 //  - LU with partial pivoting column by column, the reference's rules (include/linear/
 //    decompose.hpp:29-72: the first row with the strictly largest |a|; a zero pivot skips the
@@ -26,7 +26,7 @@ namespace sci_cuda {
     };
 
     constexpr int kSmallMax = 256;       // largest order
-    constexpr int kSmallShared = 208;    // columns kept in shared memory by the register variant
+    constexpr int kSmallShared = 192;    // columns kept in shared memory by the register variant (a multiple of 32)
     constexpr int kSmallRegisters = kSmallMax - kSmallShared;
 
     // Shared memory of one launch for systems up to order `most`.
@@ -109,6 +109,58 @@ namespace sci_cuda {
             if (i == k) v[i] = value;
     }
 
+    // A diagonal block of the blocked sweeps held in registers (columns sc + O .. sc + O + 31): its
+    // rows belong to one warp, thread r holding row r's columns, so the block's triangle is solved
+    // with shuffles and the rows beyond it read their own registers. Ends with a barrier.
+    template <int O, int V>
+    __device__ __forceinline__ void forward_block(const float (&v)[V], float *d, int b0, int bw, int n, int tid, int lane,
+                                                  int warp) {
+        if (warp == b0 / 32) {
+            float di = lane < bw ? d[b0 + lane] : 0.0f;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                if (j < bw) {
+                    const float y = __shfl_sync(0xffffffffu, di, j);
+                    if (lane > j && lane < bw) di = sub(di, mul(v[O + j], y));
+                }
+            }
+            if (lane < bw) d[b0 + lane] = di;
+        }
+        __syncthreads();
+        if (tid >= b0 + bw && tid < n) {
+            float acc = d[tid];
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+                if (j < bw) acc = sub(acc, mul(v[O + j], d[b0 + j]));
+            d[tid] = acc;
+        }
+    }
+    template <int O, int V>
+    __device__ __forceinline__ void backward_block(const float (&v)[V], float *d, int b0, int bw, int n, int tid, int lane,
+                                                   int warp) {
+        if (warp == b0 / 32) {
+            float di = lane < bw ? d[b0 + lane] : 0.0f;
+#pragma unroll
+            for (int j = 31; j >= 0; --j) {
+                if (j < bw) {
+                    const float own = lane == j ? div(di, v[O + j]) : di;
+                    const float z = __shfl_sync(0xffffffffu, own, j);
+                    if (lane == j) di = z;
+                    else if (lane < j) di = sub(di, mul(v[O + j], z));
+                }
+            }
+            if (lane < bw) d[b0 + lane] = di;
+        }
+        __syncthreads();
+        if (tid < b0) {
+            float acc = d[tid];
+#pragma unroll
+            for (int j = 31; j >= 0; --j)
+                if (j < bw) acc = sub(acc, mul(v[O + j], d[b0 + j]));
+            d[tid] = acc;
+        }
+    }
+
     template <int T, int RC>
     __global__ void __launch_bounds__(T) small_solve(const SmallSystem *systems, const unsigned *order, double *errors,
                                                      int *iterations) {
@@ -134,35 +186,43 @@ namespace sci_cuda {
         double *r = x + n;
         float *d = reinterpret_cast<float *>(r + n);
         int *rows = reinterpret_cast<int *>(d + n);
-        const bool owner = RC > 0 && tid < n;  // thread tid holds the register columns of row tid
+        // thread tid holds the register columns of row tid (only systems wider than the shared columns have any)
+        const bool owner = RC > 0 && n > kSmallShared && tid < n;
 
         // load A in FP32 (and |A|_inf, |b|_inf in FP64)
         float v[V];
 #pragma unroll
         for (int k = 0; k < V; ++k) v[k] = 0.0f;
-        for (int e = tid; e < n * sc; e += T) {
-            const int row = e / sc, col = e % sc;
-            A[row * P + col] = static_cast<float>(sys.a[row * n + col]);
+        // one warp per row, each lane's loads of the row issued before its stores; the row's |a| sum
+        // (for |A|_inf) comes from the same loads
+        double row_sum = 0.0, b_max = 0.0;
+        for (int row = tid >> 5; row < n; row += T / 32) {
+            constexpr int G = kSmallMax / 32;
+            double values[G];
+#pragma unroll
+            for (int u = 0; u < G; ++u) {
+                const int col = (tid & 31) + 32 * u;
+                values[u] = col < n ? sys.a[row * n + col] : 0.0;
+            }
+            double sum = 0.0;
+#pragma unroll
+            for (int u = 0; u < G; ++u) {
+                const int col = (tid & 31) + 32 * u;
+                if (col < sc) A[row * P + col] = static_cast<float>(values[u]);
+                sum += fabs(values[u]);
+            }
+#pragma unroll
+            for (int offset = 16; offset > 0; offset >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, offset);
+            row_sum = (sum > row_sum || sum != sum) ? sum : row_sum;
         }
         if (RC > 0 && owner) {
 #pragma unroll
             for (int k = 0; k < V; ++k)
                 if (sc + k < n) v[k] = static_cast<float>(sys.a[tid * n + sc + k]);
         }
-        double row_sum = 0.0, b_max = 0.0;
-        {
-            const int lane = tid & 31, warp = tid >> 5;
-            for (int row = warp; row < n; row += T / 32) {  // one warp per row, coalesced
-                double s = 0.0;
-                for (int c = lane; c < n; c += 32) s += fabs(sys.a[row * n + c]);
-#pragma unroll
-                for (int offset = 16; offset > 0; offset >>= 1) s += __shfl_xor_sync(0xffffffffu, s, offset);
-                row_sum = (s > row_sum || s != s) ? s : row_sum;
-            }
-            for (int row = tid; row < n; row += T) {
-                const double bv = fabs(sys.b[row]);
-                b_max = (bv > b_max || bv != bv) ? bv : b_max;
-            }
+        for (int row = tid; row < n; row += T) {
+            const double bv = fabs(sys.b[row]);
+            b_max = (bv > b_max || bv != bv) ? bv : b_max;
         }
         const double a_norm = block_max<T>(row_sum, reduce_scratch);
         const double b_norm = block_max<T>(b_max, reduce_scratch);
@@ -198,7 +258,7 @@ namespace sci_cuda {
                     A[j * P + c] = A[p * P + c];
                     A[p * P + c] = t0;
                 }
-                if (RC > 0) {
+                if (RC > 0 && n > sc) {
                     if (tid == p) {
 #pragma unroll
                         for (int k = 0; k < V; ++k) swap_reg[k] = v[k];
@@ -224,11 +284,13 @@ namespace sci_cuda {
                 }
             }
             __syncthreads();
-            if (RC > 0 && tid == j) {
+            if (RC > 0 && n > sc) {
+                if (tid == j) {
 #pragma unroll
-                for (int k = 0; k < V; ++k) pivot_reg[k] = v[k];
+                    for (int k = 0; k < V; ++k) pivot_reg[k] = v[k];
+                }
+                __syncthreads();
             }
-            __syncthreads();
             const float diagonal = j < sc ? A[j * P + j] : pivot_reg[j - sc];
             if (diagonal != 0.0f) {
                 // multipliers
@@ -238,20 +300,38 @@ namespace sci_cuda {
                     place<V>(v, j - sc, div(pick<V>(v, j - sc), diagonal));
                 }
                 __syncthreads();
-                // rank-1 update of the shared columns: a warp walks 32 consecutive columns of a row
+                // rank-1 update of the shared columns: lane l keeps the pivot row's columns
+                // j + 1 + l + 32 u in registers for the whole step, and a warp walks its rows with every
+                // load of a row issued before the row's stores (no chain through shared memory)
                 if (j + 1 < sc) {
+                    constexpr int G = kSmallMax / 32;
+                    const int lane = tid & 31, cols = sc - j - 1;
+                    float pivot[G];
+#pragma unroll
+                    for (int u = 0; u < G; ++u) pivot[u] = lane + 32 * u < cols ? A[j * P + j + 1 + lane + 32 * u] : 0.0f;
                     for (int row = j + 1 + tid / 32; row < n; row += T / 32) {
+                        float *target = A + row * P + j + 1;
                         const float l = A[row * P + j];
-                        for (int c = j + 1 + (tid & 31); c < sc; c += 32)
-                            A[row * P + c] = sub(A[row * P + c], mul(l, A[j * P + c]));
+                        float old[G];
+#pragma unroll
+                        for (int u = 0; u < G; ++u)
+                            if (lane + 32 * u < cols) old[u] = target[lane + 32 * u];
+#pragma unroll
+                        for (int u = 0; u < G; ++u)
+                            if (lane + 32 * u < cols) target[lane + 32 * u] = sub(old[u], mul(l, pivot[u]));
                     }
                 }
-                // and of this thread's register columns
+                // and of this thread's register columns, in halves of 32 that hold live columns
                 if (RC > 0 && owner && tid > j) {
                     const float l = j < sc ? A[tid * P + j] : pick<V>(v, j - sc);
 #pragma unroll
-                    for (int k = 0; k < V; ++k)
-                        if (sc + k > j && sc + k < n) v[k] = sub(v[k], mul(l, pivot_reg[k]));
+                    for (int h = 0; h < V / 32; ++h) {
+                        if (n > sc + 32 * h && j < sc + 32 * h + 31) {
+#pragma unroll
+                            for (int k = 32 * h; k < 32 * h + 32; ++k)
+                                if (sc + k > j && sc + k < n) v[k] = sub(v[k], mul(l, pivot_reg[k]));
+                        }
+                    }
                 }
             }
             __syncthreads();
@@ -270,6 +350,68 @@ namespace sci_cuda {
             // d = P r in FP32
             for (int i = tid; i < n; i += T) d[i] = static_cast<float>(r[rows[i]]);
             __syncthreads();
+            if (T >= n) {
+                // Blocked sweeps: every 32-row block belongs to one warp (thread r holds row r), which
+                // solves the block's triangle with shuffles; one barrier later the threads of the rows
+                // beyond it apply the block. Each row sees its updates in the same order as the
+                // column-by-column sweep below, so the result is the same to the bit.
+                for (int b0 = 0; b0 < n; b0 += 32) {
+                    const int bw = n - b0 < 32 ? n - b0 : 32;
+                    if (b0 >= sc) {
+                        if constexpr (RC > 0) {
+                            if (b0 - sc == 0) forward_block<0>(v, d, b0, bw, n, tid, lane, warp);
+                            else forward_block<32>(v, d, b0, bw, n, tid, lane, warp);
+                        }
+                    } else {
+                        if (warp == b0 / 32) {
+                            float di = lane < bw ? d[b0 + lane] : 0.0f;
+                            for (int j = 0; j < bw; ++j) {
+                                const float y = __shfl_sync(0xffffffffu, di, j);
+                                if (lane > j && lane < bw) di = sub(di, mul(A[(b0 + lane) * P + b0 + j], y));
+                            }
+                            if (lane < bw) d[b0 + lane] = di;
+                        }
+                        __syncthreads();
+                        if (tid >= b0 + bw && tid < n) {
+                            float acc = d[tid];
+                            for (int j = 0; j < bw; ++j) acc = sub(acc, mul(A[tid * P + b0 + j], d[b0 + j]));
+                            d[tid] = acc;
+                        }
+                    }
+                    __syncthreads();
+                }
+                for (int b0 = (n - 1) / 32 * 32; b0 >= 0; b0 -= 32) {
+                    const int bw = n - b0 < 32 ? n - b0 : 32;
+                    if (b0 >= sc) {
+                        if constexpr (RC > 0) {
+                            if (b0 - sc == 0) backward_block<0>(v, d, b0, bw, n, tid, lane, warp);
+                            else backward_block<32>(v, d, b0, bw, n, tid, lane, warp);
+                        }
+                    } else {
+                        if (warp == b0 / 32) {
+                            float di = lane < bw ? d[b0 + lane] : 0.0f;
+                            for (int j = bw - 1; j >= 0; --j) {
+                                const float own = lane == j ? div(di, A[(b0 + j) * P + b0 + j]) : di;
+                                const float z = __shfl_sync(0xffffffffu, own, j);
+                                if (lane == j) di = z;
+                                else if (lane < j) di = sub(di, mul(A[(b0 + lane) * P + b0 + j], z));
+                            }
+                            if (lane < bw) d[b0 + lane] = di;
+                        }
+                        __syncthreads();
+                        if (tid < b0) {
+                            float acc = d[tid];
+                            for (int j = bw - 1; j >= 0; --j) {
+                                const int col = b0 + j;
+                                const float u = col < sc ? A[tid * P + col] : pick<V>(v, col - sc);
+                                acc = sub(acc, mul(u, d[col]));
+                            }
+                            d[tid] = acc;
+                        }
+                    }
+                    __syncthreads();
+                }
+            } else {
             // forward: unit lower, column by column
             for (int j = 0; j < n; ++j) {
                 const float y = d[j];
@@ -306,13 +448,21 @@ namespace sci_cuda {
                 }
                 __syncthreads();
             }
+            }
             // x += d; r = b - A x in FP64, one warp per row
             for (int i = tid; i < n; i += T) x[i] += static_cast<double>(d[i]);
             __syncthreads();
             double r_max = 0.0, x_max = 0.0;
             for (int row = warp; row < n; row += T / 32) {
+                // every load of the row is issued before the first multiply
+                constexpr int G = kSmallMax / 32;
+                double values[G];
+#pragma unroll
+                for (int u = 0; u < G; ++u) values[u] = lane + 32 * u < n ? sys.a[row * n + lane + 32 * u] : 0.0;
                 double s = 0.0;
-                for (int c = lane; c < n; c += 32) s = fma(sys.a[row * n + c], x[c], s);
+#pragma unroll
+                for (int u = 0; u < G; ++u)
+                    if (lane + 32 * u < n) s = fma(values[u], x[lane + 32 * u], s);
 #pragma unroll
                 for (int offset = 16; offset > 0; offset >>= 1) s += __shfl_xor_sync(0xffffffffu, s, offset);
                 const double residual = sys.b[row] - s;
