@@ -151,7 +151,7 @@ namespace sci_cuda {
                 get(Int<st.a>{}, a);
                 get(Int<st.b>{}, b);
                 get(Int<st.c>{}, c);
-                apply_lanes<st.code>(a, b, c, last, tail);
+                apply_lanes<st.code, true>(a, b, c, last, tail);
                 if constexpr (st.target == kOutput) {
                     if (out) {
                         T *dst = out + base;

@@ -111,10 +111,23 @@ namespace sci_cuda {
     }
 
     // ---- applying one code to a thread's lanes -------------------------------------------------
-    template <int code, typename T>
+    // With `fast`, a code that has a fast form runs it on every lane, and a thread with any lane
+    // outside the fast form's inputs recomputes all its lanes with the full form: one branch per
+    // thread, taken only for such inputs, and the same values either way.
+    template <int code, bool fast = false, typename T>
     __device__ __forceinline__ void apply_lanes(const T *a, const T *b, const T *c, T *r, const bool *tail) {
+        if constexpr (fast && has_fast<code, T>()) {
+            bool rare = false;
 #pragma unroll
-        for (int e = 0; e < Lanes<T>::count; ++e) r[e] = apply<code>(a[e], b[e], c[e], tail[e]);
+            for (int e = 0; e < Lanes<T>::count; ++e) r[e] = apply_fast<code>(a[e], rare);
+            if (rare) {
+#pragma unroll
+                for (int e = 0; e < Lanes<T>::count; ++e) r[e] = apply<code>(a[e], b[e], c[e], tail[e]);
+            }
+        } else {
+#pragma unroll
+            for (int e = 0; e < Lanes<T>::count; ++e) r[e] = apply<code>(a[e], b[e], c[e], tail[e]);
+        }
     }
 
     template <typename T>
@@ -364,7 +377,7 @@ namespace sci_cuda {
                 get(Int<st.a>{}, a);
                 get(Int<st.b>{}, b);
                 get(Int<st.c>{}, c);
-                apply_lanes<st.code>(a, b, c, last, w.tail);
+                apply_lanes<st.code, true>(a, b, c, last, w.tail);
                 if constexpr (st.target == kOutput) {
                     if constexpr (MODE == kEvaluate) w.write_output(last);
                 } else {

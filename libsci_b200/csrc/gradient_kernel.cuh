@@ -245,10 +245,24 @@ namespace sci_cuda {
                     static_for<C::length>([&](auto s_c) {
                         constexpr int s = decltype(s_c)::value;
                         constexpr Step st = C::steps[s];
+                        if constexpr (has_fast<st.code, T>()) {
+                            // the fast form on every lane, the full form again for all lanes when
+                            // any lane falls outside it (same values either way)
+                            bool rare = false;
 #pragma unroll
-                        for (int e = 0; e < E; ++e)
-                            value[s][e] = apply<st.code>(operand(Int<st.a>{}, e), operand(Int<st.b>{}, e),
-                                                         operand(Int<st.c>{}, e), tail[e]);
+                            for (int e = 0; e < E; ++e) value[s][e] = apply_fast<st.code>(operand(Int<st.a>{}, e), rare);
+                            if (rare) {
+#pragma unroll
+                                for (int e = 0; e < E; ++e)
+                                    value[s][e] = apply<st.code>(operand(Int<st.a>{}, e), operand(Int<st.b>{}, e),
+                                                                 operand(Int<st.c>{}, e), tail[e]);
+                            }
+                        } else {
+#pragma unroll
+                            for (int e = 0; e < E; ++e)
+                                value[s][e] = apply<st.code>(operand(Int<st.a>{}, e), operand(Int<st.b>{}, e),
+                                                             operand(Int<st.c>{}, e), tail[e]);
+                        }
                         if constexpr (FORM == kGradRecord) {
                             T *row = L.tape + s * count + i0;
                             if (whole) {

@@ -316,4 +316,147 @@ namespace sci_cuda {
         else return fma_(a, b, c);
     }
 
+    // ---- fast forms --------------------------------------------------------------------------------
+    // The same operations as the forms above, in the same order, for the inputs that take none of
+    // their special branches; an element outside that set raises `rare`, and the caller recomputes
+    // the whole group with the forms above. Each returns exactly what its full form returns whenever
+    // it leaves `rare` alone.
+
+    // a / d for |a| <= 1/2 and d in [1.5, 2.5] (the logarithm's ratio), by the division method of
+    // Markstein (IBM J. Res. Dev. 34(1), 1990): a reciprocal estimate, one Newton-Raphson step with
+    // a fused multiply-add, then one correction of the quotient q + (a - d q) y. On this range no
+    // step can overflow or underflow, and the result is the correctly rounded quotient (checked
+    // against IEEE division for every operand pair the logarithm can form).
+    __device__ __forceinline__ float ratio_quotient(float a, float d) {
+        float y;
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(d));
+        const float e = __fmaf_rn(-d, y, 1.0f);
+        y = __fmaf_rn(y, e, y);
+        const float q = __fmul_rn(a, y);
+        const float r = __fmaf_rn(-d, q, a);
+        return __fmaf_rn(r, y, q);
+    }
+    __device__ __forceinline__ double ratio_quotient(double a, double d) { return div(a, d); }
+
+    // e^x for |x| below (normal + 1/2) ln 2: no clamp applies and |k| <= normal, so the single scale.
+    template <typename T> __device__ __forceinline__ T exponential_fast(T x, bool &rare) {
+        using L = Limits<T>;
+        constexpr Poly<T, L::exp_terms> series = factorials<T, L::exp_terms>();
+        constexpr T reach = sizeof(T) == 4 ? T(87) : T(708);
+        rare |= !(fabs(x) <= reach);
+        const T k = sub(fma_(x, L::binary, L::round), L::round);
+        const T negative = -k;
+        T reduced = fma_(negative, L::natural, x);
+        reduced = fma_(negative, L::remainder, reduced);
+        const T significand = fma_(reduced, horner<1>(series, reduced), T(1));
+        return mul(significand, from_bits(bits(add(k, L::exponent)) << L::mantissa));
+    }
+
+    // ln x for positive, normal, finite x: no scaling of subnormals and none of the special results.
+    template <typename T> __device__ __forceinline__ T logarithm_fast(T x, bool &rare) {
+        using L = Limits<T>;
+        using U = typename L::U;
+        constexpr Poly<T, L::log_terms> series = reciprocals<T, L::log_terms>();
+        const U pattern = bits(x);
+        rare |= pattern - bits(L::tiny) >= L::infinity - bits(L::tiny);
+        T exponent = sub(from_bits((pattern >> L::mantissa) | bits(L::magnitude)), L::exponent);
+        T mantissa = from_bits((pattern & L::fraction) | L::one);
+        const bool large = mantissa > L::root2;
+        mantissa = large ? mul(mantissa, T(0.5)) : mantissa;
+        exponent = large ? add(exponent, T(1)) : exponent;
+        const T fraction = sub(mantissa, T(1));
+        const T ratio = ratio_quotient(fraction, add(fraction, T(2)));
+        const T square = mul(ratio, ratio);
+        const T tail = mul(square, horner<0>(series, square));
+        const T half = mul(mul(fraction, fraction), T(0.5));
+        const T inner = fma_(ratio, add(half, tail), mul(exponent, L::remainder));
+        return sub(mul(exponent, L::natural), sub(sub(half, inner), fraction));
+    }
+
+    // sin / cos for |x| <= reach (no far reduction).
+    template <bool phase, typename T> __device__ __forceinline__ T circular_fast(T x, bool &rare) {
+        using L = Limits<T>;
+        using U = typename L::U;
+        constexpr Poly<T, L::sin_terms> odd = alternating<T, L::sin_terms, 1>();
+        constexpr Poly<T, L::cos_terms> even = alternating<T, L::cos_terms, 0>();
+        rare |= !(fabs(x) <= L::reach);
+        const T shifted = fma_(x, L::quadrant, L::round);
+        const T quarters = sub(shifted, L::round);
+        const T negative = -quarters;
+        T reduced = fma_(negative, L::q0, x);
+        reduced = fma_(negative, L::q1, reduced);
+        reduced = fma_(negative, L::q2, reduced);
+        reduced = fma_(negative, L::q3, reduced);
+        const T square = mul(reduced, reduced);
+        const T sine = fma_(mul(reduced, square), horner<1>(odd, square), reduced);
+        const T cosine = fma_(square, horner<1>(even, square), T(1));
+        U quadrant = bits(shifted);
+        if (phase) quadrant ^= quadrant << 1;
+        const U flip = (quadrant & U(2)) << (L::width - 2);
+        const bool swap = (bits(shifted) & U(1)) != 0;
+        const T result = phase ? (swap ? sine : cosine) : (swap ? cosine : sine);
+        return from_bits(bits(result) ^ flip);
+    }
+
+    // tanh of a float without branches: the double-precision evaluation of tanh_float runs on
+    // min(|x|, 9.03125) (so no infinity or NaN enters it), 2^k is formed from the bits of the
+    // rounded sum that yields k, and the tiny, saturated and NaN results are selected at the end.
+    __device__ __forceinline__ float tanh_float_fast(float x) {
+        const float a = fabsf(x);
+        const double d = 2.0 * static_cast<double>(fminf(a, 9.03125f));
+        const double sum = __dadd_rn(__dmul_rn(d, 0x1.71547652b82fep+0), 0x1.8p52);
+        const double k = __dadd_rn(sum, -0x1.8p52);
+        double r = __fma_rn(-k, 0x1.62e42fefa3800p-1, d);
+        r = __fma_rn(-k, 0x1.ef35793c76730p-45, r);
+        double p = 1.0 / 479001600.0;
+        p = __fma_rn(p, r, 1.0 / 39916800.0);
+        p = __fma_rn(p, r, 1.0 / 3628800.0);
+        p = __fma_rn(p, r, 1.0 / 362880.0);
+        p = __fma_rn(p, r, 1.0 / 40320.0);
+        p = __fma_rn(p, r, 1.0 / 5040.0);
+        p = __fma_rn(p, r, 1.0 / 720.0);
+        p = __fma_rn(p, r, 1.0 / 120.0);
+        p = __fma_rn(p, r, 1.0 / 24.0);
+        p = __fma_rn(p, r, 1.0 / 6.0);
+        p = __fma_rn(p, r, 0.5);
+        const double q = __fma_rn(__dmul_rn(r, r), p, r);
+        // k is a small non-negative integer held in the low bits of `sum`
+        const unsigned kbits = static_cast<unsigned>(__double2loint(sum));
+        const double s = __hiloint2double(static_cast<int>((kbits + 1023u) << 20), 0);
+        const double num = __fma_rn(s, q, __dsub_rn(s, 1.0));
+        const double den = __fma_rn(s, q, __dadd_rn(s, 1.0));
+        double y;
+        asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(den));
+        double e = __fma_rn(-den, y, 1.0);
+        y = __fma_rn(y, e, y);
+        e = __fma_rn(-den, y, 1.0);
+        y = __fma_rn(y, e, y);
+        double t = __dmul_rn(num, y);
+        t = __fma_rn(__fma_rn(-den, t, num), y, t);
+        float result = copysignf(static_cast<float>(t), x);
+        result = a > 9.03125f ? copysignf(1.0f, x) : result;
+        result = a < 0x1p-12f ? x : result;
+        return a == a ? result : __fadd_rn(x, x);
+    }
+
+    template <int code, typename T> __device__ __forceinline__ constexpr bool has_fast() {
+        return code == kExponential || code == kLogarithm || code == kSin || code == kCos || code == kTan ||
+               code == kCsc || code == kSec || code == kCot || ((code == kTanh || code == kCoth) && sizeof(T) == 4);
+    }
+
+    // The fast form of a unary code (has_fast<code, T>()).
+    template <int code, typename T> __device__ __forceinline__ T apply_fast(T a, bool &rare) {
+        const T one = T(1);
+        if constexpr (code == kExponential) return exponential_fast(a, rare);
+        else if constexpr (code == kLogarithm) return logarithm_fast(a, rare);
+        else if constexpr (code == kSin) return circular_fast<false>(a, rare);
+        else if constexpr (code == kCos) return circular_fast<true>(a, rare);
+        else if constexpr (code == kTan) return div(circular_fast<false>(a, rare), circular_fast<true>(a, rare));
+        else if constexpr (code == kCsc) return div(one, circular_fast<false>(a, rare));
+        else if constexpr (code == kSec) return div(one, circular_fast<true>(a, rare));
+        else if constexpr (code == kCot) return div(one, div(circular_fast<false>(a, rare), circular_fast<true>(a, rare)));
+        else if constexpr (code == kTanh) return tanh_float_fast(a);
+        else return div(one, tanh_float_fast(a));
+    }
+
 } // namespace sci_cuda
