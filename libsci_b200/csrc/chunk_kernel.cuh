@@ -111,15 +111,21 @@ namespace sci_cuda {
     }
 
     // ---- applying one code to a thread's lanes -------------------------------------------------
-    // With `fast`, a code that has a fast form runs it on every lane, and a thread with any lane
-    // outside the fast form's inputs recomputes all its lanes with the full form: one branch per
-    // thread, taken only for such inputs, and the same values either way.
+    // With `fast`, a code that has a fast form runs it on every lane (two lanes per instruction where
+    // it has a paired form), and a thread with any lane outside the fast form's inputs recomputes all
+    // its lanes with the full form: one branch per thread, taken only for such inputs, and the same
+    // values either way.
     template <int code, bool fast = false, typename T>
     __device__ __forceinline__ void apply_lanes(const T *a, const T *b, const T *c, T *r, const bool *tail) {
         if constexpr (fast && has_fast<code, T>()) {
             bool rare = false;
+            if constexpr (has_pair<code, T>()) {
 #pragma unroll
-            for (int e = 0; e < Lanes<T>::count; ++e) r[e] = apply_fast<code>(a[e], rare);
+                for (int e = 0; e < Lanes<T>::count; e += 2) apply_pair<code>(a[e], a[e + 1], rare, r[e], r[e + 1]);
+            } else {
+#pragma unroll
+                for (int e = 0; e < Lanes<T>::count; ++e) r[e] = apply_fast<code>(a[e], rare);
+            }
             if (rare) {
 #pragma unroll
                 for (int e = 0; e < Lanes<T>::count; ++e) r[e] = apply<code>(a[e], b[e], c[e], tail[e]);
@@ -564,10 +570,9 @@ namespace sci_cuda {
                 }
             }
             unsigned long long n = 0;
+            unsigned s = 0, parity = 0;  // ring slot and phase of tile n, advanced without a division
             bool failed = false;
             for (unsigned long long k = blockIdx.x; k < full; k += grid, ++n) {
-                const unsigned s = static_cast<unsigned>(n % S);
-                const unsigned parity = static_cast<unsigned>((n / S) & 1);
                 const bool ok = barrier_wait(&bars[s], parity);
                 if (__syncthreads_or(!ok)) {
                     failed = true;
@@ -581,6 +586,10 @@ namespace sci_cuda {
                 if (t == 0) {
                     const unsigned long long next = k + S * grid;
                     if (next < full) issue(s, next);
+                }
+                if (++s == S) {
+                    s = 0;
+                    parity ^= 1u;
                 }
             }
             if (failed) {

@@ -399,12 +399,18 @@ namespace sci_cuda {
     }
 
     // tanh of a float without branches: the double-precision evaluation of tanh_float runs on
-    // min(|x|, 9.03125) (so no infinity or NaN enters it), 2^k is formed from the bits of the
-    // rounded sum that yields k, and the tiny, saturated and NaN results are selected at the end.
+    // min(|x|, 9.03125) (so no infinity or NaN enters it), and the tiny, saturated and NaN results
+    // are selected at the end. Three changes cut its FP64 work: 2|x| is assembled as a double from
+    // the float's fields with integer operations (exact for every normal float; the others are
+    // selected away), k is rounded from one fused multiply-add and 2^k is formed from the bits of
+    // that sum, and the reciprocal takes one Newton-Raphson step, since the final correction of the
+    // quotient squares its error. Its float results equal tanh_float's for every float input.
     __device__ __forceinline__ float tanh_float_fast(float x) {
         const float a = fabsf(x);
-        const double d = 2.0 * static_cast<double>(fminf(a, 9.03125f));
-        const double sum = __dadd_rn(__dmul_rn(d, 0x1.71547652b82fep+0), 0x1.8p52);
+        const unsigned field = __float_as_uint(fminf(a, 9.03125f));
+        // sign 0; exponent e - 127 + 1023 + 1 (the factor 2); the 23 fraction bits at the top of 52
+        const double d = __hiloint2double(static_cast<int>((field >> 3) + (897u << 20)), static_cast<int>(field << 29));
+        const double sum = __fma_rn(d, 0x1.71547652b82fep+0, 0x1.8p52);
         const double k = __dadd_rn(sum, -0x1.8p52);
         double r = __fma_rn(-k, 0x1.62e42fefa3800p-1, d);
         r = __fma_rn(-k, 0x1.ef35793c76730p-45, r);
@@ -427,16 +433,183 @@ namespace sci_cuda {
         const double den = __fma_rn(s, q, __dadd_rn(s, 1.0));
         double y;
         asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(den));
-        double e = __fma_rn(-den, y, 1.0);
-        y = __fma_rn(y, e, y);
-        e = __fma_rn(-den, y, 1.0);
-        y = __fma_rn(y, e, y);
+        y = __fma_rn(y, __fma_rn(-den, y, 1.0), y);
         double t = __dmul_rn(num, y);
         t = __fma_rn(__fma_rn(-den, t, num), y, t);
         float result = copysignf(static_cast<float>(t), x);
         result = a > 9.03125f ? copysignf(1.0f, x) : result;
         result = a < 0x1p-12f ? x : result;
         return a == a ? result : __fadd_rn(x, x);
+    }
+
+    // ---- two floats per instruction ----------------------------------------------------------------
+    // sm_100 adds packed two-lane FP32 arithmetic (add / sub / mul / fma .rn .f32x2): each lane is
+    // rounded exactly as the one-lane instruction rounds it, and one instruction issues for both. The
+    // paired fast forms below run the fast forms' floating-point steps on two elements at once
+    // (integer, compare and select steps stay per lane) and return the same bits. Where a fast form
+    // multiplies by a negated value, the pair form multiplies by the negated constant instead: the
+    // exact products are equal, so the rounded results are.
+    struct Pair {
+        unsigned long long v;
+    };
+    __device__ __forceinline__ Pair pair(float lo, float hi) {
+        Pair p;
+        asm("mov.b64 %0, {%1, %2};" : "=l"(p.v) : "f"(lo), "f"(hi));
+        return p;
+    }
+    __device__ __forceinline__ Pair pair(float both) { return pair(both, both); }
+    __device__ __forceinline__ void unpair(Pair p, float &lo, float &hi) {
+        asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(p.v));
+    }
+    __device__ __forceinline__ Pair add(Pair a, Pair b) {
+        Pair d;
+        asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+        return d;
+    }
+    __device__ __forceinline__ Pair sub(Pair a, Pair b) {
+        Pair d;
+        asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+        return d;
+    }
+    __device__ __forceinline__ Pair mul(Pair a, Pair b) {
+        Pair d;
+        asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d.v) : "l"(a.v), "l"(b.v));
+        return d;
+    }
+    __device__ __forceinline__ Pair fma_(Pair a, Pair b, Pair c) {
+        Pair d;
+        asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+        return d;
+    }
+    template <int from, int N> __device__ __forceinline__ Pair horner(const Poly<float, N> &p, Pair x) {
+        Pair r = pair(p.c[N - 1]);
+#pragma unroll
+        for (int k = N - 2; k >= from; --k) r = fma_(r, x, pair(p.c[k]));
+        return r;
+    }
+
+    // exponential_fast on two elements.
+    __device__ __forceinline__ void exponential_pair(float x0, float x1, bool &rare, float &r0, float &r1) {
+        using L = Limits<float>;
+        constexpr Poly<float, L::exp_terms> series = factorials<float, L::exp_terms>();
+        rare |= !(fabsf(x0) <= 87.0f) | !(fabsf(x1) <= 87.0f);
+        const Pair x = pair(x0, x1);
+        const Pair k = sub(fma_(x, pair(L::binary), pair(L::round)), pair(L::round));
+        Pair reduced = fma_(k, pair(-L::natural), x);
+        reduced = fma_(k, pair(-L::remainder), reduced);
+        const Pair significand = fma_(reduced, horner<1>(series, reduced), pair(1.0f));
+        float e0, e1;
+        unpair(add(k, pair(L::exponent)), e0, e1);
+        const Pair scale = pair(from_bits(bits(e0) << L::mantissa), from_bits(bits(e1) << L::mantissa));
+        unpair(mul(significand, scale), r0, r1);
+    }
+
+    // logarithm_fast on two elements. The two selects of the `large` adjustment become a multiply by
+    // 1/2 or 1 and an add of 1 or 0 (exact either way; the exponent is never -0).
+    __device__ __forceinline__ void logarithm_pair(float x0, float x1, bool &rare, float &r0, float &r1) {
+        using L = Limits<float>;
+        constexpr Poly<float, L::log_terms> series = reciprocals<float, L::log_terms>();
+        const unsigned p0 = bits(x0), p1 = bits(x1);
+        rare |= (p0 - bits(L::tiny) >= L::infinity - bits(L::tiny)) | (p1 - bits(L::tiny) >= L::infinity - bits(L::tiny));
+        const Pair field = pair(from_bits((p0 >> L::mantissa) | bits(L::magnitude)),
+                                from_bits((p1 >> L::mantissa) | bits(L::magnitude)));
+        const float m0 = from_bits((p0 & L::fraction) | L::one), m1 = from_bits((p1 & L::fraction) | L::one);
+        const bool g0 = m0 > L::root2, g1 = m1 > L::root2;
+        const Pair mantissa = mul(pair(m0, m1), pair(g0 ? 0.5f : 1.0f, g1 ? 0.5f : 1.0f));
+        const Pair exponent = add(sub(field, pair(L::exponent)), pair(g0 ? 1.0f : 0.0f, g1 ? 1.0f : 0.0f));
+        const Pair fraction = sub(mantissa, pair(1.0f));
+        // ratio_quotient(fraction, fraction + 2) with the negated divisor formed directly
+        const Pair divisor = add(fraction, pair(2.0f));
+        const Pair negated = sub(pair(-2.0f), fraction);
+        float d0, d1, y0, y1;
+        unpair(divisor, d0, d1);
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y0) : "f"(d0));
+        asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y1) : "f"(d1));
+        Pair y = pair(y0, y1);
+        y = fma_(y, fma_(negated, y, pair(1.0f)), y);
+        const Pair q = mul(fraction, y);
+        const Pair ratio = fma_(fma_(negated, q, fraction), y, q);
+        const Pair square = mul(ratio, ratio);
+        // One-lane multiplies for the tail: a packed multiply feeding the packed add below can be
+        // fused into one packed fma by the code generator (seen on sm_100a despite .rn), which
+        // changes the rounding; the other products that feed adds here are exact (mantissa x 1/2,
+        // fraction^2 x 1/2, exponent x 355/512), so fusing them changes nothing.
+        float s0, s1, h0, h1;
+        unpair(square, s0, s1);
+        unpair(horner<0>(series, square), h0, h1);
+        const Pair tail = pair(mul(s0, h0), mul(s1, h1));
+        const Pair half = mul(mul(fraction, fraction), pair(0.5f));
+        const Pair inner = fma_(ratio, add(half, tail), mul(exponent, pair(L::remainder)));
+        unpair(sub(mul(exponent, pair(L::natural)), sub(sub(half, inner), fraction)), r0, r1);
+    }
+
+    // circular_fast<phase> on two elements.
+    template <bool phase>
+    __device__ __forceinline__ void circular_pair(float x0, float x1, bool &rare, float &r0, float &r1) {
+        using L = Limits<float>;
+        constexpr Poly<float, L::sin_terms> odd = alternating<float, L::sin_terms, 1>();
+        constexpr Poly<float, L::cos_terms> even = alternating<float, L::cos_terms, 0>();
+        rare |= !(fabsf(x0) <= L::reach) | !(fabsf(x1) <= L::reach);
+        const Pair x = pair(x0, x1);
+        const Pair shifted = fma_(x, pair(L::quadrant), pair(L::round));
+        const Pair quarters = sub(shifted, pair(L::round));
+        Pair reduced = fma_(quarters, pair(-L::q0), x);
+        reduced = fma_(quarters, pair(-L::q1), reduced);
+        reduced = fma_(quarters, pair(-L::q2), reduced);
+        reduced = fma_(quarters, pair(-L::q3), reduced);
+        const Pair square = mul(reduced, reduced);
+        const Pair sine = fma_(mul(reduced, square), horner<1>(odd, square), reduced);
+        const Pair cosine = fma_(square, horner<1>(even, square), pair(1.0f));
+        float s[2], c[2], h[2], out[2];
+        unpair(sine, s[0], s[1]);
+        unpair(cosine, c[0], c[1]);
+        unpair(shifted, h[0], h[1]);
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            unsigned quadrant = bits(h[i]);
+            if (phase) quadrant ^= quadrant << 1;
+            const unsigned flip = (quadrant & 2u) << 30;
+            const bool swap = (bits(h[i]) & 1u) != 0;
+            const float result = phase ? (swap ? s[i] : c[i]) : (swap ? c[i] : s[i]);
+            out[i] = from_bits(bits(result) ^ flip);
+        }
+        r0 = out[0];
+        r1 = out[1];
+    }
+
+    template <int code, typename T> __device__ __forceinline__ constexpr bool has_pair() {
+        return sizeof(T) == 4 && (code == kExponential || code == kLogarithm || code == kSin || code == kCos ||
+                                  code == kTan || code == kCsc || code == kSec || code == kCot);
+    }
+
+    // The paired fast form of a code (has_pair<code, float>()).
+    template <int code> __device__ __forceinline__ void apply_pair(float a0, float a1, bool &rare, float &r0, float &r1) {
+        if constexpr (code == kExponential) {
+            exponential_pair(a0, a1, rare, r0, r1);
+        } else if constexpr (code == kLogarithm) {
+            logarithm_pair(a0, a1, rare, r0, r1);
+        } else if constexpr (code == kSin) {
+            circular_pair<false>(a0, a1, rare, r0, r1);
+        } else if constexpr (code == kCos) {
+            circular_pair<true>(a0, a1, rare, r0, r1);
+        } else {
+            float s0, s1, c0, c1;
+            if constexpr (code != kSec) circular_pair<false>(a0, a1, rare, s0, s1);
+            if constexpr (code != kCsc) circular_pair<true>(a0, a1, rare, c0, c1);
+            if constexpr (code == kTan) {
+                r0 = div(s0, c0);
+                r1 = div(s1, c1);
+            } else if constexpr (code == kCsc) {
+                r0 = div(1.0f, s0);
+                r1 = div(1.0f, s1);
+            } else if constexpr (code == kSec) {
+                r0 = div(1.0f, c0);
+                r1 = div(1.0f, c1);
+            } else {
+                r0 = div(1.0f, div(s0, c0));
+                r1 = div(1.0f, div(s1, c1));
+            }
+        }
     }
 
     template <int code, typename T> __device__ __forceinline__ constexpr bool has_fast() {

@@ -194,9 +194,13 @@ namespace sci_cuda {
                 if (nvrtcCreateProgram(&program, source.c_str(), "sci_specialized.cu", 4, headers, names) != NVRTC_SUCCESS)
                     return entry;
                 nvrtcAddNameExpression(program, name.c_str());
+                // --fmad=false: the chunk codes are exact sequences of rounded operations, so no
+                // multiply and add may be contracted behind their back; the packed two-lane forms
+                // need it most, since ptxas would otherwise fuse a packed multiply into a following
+                // packed add.
                 const char *options[] = {"-default-device", "-arch=sm_100a", "-std=c++17", "-lineinfo",
-                                         "--extra-device-vectorization"};
-                const nvrtcResult built = nvrtcCompileProgram(program, 5, options);
+                                         "--extra-device-vectorization", "--fmad=false"};
+                const nvrtcResult built = nvrtcCompileProgram(program, 6, options);
                 if (built != NVRTC_SUCCESS) {
                     if (trace) {
                         size_t size = 0;

@@ -1,0 +1,87 @@
+"""The fast forms of exp, log, the sin/cos family and float tanh (sci_math.cuh) against the full
+forms they shortcut: every one of the 2^32 float inputs and 2^31 sampled doubles must give the same
+bits. The full forms are the ones the oracle parity tests pin (test_chunk_gpu.py).
+
+Two routes: a compiled checker calling both forms side by side, and the library itself, where the
+specialised (NVRTC) kernels run the fast forms and the interpreter (specialisation off) the full
+forms, over every float bit pattern."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SOURCE = os.path.join(ROOT, "tests", "fast_forms_check.cu")
+BINARY = os.path.join(ROOT, "tests", "_build", "fast_forms_check")
+HEADERS = [os.path.join(ROOT, "libsci_b200", "csrc", name) for name in ("sci_math.cuh", "chunk_kernel.cuh")]
+
+
+def build_checker() -> str:
+    """Compiles the checker for sm_100a when it is missing or older than its sources."""
+    newest = max(os.path.getmtime(p) for p in [SOURCE, *HEADERS])
+    if not os.path.exists(BINARY) or os.path.getmtime(BINARY) < newest:
+        os.makedirs(os.path.dirname(BINARY), exist_ok=True)
+        # contraction off, as the specialised kernels are compiled (specialize.cu)
+        subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17", "-fmad=false",
+                        "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "libsci_b200", "csrc"),
+                        "-o", BINARY, SOURCE], check=True)
+    return BINARY
+
+
+@pytest.mark.gpu
+def test_fast_forms_match_full_forms():
+    run = subprocess.run([build_checker()], capture_output=True, text=True, timeout=600)
+    assert run.returncode == 0, run.stdout + run.stderr
+    lines = [line.split() for line in run.stdout.splitlines() if line.strip()]
+    assert len(lines) == 20, run.stdout
+    for name, precision, checked, bad, first in lines:
+        assert int(checked) == (1 << 32 if precision == "float" else 1 << 31)
+        assert int(bad) == 0, f"{name} ({precision}): {bad} inputs differ, first {first}"
+
+
+FAST_CODES = ["exponential", "logarithm", "sin", "cos", "tan", "csc", "sec", "cot", "tanh", "coth"]
+
+
+def open_device(jit: str):
+    from libsci_b200.device import Device
+
+    saved = os.environ.get("SCI_CUDA_JIT")
+    os.environ["SCI_CUDA_JIT"] = jit
+    try:
+        return Device(0)
+    finally:
+        if saved is None:
+            del os.environ["SCI_CUDA_JIT"]
+        else:
+            os.environ["SCI_CUDA_JIT"] = saved
+
+
+@pytest.mark.gpu
+def test_specialised_kernels_match_the_interpreter_on_every_float():
+    import torch
+
+    from libsci_b200 import chunk as C
+
+    interpreter, specialised = open_device("0"), open_device("sync")
+    span = 1 << 28
+    try:
+        patterns = torch.empty(span, dtype=torch.int32, device="cuda")
+        first, second = torch.empty_like(patterns), torch.empty_like(patterns)
+        for code in FAST_CODES:
+            chunk = C.record_output(C.unary(code, C.Reference(patterns.data_ptr(), span, np.float32)))
+            for start in range(0, 1 << 32, span):
+                # the bit patterns start .. start + span - 1 as int32: shift into the int32 range,
+                # then flip the top bit back
+                shifted = torch.arange(start - (1 << 31), start - (1 << 31) + span, dtype=torch.int64, device="cuda")
+                patterns.copy_(shifted.to(torch.int32) ^ (-(1 << 31)))
+                torch.cuda.synchronize()
+                interpreter.execute(chunk, first.data_ptr(), span)
+                specialised.execute(chunk, second.data_ptr(), span)
+                interpreter.synchronize()
+                specialised.synchronize()
+                differ = int((first != second).sum())
+                assert differ == 0, f"{code}: {differ} of the patterns {start:#x}.. differ"
+    finally:
+        interpreter.close()
+        specialised.close()
