@@ -412,6 +412,16 @@ namespace sci_cuda {
         return fold == 0 ? a + b : (fold == 1 ? fmin(a, b) : fmax(a, b));
     }
 
+    __device__ __forceinline__ float nan_min(float a, float b) {
+        float r;
+        asm("min.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+        return r;
+    }
+    __device__ __forceinline__ float nan_max(float a, float b) {
+        float r;
+        asm("max.NaN.f32 %0, %1, %2;" : "=f"(r) : "f"(a), "f"(b));
+        return r;
+    }
     __device__ __forceinline__ unsigned magnitude_bits(float v) { return __float_as_uint(v) & 0x7fffffffu; }
     __device__ __forceinline__ unsigned magnitude_bits(double v) {
         // A double is NaN iff its high word without sign exceeds 0x7ff00000, or equals it with a
@@ -446,6 +456,21 @@ namespace sci_cuda {
                 for (int e = 0; e < width; ++e) lanes[e] = add(lanes[e], lanes[e + width]);
             }
             f.total += static_cast<double>(lanes[0]);
+        } else if constexpr (sizeof(T) == 4) {
+            // NaN-propagating minimum / maximum: one instruction per lane, and a NaN among the
+            // lanes shows in the result (the fold's value no longer matters then)
+            T best = fold == 1 ? from_bits(Limits<T>::infinity) : -from_bits(Limits<T>::infinity);
+            if (fold == 1) {
+#pragma unroll
+                for (int e = 0; e < N; ++e)
+                    if (full || w.position(e) < w.live) best = nan_min(best, value[e]);
+            } else {
+#pragma unroll
+                for (int e = 0; e < N; ++e)
+                    if (full || w.position(e) < w.live) best = nan_max(best, value[e]);
+            }
+            if (is_nan(best)) f.magnitude = ~0u;
+            else f.total = combine(fold, f.total, static_cast<double>(best));
         } else {
             T best = fold == 1 ? from_bits(Limits<T>::infinity) : -from_bits(Limits<T>::infinity);
             unsigned magnitude = 0;
@@ -574,15 +599,17 @@ namespace sci_cuda {
             bool failed = false;
             for (unsigned long long k = blockIdx.x; k < full; k += grid, ++n) {
                 const bool ok = barrier_wait(&bars[s], parity);
-                if (__syncthreads_or(!ok)) {
-                    failed = true;
-                    break;
-                }
                 w.at(k * tile, tile, ring + static_cast<unsigned long long>(s) * A * tile);
                 T value[N], second[N];
                 run_tile<T, Program, MODE>(w, value, second);
                 if constexpr (MODE != kEvaluate) fold_tile<T, MODE>(fold, op, value, second, w, true);
-                __syncthreads();
+                // One barrier per tile: the whole block is done with slot s, so it may be refilled,
+                // and a wait that gave up anywhere in the block (its thread computed on whatever
+                // the slot held, inside the tile's bounds) ends the loop for all threads.
+                if (__syncthreads_or(!ok)) {
+                    failed = true;
+                    break;
+                }
                 if (t == 0) {
                     const unsigned long long next = k + S * grid;
                     if (next < full) issue(s, next);

@@ -498,10 +498,12 @@ namespace sci_cuda {
         Pair reduced = fma_(k, pair(-L::natural), x);
         reduced = fma_(k, pair(-L::remainder), reduced);
         const Pair significand = fma_(reduced, horner<1>(series, reduced), pair(1.0f));
-        float e0, e1;
+        float e0, e1, s0, s1;
         unpair(add(k, pair(L::exponent)), e0, e1);
-        const Pair scale = pair(from_bits(bits(e0) << L::mantissa), from_bits(bits(e1) << L::mantissa));
-        unpair(mul(significand, scale), r0, r1);
+        // the last multiply per lane, so no packed product reaches an add of the caller's
+        unpair(significand, s0, s1);
+        r0 = mul(s0, from_bits(bits(e0) << L::mantissa));
+        r1 = mul(s1, from_bits(bits(e1) << L::mantissa));
     }
 
     // logarithm_fast on two elements. The two selects of the `large` adjustment become a multiply by

@@ -85,3 +85,63 @@ def test_specialised_kernels_match_the_interpreter_on_every_float():
     finally:
         interpreter.close()
         specialised.close()
+
+
+COMPOSITES = {
+    "exp(x) + y": lambda x, y, z: C_unary("exponential", x) + y,
+    "log(y) * x + z": lambda x, y, z: C_unary("logarithm", y) * x + z,
+    "sin(x) * cos(z) + y": lambda x, y, z: C_unary("sin", x) * C_unary("cos", z) + y,
+    "sqrt|x| * log(y) + tanh(z)": lambda x, y, z: C_unary("root", C_unary("absolute", x)) * C_unary("logarithm", y)
+    + C_unary("tanh", z),
+    "exp(-x * x) * y - z": lambda x, y, z: C_unary("exponential", -x * x) * y - z,
+    "tan(x) - cot(z) * y": lambda x, y, z: C_unary("tan", x) - C_unary("cot", z) * y,
+    "coth(z) / sec(x)": lambda x, y, z: C_unary("coth", z) / C_unary("sec", x),
+}
+
+
+def C_unary(code, item):
+    from libsci_b200 import chunk as C
+
+    return C.unary(code, item)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(COMPOSITES))
+def test_composite_chunks_match_the_interpreter(name):
+    """Fast forms inside longer chunks: packed or fused arithmetic must not leak across codes."""
+    import torch
+
+    from libsci_b200 import chunk as C
+
+    count = 1 << 26
+    g = torch.Generator(device="cuda").manual_seed(7)
+    x = torch.randn(count, device="cuda", generator=g) * 3
+    x[: count // 4] = (torch.rand(count // 4, device="cuda", generator=g) - 0.5) * 200
+    y = torch.rand(count, device="cuda", generator=g) * 9.9 + 0.1
+    z = torch.rand(count, device="cuda", generator=g) * 2 - 1
+    specials = torch.tensor([0.0, -0.0, float("inf"), -float("inf"), float("nan"), 1e-45, -1e-45, 1e-38, 88.7,
+                             -103.9, 2e6, -3e7, 1e30, 1.5707964, 0.5, -1.0], device="cuda")
+    for t in (x, y, z):
+        t[1000:1000 + len(specials)] = specials
+        t[5000:5000 + len(specials)] = specials.flip(0)
+    y[::997] = -y[::997]
+    interpreter, specialised = open_device("0"), open_device("sync")
+    try:
+        refs = [C.Reference(t.data_ptr(), count, np.float32) for t in (x, y, z)]
+        expression = COMPOSITES[name](*refs)
+        first, second = torch.empty_like(x), torch.empty_like(x)
+        chunk = C.record_output(expression)
+        torch.cuda.synchronize()
+        interpreter.execute(chunk, first.data_ptr(), count)
+        specialised.execute(chunk, second.data_ptr(), count)
+        interpreter.synchronize()
+        specialised.synchronize()
+        differ = int((first.view(torch.int32) != second.view(torch.int32)).sum())
+        assert differ == 0, f"{name}: {differ} elements differ"
+        for fold in (C.MINIMUM, C.MAXIMUM):
+            reduced = C.record_reduce(expression)
+            a, b = interpreter.reduce_chunk(reduced, fold, count), specialised.reduce_chunk(reduced, fold, count)
+            assert (np.isnan(a) and np.isnan(b)) or a == b, (name, fold, a, b)
+    finally:
+        interpreter.close()
+        specialised.close()
