@@ -88,6 +88,9 @@ namespace sci_cuda {
         std::unique_ptr<Workspace> workspace;  // product / trailing-update operands
         std::unique_ptr<Workspace> solver;     // LU copies, pivots, residuals
         std::unique_ptr<Workspace> tape;       // the stored-form gradient's forward values
+        unsigned *sweep_flags{nullptr};  // per (block row, column group) of the persistent substitution
+        size_t sweep_capacity{0};        // flags allocated
+        unsigned sweep_epoch{0};         // the value that marks a flag as set by the current sweep
         int jit_mode{1};  // 0 off, 1 background, 2 synchronous (SCI_CUDA_JIT)
         bool jit_trace{false};
 

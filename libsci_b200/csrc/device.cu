@@ -310,6 +310,7 @@ int sci_cuda_close(sci_cuda_context *context) {
         cudaFree(context->state);
         cudaFree(context->result);
         cudaFree(context->status);
+        cudaFree(context->sweep_flags);
         cudaFreeHost(context->host_result);
         cudaFreeHost(context->host_status);
         cudaStreamDestroy(context->stream);

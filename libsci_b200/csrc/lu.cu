@@ -779,6 +779,53 @@ namespace sci_cuda {
             }
         }
 
+        // The coupling blocks of the sweeps: couple[2 i] = inv(L_ii) L_i,i-1 (block rows i >= 1) and
+        // couple[2 i + 1] = inv(U_ii) U_i,i+1 (i <= blocks - 2), 128 x 128 each, rows and columns past
+        // the matrix zero. One CTA per block (blockIdx.y: 0 lower, 1 upper), 256 threads of 8 x 8
+        // outputs, k in slices of 16 staged in shared memory.
+        __global__ void __launch_bounds__(256) couple_blocks(const float *lu, const float *inv, unsigned long long n,
+                                                             float *couple) {
+            constexpr int B = kSolveBlock, K = 16;
+            __shared__ float left[B][K + 1];  // inv[:, k0 : k0 + 16]
+            __shared__ float right[K][B];     // the tile's rows k0 .. k0 + 15
+            const unsigned long long blocks = (n + B - 1) / B, i = blockIdx.x;
+            const bool upper = blockIdx.y == 1;
+            if (upper ? i + 1 >= blocks : i == 0) return;
+            const unsigned long long s = i * B, sj = upper ? s + B : s - B;
+            const float *inverse = inv + (2 * i + (upper ? 1 : 0)) * B * B;
+            float *target = couple + (2 * i + (upper ? 1 : 0)) * B * B;
+            const int t = threadIdx.x, r0 = (t / 16) * 8, c0 = (t % 16) * 8;
+            float acc[8][8] = {};
+            for (int k0 = 0; k0 < B; k0 += K) {
+                for (int q = t; q < B * K; q += 256) {
+                    const int row = q / K, k = q % K;
+                    left[row][k] = inverse[row * B + k0 + k];
+                }
+                for (int q = t; q < K * B; q += 256) {
+                    const int k = q / B, c = q % B;
+                    const unsigned long long gr = s + k0 + k, gc = sj + c;
+                    right[k][c] = (gr < n && gc < n) ? lu[gr * n + gc] : 0.0f;
+                }
+                __syncthreads();
+                for (int k = 0; k < K; ++k) {
+                    float a[8], b[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) a[u] = left[r0 + u][k];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) b[u] = right[k][c0 + u];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+#pragma unroll
+                        for (int v = 0; v < 8; ++v) acc[u][v] = fma_(a[u], b[v], acc[u][v]);
+                }
+                __syncthreads();
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+#pragma unroll
+                for (int v = 0; v < 8; ++v) target[(r0 + u) * B + c0 + v] = acc[u][v];
+        }
+
         // y[s + r][col] := sum_k inv[r][k] x[s + k][col] for the `size` rows of one diagonal block, out
         // of place: 16 rows (blockIdx.x) by 32 columns (blockIdx.y) per CTA of 512 threads, warp w
         // computing row 16 blockIdx.x + w with lane = column. inv is zero padded to kSolveBlock
@@ -996,13 +1043,19 @@ namespace sci_cuda {
             return SCI_CUDA_OK;
         }
 
+        // The inverses of the diagonal blocks (2 per block row) followed by the coupling blocks of the
+        // persistent sweeps (2 per block row, couple_blocks).
         unsigned long long inverse_elements(unsigned long long n) {
-            return 2ull * ((n + kSolveBlock - 1) / kSolveBlock) * kSolveBlock * kSolveBlock;
+            return 4ull * ((n + kSolveBlock - 1) / kSolveBlock) * kSolveBlock * kSolveBlock;
         }
 
         template <typename T> int invert_diagonal(Context &ctx, const T *lu, unsigned long long n, T *inv) {
-            invert_blocks<T><<<static_cast<unsigned>((n + kSolveBlock - 1) / kSolveBlock), kSolveBlock, 0, ctx.stream>>>(lu, n,
-                                                                                                                       inv);
+            const unsigned blocks = static_cast<unsigned>((n + kSolveBlock - 1) / kSolveBlock);
+            invert_blocks<T><<<blocks, kSolveBlock, 0, ctx.stream>>>(lu, n, inv);
+            if constexpr (sizeof(T) == 4) {
+                if (blocks > 1)
+                    couple_blocks<<<dim3(blocks, 2), 256, 0, ctx.stream>>>(lu, inv, n, inv + 2ull * blocks * kSolveBlock * kSolveBlock);
+            }
             return ctx.check(cudaGetLastError(), "inverting the diagonal blocks");
         }
 
@@ -1039,6 +1092,330 @@ namespace sci_cuda {
             return ctx.check(cudaGetLastError(), "launching the substitution");
         }
 
+        // ---- persistent substitution sweeps ---------------------------------------------------------
+        // One cooperative launch solves a whole unit-lower (L) or upper (U) system in place of the
+        // block-by-block launches. CTA (block row i, column group g) adds up the products of its
+        // off-diagonal tiles with the other block rows' results in a fixed order, each as soon as
+        // that row has published, except the adjacent block row's; applies its
+        // diagonal block's inverse to (right-hand side - sum); and only then waits for the adjacent
+        // row, whose results enter through the coupling block inv(D_ii) D_i,adjacent. So the chain from
+        // one block row to the next is one wait, one 128 x 128 x 16 product and the write. Block rows
+        // publish in chain order (written, fenced, then the group's progress mark released), so one
+        // acquire of the mark shows every block row published so far.
+        // Every CTA is resident (cooperative launch), and every wait is bounded: one that runs out
+        // sets the timeout status and ends its CTA, so the CTAs after it end the same way.
+        constexpr int kSweepThreads = 4 * kSolveBlock;  // four quarters of the block's 128 rows
+        constexpr int kSweepColumns = 16;
+        constexpr unsigned kSweepWaitLimit = 1u << 22;
+
+        __device__ __forceinline__ unsigned load_acquire(const unsigned *p) {
+            unsigned v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+            return v;
+        }
+        // A polling read: relaxed, so it does not queue behind this thread's earlier loads; the caller
+        // follows the read that sees the release with fence_acquire (relaxed read + fence is an
+        // acquire pattern of the PTX memory model).
+        __device__ __forceinline__ unsigned load_relaxed(const unsigned *p) {
+            unsigned v;
+            asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+            return v;
+        }
+        __device__ __forceinline__ void fence_acquire() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+        __device__ __forceinline__ void store_release(unsigned *p, unsigned v) {
+            asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+        }
+
+        // acc[0..15] += a * v[0..15], two columns per packed instruction
+        __device__ __forceinline__ void axpy16(float a, const float *v, Pair *acc) {
+            const Pair pa = pair(a);
+            const Pair *pv = reinterpret_cast<const Pair *>(v);
+#pragma unroll
+            for (int c = 0; c < kSweepColumns / 2; ++c) acc[c] = fma_(pa, pv[c], acc[c]);
+        }
+
+        // 16-byte asynchronous copy global -> shared through L2 only (no stale L1 line of another SM's
+        // results can be read), zero-filled when `full` is false.
+        __device__ __forceinline__ void copy16_async(void *shared, const void *global, bool full) {
+            const unsigned address = static_cast<unsigned>(__cvta_generic_to_shared(shared));
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(address), "l"(global), "r"(full ? 16 : 0)
+                         : "memory");
+        }
+        __device__ __forceinline__ void copies_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+        template <int pending> __device__ __forceinline__ void copies_wait() {
+            asm volatile("cp.async.wait_group %0;" ::"n"(pending) : "memory");
+        }
+
+        template <bool upper>
+        __global__ void __launch_bounds__(kSweepThreads, 1)
+        sweep(const float *__restrict__ lu, const float *__restrict__ inv, const float *__restrict__ couple, unsigned n,
+              unsigned width, unsigned groups, const float *__restrict__ in, float *out, unsigned *flags, unsigned epoch,
+              int *status) {
+            constexpr int B = kSolveBlock, C = kSweepColumns;
+            constexpr int P = C + 4;  // pitch of a staged block row: 16-byte aligned rows
+            constexpr int Q = C + 1;  // pitch of a partial-sum row
+            constexpr int V = B * C / kSweepThreads;  // block elements per thread in the row-major mapping
+            // staged[0]: a block of results (or the rhs) being applied; staged[1], the next block's
+            // copy in flight, lives in the partial sums' space, which is free until the tiles are done
+            __shared__ __align__(16) float space[B * P + 4 * B * Q];
+            float *const staged0 = space, *const staged1 = space + B * P;
+            float (*partial)[B * Q] = reinterpret_cast<float (*)[B * Q]>(space + B * P);
+            __shared__ bool stop;
+            __shared__ int ready_shared;
+            const unsigned blocks = (n + B - 1) / B;
+            const unsigned i = upper ? blocks - 1 - blockIdx.x / groups : blockIdx.x / groups;
+            const unsigned g = blockIdx.x % groups, s = i * B, size = min(static_cast<unsigned>(B), n - s), c0 = g * C;
+            // thread = (quarter h, row r): a warp holds 32 rows of one quarter, so the staged reads
+            // below are broadcasts; quarter h covers the columns [32 h, 32 h + 32) of each tile
+            const int t = threadIdx.x, h = t / B, r = t % B;
+            const unsigned tiles = upper ? blocks - 1 - i : i;
+            const unsigned bulk = tiles > 0 ? tiles - 1 : 0;  // all tiles but the adjacent block row's
+            if (t == 0) stop = false;
+            // loaded before any wait: this block's inverse rows and its right-hand side
+            float4 m[8];
+            const unsigned long long own = (2ull * i + (upper ? 1 : 0)) * B * B + r * B + 32 * h;
+#pragma unroll
+            for (int u = 0; u < 8; ++u) m[u] = __ldg(reinterpret_cast<const float4 *>(inv + own) + u);
+            float rhs[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const unsigned q = t + v * kSweepThreads, k = q / C, c = q % C;
+                rhs[v] = (s + k < n && c0 + c < width) ? in[static_cast<unsigned long long>(s + k) * width + c0 + c] : 0.0f;
+            }
+            Pair acc[C / 2];
+#pragma unroll
+            for (int c = 0; c < C / 2; ++c) acc[c] = pair(0.0f);
+
+            // Step k of this CTA applies the block row k places along the chain (row_of(k)), which is
+            // also its place in publishing order.
+            auto row_of = [&](unsigned step) { return upper ? blocks - 1 - step : step; };
+            // `known` (uniform): the steps seen ready so far. Waits until `step` is; false if the wait
+            // ran out. One read of the group's progress counter covers every earlier step too.
+            unsigned known = 0;
+            const unsigned base_mark = epoch << 16;
+            auto ready = [&](unsigned step) -> bool {
+                if (step < known) return true;
+                if (t == 0) {
+                    unsigned seen = 0;
+                    for (unsigned spin = 0; spin < kSweepWaitLimit; ++spin) {
+                        const unsigned mark = load_relaxed(flags + g);
+                        if (mark > base_mark + step) {  // marks of earlier sweeps are below base_mark
+                            fence_acquire();
+                            seen = mark - base_mark;
+                            break;
+                        }
+                        __nanosleep(32);  // every waiting CTA polls the same word
+                    }
+                    if (seen == 0) {
+                        atomicOr(status, kStatusTimeout);
+                        stop = true;
+                    }
+                    ready_shared = static_cast<int>(seen);
+                }
+                __syncthreads();
+                known = static_cast<unsigned>(ready_shared);
+                return !stop;
+            };
+            // Starts copying block row row_of(step)'s results into `target` (row-major mapping: thread
+            // = row t / 4, columns 4 (t % 4) .. + 3), or loads them directly when rows are not 16-byte
+            // aligned (a width not a multiple of 4, or a caller's unaligned buffer).
+            auto fetch = [&](unsigned step, float *target) {
+                const unsigned sj = row_of(step) * B;
+                if (width % 4 == 0 && (reinterpret_cast<unsigned long long>(out) & 15) == 0) {
+                    const unsigned k = t / 4, c = 4 * (t % 4);
+                    const bool inside = sj + k < n && c0 + c < width;
+                    const float *source = out + (inside ? static_cast<unsigned long long>(sj + k) * width + c0 + c : 0ull);
+                    copy16_async(target + k * P + c, source, inside);
+                } else {
+#pragma unroll
+                    for (int v = 0; v < V; ++v) {
+                        const unsigned q = t + v * kSweepThreads, k = q / C, c = q % C;
+                        target[k * P + c] = (sj + k < n && c0 + c < width)
+                                                ? __ldcg(out + static_cast<unsigned long long>(sj + k) * width + c0 + c)
+                                                : 0.0f;
+                    }
+                }
+                copies_commit();
+            };
+            // acc (zeroed) := this quarter's part of rows4 times the block in `source`
+            auto multiply = [&](const float4 *rows4, const float *source) {
+#pragma unroll
+                for (int c = 0; c < C / 2; ++c) acc[c] = pair(0.0f);
+                const float *base = source + 32 * h * P;
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    axpy16(rows4[u].x, base + (4 * u + 0) * P, acc);
+                    axpy16(rows4[u].y, base + (4 * u + 1) * P, acc);
+                    axpy16(rows4[u].z, base + (4 * u + 2) * P, acc);
+                    axpy16(rows4[u].w, base + (4 * u + 3) * P, acc);
+                }
+            };
+            // the quarters' acc into `partial` (callers have synchronised past its last reads)
+            auto publish = [&]() {
+                float lanes[C];
+#pragma unroll
+                for (int c = 0; c < C / 2; ++c) unpair(acc[c], lanes[2 * c], lanes[2 * c + 1]);
+#pragma unroll
+                for (int c = 0; c < C; ++c) partial[h][r * Q + c] = lanes[c];
+            };
+            auto total = [&](unsigned q) {
+                const unsigned k = q / C, c = q % C;
+                return ((partial[0][k * Q + c] + partial[1][k * Q + c]) + partial[2][k * Q + c]) + partial[3][k * Q + c];
+            };
+
+            // Every off-diagonal tile but the adjacent one, oldest results first, summed into acc;
+            // the next block of results is copied in while the current one is applied.
+            const float *row = lu + static_cast<unsigned long long>(r < size ? s + r : s) * n;
+            bool fetched = false;  // whether the current step's block is already on its way
+            for (unsigned step = 0; step < bulk; ++step) {
+                const unsigned sj = row_of(step) * B;
+                float4 a[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const unsigned column = sj + 32 * h + 4 * u;
+                    a[u] = (r < size && column < n) ? __ldg(reinterpret_cast<const float4 *>(row + column))
+                                                    : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                }
+                // the next block is copied in now only if it is already known to be published (a
+                // CTA that has caught up with the chain applies the block it has, then waits)
+                if (!fetched) {
+                    if (!ready(step)) return;
+                    fetch(step, (step & 1) ? staged1 : staged0);
+                }
+                fetched = step + 1 < bulk && step + 1 < known;
+                if (fetched) {
+                    fetch(step + 1, (step & 1) ? staged0 : staged1);
+                    copies_wait<1>();
+                } else {
+                    copies_wait<0>();
+                }
+                __syncthreads();  // the current block is in place for every thread
+                const float *base = ((step & 1) ? staged1 : staged0) + 32 * h * P;
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    axpy16(a[u].x, base + (4 * u + 0) * P, acc);
+                    axpy16(a[u].y, base + (4 * u + 1) * P, acc);
+                    axpy16(a[u].z, base + (4 * u + 2) * P, acc);
+                    axpy16(a[u].w, base + (4 * u + 3) * P, acc);
+                }
+                __syncthreads();  // before the buffer is refilled
+            }
+            // the coupling rows of the adjacent block row, in flight during what follows
+            float4 mc[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u)
+                mc[u] = tiles > 0 ? __ldg(reinterpret_cast<const float4 *>(couple + own) + u) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            // pre = inverse (rhs - sum), kept in registers in the row-major mapping
+            publish();
+            __syncthreads();
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const unsigned q = t + v * kSweepThreads;
+                staged0[(q / C) * P + q % C] = rhs[v] - total(q);
+            }
+            __syncthreads();
+            multiply(m, staged0);
+            publish();
+            __syncthreads();
+            float result[V];
+#pragma unroll
+            for (int v = 0; v < V; ++v) result[v] = total(t + v * kSweepThreads);
+            // then the adjacent block row: result = pre - inv(D_ii) D_i,adjacent x_adjacent
+            if (tiles > 0) {
+                __syncthreads();  // `partial` and staged0 are free again
+                if (!ready(tiles - 1)) return;
+                fetch(tiles - 1, staged0);
+                copies_wait<0>();
+                __syncthreads();
+                multiply(mc, staged0);
+                publish();
+                __syncthreads();
+#pragma unroll
+                for (int v = 0; v < V; ++v) result[v] = result[v] - total(t + v * kSweepThreads);
+            }
+#pragma unroll
+            for (int v = 0; v < V; ++v) {
+                const unsigned q = t + v * kSweepThreads, k = q / C, c = q % C;
+                if (s + k < n && c0 + c < width) out[static_cast<unsigned long long>(s + k) * width + c0 + c] = result[v];
+            }
+            // The block's writes reach thread 0 through the barrier, and its release (cumulative, after
+            // a GPU-scope fence) publishes them. This CTA is blockIdx.x / groups places along the
+            // chain and the row before it has published (its results were waited for above), so the
+            // group's mark only grows.
+            __syncthreads();
+            if (t == 0) {
+                __threadfence();
+                store_release(flags + g, base_mark + blockIdx.x / groups + 1);
+            }
+        }
+
+        // The progress marks of the sweeps (one per column group): zeroed when (re)allocated; each
+        // sweep counts from a fresh epoch.
+        int sweep_flags(Context &ctx, size_t count) {
+            if (count > ctx.sweep_capacity) {
+                if (ctx.sweep_flags) {
+                    if (int code = ctx.check(cudaStreamSynchronize(ctx.stream), "retiring the sweep flags")) return code;
+                    cudaFree(ctx.sweep_flags);
+                    ctx.sweep_flags = nullptr;
+                    ctx.sweep_capacity = 0;
+                }
+                if (int code = ctx.check(cudaMalloc(&ctx.sweep_flags, count * sizeof(unsigned)), "sweep flags")) return code;
+                ctx.sweep_capacity = count;
+                if (int code = ctx.check(cudaMemsetAsync(ctx.sweep_flags, 0, count * sizeof(unsigned), ctx.stream), "sweep flags"))
+                    return code;
+            }
+            return SCI_CUDA_OK;
+        }
+
+        // Epochs take 16 bits (the marks are epoch << 16 | rows published): on wrapping, the marks of
+        // earlier sweeps are cleared so none can look current.
+        unsigned next_epoch(Context &ctx) {
+            if (++ctx.sweep_epoch == 0x10000) {
+                cudaMemsetAsync(ctx.sweep_flags, 0, ctx.sweep_capacity * sizeof(unsigned), ctx.stream);
+                ctx.sweep_epoch = 1;
+            }
+            return ctx.sweep_epoch;
+        }
+
+        // x (n x width, the right-hand side on entry) := U^-1 L^-1 x by the two persistent sweeps, y
+        // scratch; `done` stays false (and nothing is queued) when they do not apply: n not a multiple
+        // of 4 (the tiles are read as 16-byte vectors), or more CTAs than can be resident at once.
+        int sweep_substitute(Context &ctx, const float *lu, const float *inv, unsigned long long n, float *x, float *y,
+                             unsigned long long width, bool &done) {
+            done = false;
+            const unsigned long long blocks = (n + kSolveBlock - 1) / kSolveBlock;
+            const unsigned long long groups = (width + kSweepColumns - 1) / kSweepColumns;
+            if (n % 4 != 0 || n > 0x7fffffffull || width > 0x7fffffffull) return SCI_CUDA_OK;
+            static int cooperative = -1;
+            if (cooperative < 0) {
+                int value = 0;
+                cudaDeviceGetAttribute(&value, cudaDevAttrCooperativeLaunch, ctx.device);
+                cooperative = value;
+            }
+            if (!cooperative) return SCI_CUDA_OK;
+            const int resident = std::min(ctx.blocks_per_sm(reinterpret_cast<const void *>(&sweep<false>), kSweepThreads, 0),
+                                          ctx.blocks_per_sm(reinterpret_cast<const void *>(&sweep<true>), kSweepThreads, 0));
+            if (blocks * groups > static_cast<unsigned long long>(resident) * ctx.sms) return SCI_CUDA_OK;
+            if (blocks >= 0xffff) return SCI_CUDA_OK;  // the progress marks count block rows in 16 bits
+            if (int code = sweep_flags(ctx, groups)) return code;
+            const float *couple = inv + 2ull * blocks * kSolveBlock * kSolveBlock;
+            unsigned nn = static_cast<unsigned>(n), ww = static_cast<unsigned>(width), gg = static_cast<unsigned>(groups);
+            for (int pass = 0; pass < 2; ++pass) {
+                const bool upper = pass == 1;
+                unsigned epoch = next_epoch(ctx);
+                const float *source = upper ? y : x;
+                float *target = upper ? x : y;
+                void *args[] = {&lu, &inv, &couple, &nn, &ww, &gg, &source, &target, &ctx.sweep_flags, &epoch, &ctx.status};
+                const void *kernel = upper ? reinterpret_cast<const void *>(&sweep<true>) : reinterpret_cast<const void *>(&sweep<false>);
+                if (int code = ctx.check(cudaLaunchCooperativeKernel(kernel, dim3(static_cast<unsigned>(blocks * groups)),
+                                                                    dim3(kSweepThreads), args, 0, ctx.stream),
+                                         "launching a substitution sweep"))
+                    return code;
+            }
+            done = true;
+            return SCI_CUDA_OK;
+        }
+
         // C -= A B for the substitution (k <= kSolveBlock), 32 columns of B per launch of the skinny
         // kernel; transposed: A is stored k x m (pitch lda).
         template <typename T, bool transposed = false>
@@ -1061,6 +1438,11 @@ namespace sci_cuda {
         template <typename T>
         int substitute_inverse(Context &ctx, const T *lu, const T *inv, unsigned long long n, T *x, T *y,
                                unsigned long long width) {
+            if constexpr (sizeof(T) == 4) {
+                bool done = false;
+                if (int code = sweep_substitute(ctx, lu, inv, n, x, y, width, done)) return code;
+                if (done) return SCI_CUDA_OK;
+            }
             const unsigned column_groups = static_cast<unsigned>((width + 31) / 32);
             const int apply_smem = static_cast<int>(apply_shared_bytes<T>());
             cudaFuncSetAttribute(reinterpret_cast<const void *>(&apply_inverse<T, false>),

@@ -566,14 +566,15 @@ namespace sci_cuda {
         unpair(sine, s[0], s[1]);
         unpair(cosine, c[0], c[1]);
         unpair(shifted, h[0], h[1]);
+        // Per lane, q = the low bits of `shifted`: bit 0 swaps sine and cosine, and the sign flips
+        // with bit 1 of q for the sine, with bit 1 of q ^ (q << 1) = bit 1 of q + 1 for the cosine
+        // (the forms above); shifted left by 30 either lands on the sign bit.
 #pragma unroll
         for (int i = 0; i < 2; ++i) {
-            unsigned quadrant = bits(h[i]);
-            if (phase) quadrant ^= quadrant << 1;
-            const unsigned flip = (quadrant & 2u) << 30;
-            const bool swap = (bits(h[i]) & 1u) != 0;
-            const float result = phase ? (swap ? s[i] : c[i]) : (swap ? c[i] : s[i]);
-            out[i] = from_bits(bits(result) ^ flip);
+            const unsigned q = bits(h[i]);
+            const unsigned sign = ((phase ? q + 1u : q) << 30) & 0x80000000u;
+            const float result = ((q & 1u) != 0) != phase ? c[i] : s[i];
+            out[i] = from_bits(bits(result) ^ sign);
         }
         r0 = out[0];
         r1 = out[1];
