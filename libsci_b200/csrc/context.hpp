@@ -88,7 +88,11 @@ namespace sci_cuda {
         std::unique_ptr<Workspace> workspace;  // product / trailing-update operands
         std::unique_ptr<Workspace> solver;     // LU copies, pivots, residuals
         std::unique_ptr<Workspace> tape;       // the stored-form gradient's forward values
-        unsigned *sweep_flags{nullptr};  // per (block row, column group) of the persistent substitution
+        cudaStream_t side{nullptr};             // the LU look-ahead's bulk updates (lower priority)
+        cudaEvent_t side_done{nullptr};         // the side stream's queued work has finished
+        cudaEvent_t main_ready{nullptr};        // the main stream reached the point the side waits for
+        std::unique_ptr<Workspace> side_space;  // the side stream's product operands
+        unsigned *sweep_flags{nullptr};  // progress marks of the persistent substitution sweeps
         size_t sweep_capacity{0};        // flags allocated
         unsigned sweep_epoch{0};         // the value that marks a flag as set by the current sweep
         int jit_mode{1};  // 0 off, 1 background, 2 synchronous (SCI_CUDA_JIT)

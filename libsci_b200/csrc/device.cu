@@ -270,7 +270,11 @@ int sci_cuda_open(uint32_t ordinal, sci_cuda_context **context) {
     ctx->shared_limit = props.sharedMemPerBlockOptin;
     ctx->name = props.name;
     if (cudaSetDevice(ctx->device) != cudaSuccess) return SCI_CUDA_ERROR_DEVICE;
-    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) return SCI_CUDA_ERROR_DEVICE;
+    // The context's stream at the highest priority: the LU look-ahead queues its bulk updates on a
+    // lower-priority side stream, so blocks that free up go to the critical path first.
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
+    if (cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, greatest) != cudaSuccess) return SCI_CUDA_ERROR_DEVICE;
     if (cudaMalloc(&ctx->state, sizeof(ReduceState)) != cudaSuccess || cudaMalloc(&ctx->result, sizeof(double)) != cudaSuccess ||
         cudaMalloc(&ctx->status, sizeof(int)) != cudaSuccess || cudaMallocHost(&ctx->host_result, sizeof(double)) != cudaSuccess ||
         cudaMallocHost(&ctx->host_status, sizeof(int)) != cudaSuccess) {
@@ -311,6 +315,10 @@ int sci_cuda_close(sci_cuda_context *context) {
         cudaFree(context->result);
         cudaFree(context->status);
         cudaFree(context->sweep_flags);
+        if (context->side) cudaStreamDestroy(context->side);
+        if (context->side_done) cudaEventDestroy(context->side_done);
+        if (context->main_ready) cudaEventDestroy(context->main_ready);
+        if (context->side_space) context->side_space->release();
         cudaFreeHost(context->host_result);
         cudaFreeHost(context->host_status);
         cudaStreamDestroy(context->stream);

@@ -41,6 +41,7 @@ namespace sci_cuda {
 
         constexpr unsigned long long kPanelRows = 8192;  // the panel cluster holds every row in registers
         constexpr unsigned long long kOuter = 256;
+        constexpr int kMovements = static_cast<int>(kOuter / 16);  // per-panel row movements of one outer block
         constexpr int kSolveBlock = 128;
 
         template <typename T> struct PanelWidth {
@@ -524,10 +525,10 @@ namespace sci_cuda {
         // Applies a panel's net row movement to every column outside [skip0, skip1): all reads first,
         // then all writes, so no exchange waits on another.
         template <typename T>
-        __global__ void move_rows(T *a, unsigned long long n, const Movement *moved, unsigned long long skip0,
-                                  unsigned long long skip1) {
-            const unsigned long long col = blockIdx.x * 256ull + threadIdx.x;
-            if (col >= n || (col >= skip0 && col < skip1)) return;
+        __global__ void move_rows(T *a, unsigned long long n, const Movement *moved, unsigned long long c0,
+                                  unsigned long long c1, unsigned long long skip0, unsigned long long skip1) {
+            const unsigned long long col = c0 + blockIdx.x * 256ull + threadIdx.x;
+            if (col >= c1 || (col >= skip0 && col < skip1)) return;
             const int count = static_cast<int>(moved->count);
             T values[64];
 #pragma unroll
@@ -536,6 +537,25 @@ namespace sci_cuda {
 #pragma unroll
             for (int i = 0; i < 64; ++i)
                 if (i < count) a[static_cast<unsigned long long>(moved->rows[i]) * n + col] = values[i];
+        }
+
+        // move_rows for `count` movements in turn (a block's panels, in their order), one column per
+        // thread: the movements of one column follow each other in program order.
+        template <typename T>
+        __global__ void move_rows_all(T *a, unsigned long long n, const Movement *moved, int count,
+                                      unsigned long long skip0, unsigned long long skip1) {
+            const unsigned long long col = blockIdx.x * 256ull + threadIdx.x;
+            if (col >= n || (col >= skip0 && col < skip1)) return;
+            for (int p = 0; p < count; ++p) {
+                const int rows = static_cast<int>(moved[p].count);
+                T values[64];
+#pragma unroll
+                for (int i = 0; i < 64; ++i)
+                    if (i < rows) values[i] = a[static_cast<unsigned long long>(moved[p].src[i]) * n + col];
+#pragma unroll
+                for (int i = 0; i < 64; ++i)
+                    if (i < rows) a[static_cast<unsigned long long>(moved[p].rows[i]) * n + col] = values[i];
+            }
         }
 
         // rows[] of the factorisation (the original row at each position) from the exchanges, in
@@ -969,32 +989,128 @@ namespace sci_cuda {
 
         // In-place blocked LU of an n x n row-major matrix on the context's stream; pivots to piv
         // (device, LAPACK style: at step k row k was exchanged with row piv[k]).
+        // Work queued on the context's side stream (and with its side workspace) while in scope.
+        struct OnSide {
+            Context &ctx;
+            cudaStream_t stream;
+            std::unique_ptr<Workspace> space;
+            explicit OnSide(Context &c) : ctx(c), stream(c.stream) {
+                ctx.stream = ctx.side;
+                ctx.workspace.swap(ctx.side_space);
+            }
+            ~OnSide() {
+                ctx.workspace.swap(ctx.side_space);
+                ctx.stream = stream;
+            }
+        };
+
+        int side_stream(Context &ctx) {
+            if (ctx.side) return SCI_CUDA_OK;
+            int least = 0, greatest = 0;
+            cudaDeviceGetStreamPriorityRange(&least, &greatest);
+            if (int code = ctx.check(cudaStreamCreateWithPriority(&ctx.side, cudaStreamNonBlocking, least), "side stream"))
+                return code;
+            if (int code = ctx.check(cudaEventCreateWithFlags(&ctx.side_done, cudaEventDisableTiming), "side event"))
+                return code;
+            if (int code = ctx.check(cudaEventCreateWithFlags(&ctx.main_ready, cudaEventDisableTiming), "main event"))
+                return code;
+            if (!ctx.side_space) ctx.side_space = std::make_unique<Workspace>();
+            return SCI_CUDA_OK;
+        }
+
+        // A (n x n, in place) := L\U with partial pivoting, right-looking in outer blocks of kOuter
+        // columns and panels of W inside them. moved holds kMovements row movements (one per panel
+        // of a block). With look-ahead (SCI_CUDA_LOOKAHEAD unset or not 0), each block's panels
+        // move rows only inside the block's columns; the block's movements reach every other
+        // column after the previous block's bulk update is done. Then the main stream updates the
+        // next block's columns (its U rows and trailing update) and goes on to its panels, while the
+        // side stream updates the columns beyond it. The two streams touch disjoint columns, and the
+        // main stream waits for the side before it moves rows outside a block.
         template <typename T>
         int factor_device(Context &ctx, T *a, unsigned long long n, long long *piv, Movement *moved, bool tensor,
                           bool split) {
             constexpr int W = PanelWidth<T>::value;
             if (n > kPanelRows) return ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "factor: order %llu above %llu", n, kPanelRows);
+            static const bool lookahead = [] {
+                const char *setting = std::getenv("SCI_CUDA_LOOKAHEAD");
+                return !(setting && std::strcmp(setting, "0") == 0);
+            }();
+            const bool ahead = lookahead && n > 2 * kOuter;
+            if (ahead) {
+                if (int code = side_stream(ctx)) return code;
+            }
             if (tensor && sizeof(T) == 4 && n > kOuter) {
-                // the largest trailing update reserves the product workspace once
+                // the largest trailing updates reserve the product workspaces once (the main
+                // stream's holds at most kOuter columns of U with look-ahead)
                 const unsigned long long big = n - kOuter;
-                if (int code = ctx.check(ctx.workspace->reserve((split ? 3 : 1) * (2 * big * kOuter * 2 + 2048) + 1024),
+                const unsigned long long terms = split ? 3 : 1;
+                const unsigned long long main_columns = ahead ? kOuter : big;
+                if (int code = ctx.check(ctx.workspace->reserve(terms * ((big + main_columns) * kOuter * 2 + 2048) + 1024),
                                          "reserving the trailing-update workspace"))
                     return code;
+                if (ahead) {
+                    if (int code = ctx.check(ctx.side_space->reserve(terms * (2 * big * kOuter * 2 + 2048) + 1024),
+                                             "reserving the side workspace"))
+                        return code;
+                }
             }
             const int cluster = panel_cluster<T>();
             if (cluster == 0) return ctx.fail(SCI_CUDA_ERROR_LAUNCH, "the panel kernel's cluster cannot be scheduled");
+            const unsigned move_blocks = static_cast<unsigned>((n + 255) / 256);
+            // U rows of the block (columns [c0, c1)) = L11^-1 A12, panel by panel
+            auto block_rows = [&](unsigned long long J0, unsigned long long block_end, unsigned long long c0,
+                                  unsigned long long c1) -> int {
+                if (c1 <= c0) return SCI_CUDA_OK;
+                for (unsigned long long j0 = J0; j0 < block_end; j0 += W) {
+                    const int w = static_cast<int>(std::min<unsigned long long>(W, block_end - j0));
+                    trsm_rows<T><<<static_cast<unsigned>((c1 - c0 + 127) / 128), 128, 0, ctx.stream>>>(a, n, j0, w, c0, c1);
+                    const unsigned long long below = j0 + w;
+                    if (below < block_end) {
+                        if (int code = update<T>(ctx, a + below * n + j0, n, a + j0 * n + c0, n, a + below * n + c0, n,
+                                                 block_end - below, c1 - c0, w))
+                            return code;
+                    }
+                }
+                return ctx.check(cudaGetLastError(), "launching the block's U rows");
+            };
+            // trailing update of columns [c0, c1): A[t0:, c0:c1] -= L[t0:, J0:t0] U[J0:t0, c0:c1]
+            // narrow: the next block's columns on the critical path, where the SIMT rank update
+            // (no operand conversion) beats a small tensor-core product
+            auto trailing = [&](unsigned long long J0, unsigned long long t0, unsigned long long c0,
+                                unsigned long long c1, bool narrow) -> int {
+                if (t0 >= n || c1 <= c0) return SCI_CUDA_OK;
+                const unsigned long long ob = t0 - J0;
+                if (narrow) return update<T>(ctx, a + t0 * n + J0, n, a + J0 * n + c0, n, a + t0 * n + c0, n, n - t0, c1 - c0, ob);
+                if constexpr (sizeof(T) == 4) {
+                    if (tensor)
+                        return tensor_gemm(ctx, split ? 3 : 1, a + t0 * n + J0, n, a + J0 * n + c0, n, a + t0 * n + c0, n,
+                                           n - t0, c1 - c0, ob, true);
+                }
+                return simt_gemm<T>(ctx, a + t0 * n + J0, n, a + J0 * n + c0, n, a + t0 * n + c0, n, n - t0, c1 - c0, ob,
+                                    true);
+            };
+            static const bool narrow_simt = [] {
+                const char *setting = std::getenv("SCI_CUDA_NARROW");
+                return !(setting && std::strcmp(setting, "tensor") == 0);
+            }();
+            bool side_pending = false;
             for (unsigned long long J0 = 0; J0 < n; J0 += kOuter) {
-                const unsigned long long ob = std::min<unsigned long long>(kOuter, n - J0);
-                for (unsigned long long j0 = J0; j0 < J0 + ob; j0 += W) {
-                    const int w = static_cast<int>(std::min<unsigned long long>(W, J0 + ob - j0));
-                    const cudaError_t launched = cluster == 16 ? launch_panel<T, 16>(ctx.stream, a, n, j0, w, piv, moved)
-                                                               : launch_panel<T, 8>(ctx.stream, a, n, j0, w, piv, moved);
+                const unsigned long long ob = std::min<unsigned long long>(kOuter, n - J0), block_end = J0 + ob;
+                int panels = 0;
+                for (unsigned long long j0 = J0; j0 < block_end; j0 += W, ++panels) {
+                    const int w = static_cast<int>(std::min<unsigned long long>(W, block_end - j0));
+                    Movement *mine = moved + panels;
+                    const cudaError_t launched = cluster == 16 ? launch_panel<T, 16>(ctx.stream, a, n, j0, w, piv, mine)
+                                                               : launch_panel<T, 8>(ctx.stream, a, n, j0, w, piv, mine);
                     if (int code = ctx.check(launched, "launching the panel factorisation")) return code;
-                    move_rows<T><<<static_cast<unsigned>((n + 255) / 256), 256, 0, ctx.stream>>>(a, n, moved, j0, j0 + w);
+                    // the panel's row movement: now inside the block (everywhere without look-ahead)
+                    const unsigned long long m0 = ahead ? J0 : 0, m1 = ahead ? block_end : n;
+                    move_rows<T><<<static_cast<unsigned>((m1 - m0 + 255) / 256), 256, 0, ctx.stream>>>(a, n, mine, m0, m1, j0,
+                                                                                                      j0 + w);
                     // Inside the outer block only: U rows of the panel, then the rows below it. Columns
                     // beyond the block wait until the block's pivots are all known (a later pivot of
                     // this block may still bring a row up from below).
-                    const unsigned long long right = j0 + w, block_end = J0 + ob;
+                    const unsigned long long right = j0 + w;
                     if (right < block_end) {
                         trsm_rows<T><<<static_cast<unsigned>((block_end - right + 127) / 128), 128, 0, ctx.stream>>>(
                                 a, n, j0, w, right, block_end);
@@ -1004,41 +1120,35 @@ namespace sci_cuda {
                     }
                     if (int code = ctx.check(cudaGetLastError(), "launching the panel updates")) return code;
                 }
-                // U12 (the block's rows, columns beyond it) = L11^-1 A12, panel by panel, now that
-                // every row exchange of the block has been applied.
-                const unsigned long long block_end = J0 + ob;
-                if (block_end < n) {
-                    for (unsigned long long j0 = J0; j0 < block_end; j0 += W) {
-                        const int w = static_cast<int>(std::min<unsigned long long>(W, block_end - j0));
-                        trsm_rows<T><<<static_cast<unsigned>((n - block_end + 127) / 128), 128, 0, ctx.stream>>>(
-                                a, n, j0, w, block_end, n);
-                        const unsigned long long below = j0 + w;
-                        if (below < block_end) {
-                            if (int code = update<T>(ctx, a + below * n + j0, n, a + j0 * n + block_end, n,
-                                                     a + below * n + block_end, n, block_end - below, n - block_end, w))
-                                return code;
-                        }
+                if (ahead) {
+                    // the block's movements reach the other columns once the side stream is done with them
+                    if (side_pending) {
+                        if (int code = ctx.check(cudaStreamWaitEvent(ctx.stream, ctx.side_done, 0), "waiting for the side"))
+                            return code;
+                        side_pending = false;
                     }
-                    if (int code = ctx.check(cudaGetLastError(), "launching the block's U rows")) return code;
+                    move_rows_all<T><<<move_blocks, 256, 0, ctx.stream>>>(a, n, moved, panels, J0, block_end);
                 }
-                // trailing update: A22 -= L21 * U12, K = ob
-                const unsigned long long t0 = J0 + ob;
-                if (t0 < n) {
-                    int code;
-                    if constexpr (sizeof(T) == 4) {
-                        if (tensor) {
-                            code = tensor_gemm(ctx, split ? 3 : 1, a + t0 * n + J0, n, a + J0 * n + t0, n, a + t0 * n + t0, n,
-                                               n - t0, n - t0, ob, true);
-                        } else {
-                            code = simt_gemm<T>(ctx, a + t0 * n + J0, n, a + J0 * n + t0, n, a + t0 * n + t0, n, n - t0,
-                                                n - t0, ob, true);
-                        }
-                    } else {
-                        code = simt_gemm<T>(ctx, a + t0 * n + J0, n, a + J0 * n + t0, n, a + t0 * n + t0, n, n - t0, n - t0,
-                                            ob, true);
-                    }
-                    if (code) return code;
+                if (block_end >= n) continue;
+                const unsigned long long next = ahead ? std::min<unsigned long long>(kOuter, n - block_end) : n - block_end;
+                const unsigned long long split_at = block_end + next;
+                if (split_at < n) {
+                    // the columns beyond the next block: on the side stream, from here on
+                    if (int code = ctx.check(cudaEventRecord(ctx.main_ready, ctx.stream), "recording the main stream"))
+                        return code;
+                    OnSide side(ctx);
+                    if (int code = ctx.check(cudaStreamWaitEvent(ctx.stream, ctx.main_ready, 0), "side waits")) return code;
+                    if (int code = block_rows(J0, block_end, split_at, n)) return code;
+                    if (int code = trailing(J0, block_end, split_at, n, false)) return code;
+                    if (int code = ctx.check(cudaEventRecord(ctx.side_done, ctx.stream), "recording the side")) return code;
+                    side_pending = true;
                 }
+                // the next block's columns (all columns beyond without look-ahead)
+                if (int code = block_rows(J0, block_end, block_end, split_at)) return code;
+                if (int code = trailing(J0, block_end, block_end, split_at, ahead && narrow_simt)) return code;
+            }
+            if (side_pending) {
+                if (int code = ctx.check(cudaStreamWaitEvent(ctx.stream, ctx.side_done, 0), "waiting for the side")) return code;
             }
             return SCI_CUDA_OK;
         }
@@ -1582,10 +1692,10 @@ extern "C" int sci_cuda_factor(sci_cuda_context *context, uint32_t precision, ui
     if (order == 0) return SCI_CUDA_OK;
     if (!matrix || !rows) return context->fail(SCI_CUDA_ERROR_INVALID, "null matrix or rows");
     cudaSetDevice(context->device);
-    if (int code = context->check(context->solver->reserve(order * 8 + sizeof(Movement) + 1024), "pivot storage")) return code;
+    if (int code = context->check(context->solver->reserve(order * 8 + kMovements * sizeof(Movement) + 1024), "pivot storage")) return code;
     Carve carve{static_cast<unsigned char *>(context->solver->memory)};
     long long *piv = carve.take<long long>(order);
-    Movement *moved = carve.take<Movement>(1);
+    Movement *moved = carve.take<Movement>(kMovements);
     int code = precision == SCI_PRECISION_WIDE
                        ? factor_device<double>(*context, static_cast<double *>(matrix), order, piv, moved, false, false)
                        : factor_device<float>(*context, static_cast<float *>(matrix), order, piv, moved,
@@ -1684,12 +1794,12 @@ extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uin
     const unsigned long long n = order, nw = order * width;
     const bool wide = precision == SCI_PRECISION_WIDE;
     const size_t element = (wide && refine == SCI_REFINE_NONE) ? 8 : 4;
-    const unsigned long long need = n * n * element + n * 8 + sizeof(Movement) + n * 4 + nw * 12 + n * 8 + width * 16 +
+    const unsigned long long need = n * n * element + n * 8 + kMovements * sizeof(Movement) + n * 4 + nw * 12 + n * 8 + width * 16 +
                                     inverse_elements(n) * 4 + nw * 4 + 8192;
     if (int code = context->check(context->solver->reserve(need), "reserving the solver workspace")) return code;
     Carve carve{static_cast<unsigned char *>(context->solver->memory)};
     long long *piv = carve.take<long long>(n);
-    Movement *moved = carve.take<Movement>(1);
+    Movement *moved = carve.take<Movement>(kMovements);
     unsigned *rows = carve.take<unsigned>(n);
 
     if (refine == SCI_REFINE_NONE) {
@@ -1821,11 +1931,11 @@ extern "C" int sci_cuda_solve_gradient(sci_cuda_context *context, uint32_t preci
     const size_t element = precision == SCI_PRECISION_WIDE ? 8 : 4;
     // everything either form carves, generously: matrices, inverses, right-hand-side blocks, norms
     const unsigned long long need = n * n * (8 + element) + inverse_elements(n) * element + nw * 8 * 10 + n * 32 +
-                                    sizeof(Movement) + width * 16 + 16384;
+                                    kMovements * sizeof(Movement) + width * 16 + 16384;
     if (int code = context->check(context->solver->reserve(need), "reserving the solver workspace")) return code;
     Carve carve{static_cast<unsigned char *>(context->solver->memory)};
     long long *piv = carve.take<long long>(n);
-    Movement *moved = carve.take<Movement>(1);
+    Movement *moved = carve.take<Movement>(kMovements);
     unsigned *rows = carve.take<unsigned>(n);
 
     if (refine == SCI_REFINE_NONE) {
