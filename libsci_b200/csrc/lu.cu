@@ -943,6 +943,72 @@ namespace sci_cuda {
                 if (c4 + j < w) c[gr * ldc + c4 + j] = sub(c[gr * ldc + c4 + j], acc[j]);
         }
 
+        // r = b - A x in FP64, the refinement's residual: 32 rows (blockIdx.x) by 16 columns of x
+        // (blockIdx.y) per CTA. A is streamed through shared memory in slices of 64 columns, coalesced,
+        // the next slice's loads issued before the current one is used; warp w sums the slice's columns
+        // [8 w, 8 w + 8) for row = lane (x's entries are then broadcasts); at the end the eight warps'
+        // sums are added in warp order. A is read once: the kernel is bound by HBM.
+        constexpr int kResidualRows = 32, kResidualSlice = 64, kResidualColumns = 16;
+        __global__ void __launch_bounds__(256, 2) residual_rows(const double *__restrict__ a, const double *__restrict__ x,
+                                                                const double *__restrict__ b, double *__restrict__ r,
+                                                                unsigned long long n, unsigned long long width) {
+            constexpr int R = kResidualRows, K = kResidualSlice, C = kResidualColumns, PA = K + 1;
+            constexpr int LA = R * K / 256, LX = K * C / 256;
+            __shared__ double as[R * PA];  // the slice of A, then the warps' sums (half the columns at a time)
+            __shared__ double xs[K * C];
+            const unsigned long long r0 = blockIdx.x * 1ull * R, c0 = blockIdx.y * 1ull * C;
+            const int t = threadIdx.x, lane = t % 32, warp = t / 32;
+            double na[LA], nx[LX];
+            auto load = [&](unsigned long long k0) {
+    #pragma unroll
+                for (int u = 0; u < LA; ++u) {
+                    const int i = t + u * 256, row = i / K, k = i % K;
+                    na[u] = (r0 + row < n && k0 + k < n) ? a[(r0 + row) * n + k0 + k] : 0.0;
+                }
+    #pragma unroll
+                for (int u = 0; u < LX; ++u) {
+                    const int i = t + u * 256, k = i / C, c = i % C;
+                    nx[u] = (k0 + k < n && c0 + c < width) ? x[(k0 + k) * width + c0 + c] : 0.0;
+                }
+            };
+            double acc[C];
+    #pragma unroll
+            for (int c = 0; c < C; ++c) acc[c] = 0.0;
+            load(0);
+            for (unsigned long long k0 = 0; k0 < n; k0 += K) {
+                __syncthreads();  // the previous slice is used up
+    #pragma unroll
+                for (int u = 0; u < LA; ++u) {
+                    const int i = t + u * 256;
+                    as[(i / K) * PA + i % K] = na[u];
+                }
+    #pragma unroll
+                for (int u = 0; u < LX; ++u) xs[t + u * 256] = nx[u];
+                __syncthreads();
+                if (k0 + K < n) load(k0 + K);
+    #pragma unroll
+                for (int k = 8 * warp; k < 8 * warp + 8; ++k) {
+                    const double av = as[lane * PA + k];
+    #pragma unroll
+                    for (int c = 0; c < C; ++c) acc[c] = fma(av, xs[k * C + c], acc[c]);
+                }
+            }
+            // r = b - (warp 0 + warp 1 + ... + warp 7), eight columns at a time through `as`
+    #pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                __syncthreads();
+    #pragma unroll
+                for (int c = 0; c < C / 2; ++c) as[(warp * R + lane) * (C / 2) + c] = acc[half * (C / 2) + c];
+                __syncthreads();
+                const int row = t / (C / 2), c = half * (C / 2) + t % (C / 2);
+                double sum = 0.0;
+    #pragma unroll
+                for (int w = 0; w < 8; ++w) sum += as[(w * R + row) * (C / 2) + t % (C / 2)];
+                const unsigned long long gr = r0 + row, gc = c0 + c;
+                if (gr < n && gc < width) r[gr * width + gc] = b[gr * width + gc] - sum;
+            }
+        }
+
         // ---- FP64 helpers of the refinement -----------------------------------------------------------
         __global__ void narrow(const double *in, float *out, unsigned long long count) {
             for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < count; i += 256ull * gridDim.x)
@@ -1719,8 +1785,10 @@ namespace {
     int backward_error(Context &ctx, const double *a, const double *b, const double *x, double *r, double *sums,
                        double *norms, unsigned long long n, unsigned long long width, double a_norm, const double *b_norm,
                        double &berr) {
-        cudaMemcpyAsync(r, b, n * width * 8, cudaMemcpyDeviceToDevice, ctx.stream);
-        if (int code = update<double>(ctx, a, n, x, width, r, width, n, width, n)) return code;
+        residual_rows<<<dim3(static_cast<unsigned>((n + kResidualRows - 1) / kResidualRows),
+                             static_cast<unsigned>((width + kResidualColumns - 1) / kResidualColumns)),
+                        256, 0, ctx.stream>>>(a, x, b, r, n, width);
+        if (int code = ctx.check(cudaGetLastError(), "launching the residual")) return code;
         column_max<<<static_cast<unsigned>(width), 256, 0, ctx.stream>>>(r, n, width, norms);
         column_max<<<static_cast<unsigned>(width), 256, 0, ctx.stream>>>(x, n, width, norms + width);
         std::vector<double> host(2 * width);
