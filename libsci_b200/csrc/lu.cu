@@ -1155,10 +1155,6 @@ namespace sci_cuda {
                 return simt_gemm<T>(ctx, a + t0 * n + J0, n, a + J0 * n + c0, n, a + t0 * n + c0, n, n - t0, c1 - c0, ob,
                                     true);
             };
-            static const bool narrow_simt = [] {
-                const char *setting = std::getenv("SCI_CUDA_NARROW");
-                return !(setting && std::strcmp(setting, "tensor") == 0);
-            }();
             bool side_pending = false;
             for (unsigned long long J0 = 0; J0 < n; J0 += kOuter) {
                 const unsigned long long ob = std::min<unsigned long long>(kOuter, n - J0), block_end = J0 + ob;
@@ -1211,7 +1207,7 @@ namespace sci_cuda {
                 }
                 // the next block's columns (all columns beyond without look-ahead)
                 if (int code = block_rows(J0, block_end, block_end, split_at)) return code;
-                if (int code = trailing(J0, block_end, block_end, split_at, ahead && narrow_simt)) return code;
+                if (int code = trailing(J0, block_end, block_end, split_at, ahead)) return code;
             }
             if (side_pending) {
                 if (int code = ctx.check(cudaStreamWaitEvent(ctx.stream, ctx.side_done, 0), "waiting for the side")) return code;
