@@ -57,6 +57,14 @@ namespace sci_cuda {
         __device__ __forceinline__ void cluster_sync() {
             asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
         }
+        // 16 bytes into another CTA's shared memory (a shared::cluster address from mapa), counted
+        // as complete_tx bytes on that CTA's mbarrier `bar` (also a mapped address).
+        __device__ __forceinline__ void send16(unsigned address, unsigned x, unsigned y, unsigned z, unsigned w, unsigned bar) {
+            asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];" ::"r"(
+                                 address),
+                         "r"(x), "r"(y), "r"(z), "r"(w), "r"(bar)
+                         : "memory");
+        }
         __device__ __forceinline__ unsigned remote(const void *local, unsigned rank) {
             const unsigned address = static_cast<unsigned>(__cvta_generic_to_shared(local));
             unsigned mapped;
@@ -185,15 +193,16 @@ namespace sci_cuda {
         // at once. A final permutation moves the at most 2 W displaced rows to their positions.
         //
         // Per column: each warp's best row is published in shared memory; warp 0 alone waits for
-        // them (a named barrier the other warps only arrive at) and publishes the CTA's candidate
-        // with its values; one cluster barrier; warp 0 of every CTA then reads all 8 candidates, their
-        // rows and the row at the pivot position in one round of distributed shared-memory loads,
-        // picks the pivot, and one CTA barrier hands it to every thread. Buffers read across the
-        // cluster alternate by column parity, so one is rewritten only after a later cluster barrier
-        // every reader has passed.
+        // them (a named barrier the other warps only arrive at) and pushes the CTA's candidate with
+        // its values into every CTA's inbox (st.async, counted on the receiver's mbarrier; CTA 0
+        // also pushes the row at the pivot position); warp 0 of every CTA waits for its own inbox
+        // to fill (a bounded wait), picks the pivot, and one CTA barrier hands it to every thread.
+        // Inboxes alternate by column parity; a CTA sends into one again only after its own pivot
+        // decision of the column in between, which needed every CTA's message of that column.
         template <typename T, int CL>
         __global__ void __launch_bounds__(kPanelBlock, 1)
-                panel_factor(T *a, unsigned long long n, unsigned long long j0, int width, long long *piv, Movement *moved) {
+                panel_factor(T *a, unsigned long long n, unsigned long long j0, int width, long long *piv, Movement *moved,
+                             int *status) {
             constexpr int kClusterCtas = CL, kCtaRows = PanelShape<CL>::rows;
             constexpr int W = PanelWidth<T>::value, R = PanelShape<CL>::per_thread, TH = kPanelBlock, WARPS = TH / 32;
             constexpr int P = kCtaRows + 1;  // pitch of the staged multipliers
@@ -205,10 +214,13 @@ namespace sci_cuda {
             __shared__ unsigned warp_rel[WARPS];
             __shared__ unsigned long long warp_origin[WARPS];
             __shared__ __align__(16) T warp_values[WARPS][W];
-            __shared__ Key cand_key[2];
-            __shared__ unsigned cand_rel[2];
-            __shared__ unsigned long long cand_origin[2];
-            __shared__ __align__(16) T cand_values[2][W];
+            // The inbox, by column parity: slot q < CL holds CTA q's candidate (its values, then a
+            // 32-byte head: key, origin, row), slot CL the row at the pivot position (from CTA 0).
+            // Senders write it with st.async; inbox_bar[parity] counts the bytes.
+            __shared__ __align__(16) T inbox[2][kClusterCtas + 1][W];
+            __shared__ __align__(16) unsigned long long inbox_head[2][kClusterCtas + 1][4];
+            __shared__ __align__(8) unsigned long long inbox_bar[2];
+            __shared__ bool stalled;
             __shared__ __align__(16) T jbuf[2][W];  // CTA 0: the row at the pivot position
             __shared__ unsigned long long jbuf_origin[2];
             __shared__ __align__(16) T pivot_row[W];
@@ -284,32 +296,50 @@ namespace sci_cuda {
                     unsigned r2 = lane < WARPS ? warp_rel[lane] : kNoRow;
                     best_of_warp(k2, r2);
                     const unsigned source = r2 == kNoRow ? 0u : ((r2 - c * kCtaRows) % TH) / 32;
-                    if (lane < Q) cand_values[par][lane] = warp_values[source][lane];
-                    if (lane == 0) {
-                        cand_key[par] = k2;
-                        cand_rel[par] = r2;
-                        cand_origin[par] = warp_origin[source];
+                    // 2. lane q sends this CTA's candidate (and CTA 0 the pivot-position row) to CTA q,
+                    //    16 bytes per store; every CTA then waits for its own inbox to fill. A slot of
+                    //    parity par is rewritten two columns later, after every reader has taken its
+                    //    pivot from it (each CTA's next message follows its own pivot decision).
+                    constexpr unsigned kValueBytes = Q * sizeof(T), kMessage = kValueBytes + 32;
+                    static_assert(kValueBytes % 16 == 0, "16-byte stores");
+                    if (lane < static_cast<unsigned>(kClusterCtas)) {
+                        const unsigned bar = remote(&inbox_bar[par], lane);
+                        auto send = [&](const T *values, unsigned slot, unsigned long long k, unsigned long long o, unsigned rw) {
+                            const unsigned *words = reinterpret_cast<const unsigned *>(values);
+                            const unsigned base = remote(&inbox[par][slot][0], lane);
+#pragma unroll
+                            for (unsigned m = 0; m < kValueBytes / 16; ++m)
+                                send16(base + 16 * m, words[4 * m], words[4 * m + 1], words[4 * m + 2], words[4 * m + 3], bar);
+                            const unsigned head = remote(&inbox_head[par][slot][0], lane);
+                            send16(head, static_cast<unsigned>(k), static_cast<unsigned>(k >> 32), static_cast<unsigned>(o),
+                                   static_cast<unsigned>(o >> 32), bar);
+                            send16(head + 16, rw, 0u, 0u, 0u, bar);
+                        };
+                        send(warp_values[source], c, static_cast<unsigned long long>(k2), warp_origin[source], r2);
+                        if (c == 0) send(jbuf[par], kClusterCtas, 0ull, jbuf_origin[par], 0u);
                     }
-                } else {
-                    named_arrive(1, TH);
-                }
-                cluster_sync();  // the candidates and the pivot-position row are published
-                // 2. the pivot: warp 0 of every CTA reads all candidates in one round of loads
-                if (warp == 0) {
+                    if (lane == 0) barrier_expect(&inbox_bar[par], (kClusterCtas + 1) * kMessage);
+                    const bool arrived = stalled ? false : barrier_wait(&inbox_bar[par], static_cast<unsigned>(j >> 1) & 1u);
+                    if (!arrived && lane == 0 && !stalled) {
+                        // a message never came: flag it, take no more waits, finish with what is here
+                        stalled = true;
+                        atomicOr(status, kStatusTimeout);
+                    }
+                    __syncwarp();
+                    // 3. the pivot, from the inbox
                     Key k3 = 0;
                     unsigned r3 = kNoRow;
                     unsigned long long org = 0;
                     if (lane < kClusterCtas) {
-                        k3 = load_remote_key(remote(&cand_key[par], lane), Key(0));
-                        r3 = load_remote_u32(remote(&cand_rel[par], lane));
-                        org = load_remote_u64(remote(&cand_origin[par], lane));
+                        k3 = static_cast<Key>(inbox_head[par][lane][0]);
+                        org = inbox_head[par][lane][1];
+                        r3 = static_cast<unsigned>(inbox_head[par][lane][2]);
                     }
                     T values[kClusterCtas];
 #pragma unroll
-                    for (int q = 0; q < kClusterCtas; ++q)
-                        values[q] = lane < Q ? load_remote(remote(&cand_values[par][lane], q), T(0)) : T(0);
-                    const T there = lane < Q ? load_remote(remote(&jbuf[par][lane], 0), T(0)) : T(0);
-                    const unsigned long long there_origin = load_remote_u64(remote(&jbuf_origin[par], 0));
+                    for (int q = 0; q < kClusterCtas; ++q) values[q] = lane < Q ? inbox[par][q][lane] : T(0);
+                    const T there = lane < Q ? inbox[par][kClusterCtas][lane] : T(0);
+                    const unsigned long long there_origin = inbox_head[par][kClusterCtas][1];
                     best_of_warp(k3, r3);
                     // the winner's CTA owns its row; no candidate cannot happen (row_j is one)
                     const unsigned q = r3 == kNoRow ? 0u : r3 / kCtaRows;
@@ -330,6 +360,8 @@ namespace sci_cuda {
                         if (exchange) displaced_origin = there_origin;
                         if (c == 0) exchanges[j] = static_cast<long long>(prow);
                     }
+                } else {
+                    named_arrive(1, TH);
                 }
                 __syncthreads();
                 const unsigned long long prow = pivot_at;
@@ -372,6 +404,13 @@ namespace sci_cuda {
                     v[i][Q - 1] = T(0);
                 }
             };
+            if (t == 0) {
+                barrier_init(&inbox_bar[0], 1);
+                barrier_init(&inbox_bar[1], 1);
+                stalled = false;
+                asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            }
+            cluster_sync();  // every CTA's inbox barriers exist before the first message
 #pragma unroll 1
             for (int j = 0; j < width; ++j) {
                 const int live = width - j;
@@ -465,7 +504,7 @@ namespace sci_cuda {
         // Launches panel_factor<T, CL> as one cluster of CL CTAs.
         template <typename T, int CL>
         cudaError_t launch_panel(cudaStream_t stream, T *a, unsigned long long n, unsigned long long j0, int w, long long *piv,
-                                 Movement *moved) {
+                                 Movement *moved, int *status) {
             cudaLaunchConfig_t config{};
             config.gridDim = dim3(CL);
             config.blockDim = dim3(kPanelBlock);
@@ -478,7 +517,7 @@ namespace sci_cuda {
             attribute[0].val.clusterDim.z = 1;
             config.attrs = attribute;
             config.numAttrs = 1;
-            return cudaLaunchKernelEx(&config, panel_factor<T, CL>, a, n, j0, w, piv, moved);
+            return cudaLaunchKernelEx(&config, panel_factor<T, CL>, a, n, j0, w, piv, moved, status);
         }
 
         // The panel's cluster size for this process: 16 CTAs (half the rows per SM, a non-portable
@@ -1162,8 +1201,8 @@ namespace sci_cuda {
                 for (unsigned long long j0 = J0; j0 < block_end; j0 += W, ++panels) {
                     const int w = static_cast<int>(std::min<unsigned long long>(W, block_end - j0));
                     Movement *mine = moved + panels;
-                    const cudaError_t launched = cluster == 16 ? launch_panel<T, 16>(ctx.stream, a, n, j0, w, piv, mine)
-                                                               : launch_panel<T, 8>(ctx.stream, a, n, j0, w, piv, mine);
+                    const cudaError_t launched = cluster == 16 ? launch_panel<T, 16>(ctx.stream, a, n, j0, w, piv, mine, ctx.status)
+                                                               : launch_panel<T, 8>(ctx.stream, a, n, j0, w, piv, mine, ctx.status);
                     if (int code = ctx.check(launched, "launching the panel factorisation")) return code;
                     // the panel's row movement: now inside the block (everywhere without look-ahead)
                     const unsigned long long m0 = ahead ? J0 : 0, m1 = ahead ? block_end : n;
