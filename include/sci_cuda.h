@@ -168,7 +168,8 @@ int sci_cuda_factor(sci_cuda_context *context, uint32_t precision, uint32_t mode
 /* linear::solve (include/linear/solve.hpp:60-76): solution (order x width) with matrix * solution =
  * right, all device memory, row-major. refine = SCI_REFINE_NONE factors and substitutes in the
  * element type (the reference's behaviour); SCI_REFINE_FP64 (double operands) factors in FP32
- * and iterates r = b - A x in FP64 until the normwise backward error is <= 1e-15 or stalls.
+ * and iterates r = b - A x in FP64 until the normwise backward error is <= min(sqrt(n) 2^-53, 1e-14)
+ * (LAPACK DSGESV's test) or stalls.
  * `report` (may be null) receives the backward error and iteration count. Waits. order <= 8192. */
 int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uint32_t refine, const void *matrix, const void *right,
                    void *solution, uint64_t order, uint64_t width, sci_solve_report *report);

@@ -23,7 +23,8 @@
 // solve with refinement (SCI_REFINE_FP64): the matrix is factored in FP32, then
 //    x = 0, r = b;  repeat: solve LU d = P r in FP32; x += d;  r = b - A x in FP64
 // until the normwise backward error |r|_inf / (|A|_inf |x|_inf + |b|_inf) of every column is at
-// most 1e-15 or stops improving. Only the residual and the update run in FP64.
+// most sqrt(n) eps (eps = 2^-53, as LAPACK's DSGESV; at most 1e-14) or stops improving. Only the
+// residual and the update run in FP64.
 #include "context.hpp"
 #include "workspace.hpp"
 
@@ -1853,8 +1854,11 @@ namespace {
     }
 
     // The refinement loop for a x = b (a n x n, b and x n x width, double): x = 0, r = b; repeat
-    // { x += correct(r); r = b - a x in FP64 } until the normwise backward error is at most 1e-15 or
-    // stops halving, at most 30 corrections. correct(r, x) adds the FP32 correction for residual r into x.
+    // { x += correct(r); r = b - a x in FP64 } until the normwise backward error
+    // max_j |r_j|_inf / (|A|_inf |x_j|_inf + |b_j|_inf) is at most sqrt(n) eps (eps = 2^-53, the
+    // stopping test of LAPACK's mixed-precision DSGESV) capped at 1e-14, or stops halving; at most
+    // 30 corrections.
+    // correct(r, x) adds the FP32 correction for residual r into x.
     template <class Correct>
     int refine_loop(Context &ctx, const double *a, const double *b, double *x, double *r, double *sums, double *norms,
                     unsigned long long n, unsigned long long width, Correct correct, double &berr, int &iterations) {
@@ -1862,6 +1866,7 @@ namespace {
         std::vector<double> b_norm;
         if (int code = norms_of(ctx, a, b, sums, norms, n, width, a_norm, b_norm)) return code;
         cudaMemsetAsync(x, 0, n * width * 8, ctx.stream);
+        const double target = std::min(std::sqrt(static_cast<double>(n)) * 0x1p-53, 1e-14);
         constexpr int kMaxIterations = 30;
         double previous = INFINITY;
         berr = INFINITY;
@@ -1872,7 +1877,7 @@ namespace {
             ++iterations;
             if (int code = backward_error(ctx, a, b, x, r, sums, norms, n, width, a_norm, b_norm.data(), berr)) return code;
             residual = r;
-            if (!(berr > 1e-15) || !(berr < 0.5 * previous)) break;
+            if (!(berr > target) || !(berr < 0.5 * previous)) break;
             previous = berr;
         }
         return SCI_CUDA_OK;

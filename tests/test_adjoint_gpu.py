@@ -5,7 +5,7 @@ error bounds of each product mode (tests/test_product_gpu.py) and against libsci
 of the transposed operands.
 solve: for X = A^-1 B, dL/dB = lambda = A^-T G and dL/dA = -lambda X^T, checked against FP64 numpy
 and against central differences of L = sum(G * solve(A, B)) through libsci's own CPU solve<double>.
-Refined solves reach a backward error <= 1e-15 in both the forward and the transposed system, so
+Refined solves reach a backward error <= 1e-14 in both the forward and the transposed system, so
 their gradients match FP64 to 1e-10 relative (normwise) on these well-conditioned systems.
 """
 import numpy as np
