@@ -1,6 +1,6 @@
 """Python host layer over the C ABI: a CUDA ``Device`` and arrays that live on it.
 
-Mirrors the parts of libsci's C++ front end the north-star path uses:
+Mirrors the parts of libsci's C++ front end that the chunk, product and solve paths use:
 
 - ``Device`` is ``sci::Device`` with a CUDA target (include/core/drivers/device.hpp:27-89):
   ``execute`` / ``reduce`` / ``synchronize`` / ``name`` and memory.
