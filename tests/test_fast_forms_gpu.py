@@ -145,3 +145,49 @@ def test_composite_chunks_match_the_interpreter(name):
     finally:
         interpreter.close()
         specialised.close()
+
+
+REACH = 1048576.0  # 2^20: the circular functions' own reduction reaches this far
+CIRCULAR = {"sin": 2, "cos": 2, "tan": 4, "csc": 4, "sec": 4, "cot": 4}  # ulp allowed beyond REACH
+
+
+@pytest.mark.gpu
+def test_exact_codes_match_the_oracle_across_the_float_range(oracle):
+    """The exact codes (every code but the C-library functions) through the interpreter and through
+    the specialised kernels, against the oracle (itself pinned to libsci's CPU path over the same
+    inputs in test_oracle.py): every 257th float bit pattern and 2^22 hashed doubles, bit for bit,
+    except the circular functions beyond |x| = 2^20, which both sides take from a double-precision
+    library and which stay within 2 ulp (4 for the quotients)."""
+    from libsci_b200 import chunk as C
+    from tests import _oracle
+    from tests.test_oracle import EXACT_UNARY, hashed_doubles, spread_floats
+
+    devices = [open_device("0"), open_device("sync")]
+    try:
+        for x in (spread_floats(), hashed_doubles(1 << 22)):
+            n = x.size
+            expected = {}
+            for device in devices:
+                dx = device.array(x)
+                out = device.empty(n, x.dtype)
+                for code in EXACT_UNARY:
+                    chunk = C.record_output(C.Node(code, [dx.expression()]))
+                    if code not in expected:
+                        expected[code] = _oracle.execute(oracle, _oracle.on_host(chunk, {dx.pointer: x}), n, x.dtype)
+                    device.execute(chunk, out.pointer, n)
+                    device.synchronize()
+                    got = out.numpy()
+                    near = ~(np.abs(x) > REACH) if code in CIRCULAR else np.ones(n, bool)
+                    bad = _oracle.mismatches(got[near], expected[code][near])
+                    assert bad.size == 0, f"{code} ({x.dtype}): {bad.size} differ, first input {x[near][bad[0]]!r}"
+                    if code in CIRCULAR:
+                        # beyond the reduction's reach both sides round a double-precision library
+                        # result, CUDA's here and glibc's in the reference
+                        far = ~near
+                        worst = int(_oracle.ulp_distance(got[far], expected[code][far]).max(initial=0))
+                        assert worst <= CIRCULAR[code], f"{code} ({x.dtype}) beyond 2^20: {worst} ulp"
+                dx.free()
+                out.free()
+    finally:
+        for device in devices:
+            device.close()

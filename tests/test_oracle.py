@@ -143,3 +143,37 @@ def test_factor_restates_the_reference(oracle, reference):
     reference.sci_ref_factor_f32(m2.ctypes.data, r2.ctypes.data, 128)
     assert np.array_equal(r1, r2)
     assert _oracle.mismatches(m1.ravel(), m2.ravel()).size == 0
+
+
+# The codes whose results are exact sequences of rounded operations (not the C library's): every one
+# must match libsci's CPU path bit for bit on any input.
+EXACT_UNARY = ["copy", "negate", "absolute", "root", "exponential", "logarithm", "sin", "cos", "tan", "csc",
+               "sec", "cot"]
+
+
+def spread_floats(stride: int = 257) -> np.ndarray:
+    """Every stride-th float bit pattern, 2^32 / stride values spanning every exponent and sign."""
+    return (np.arange(0, 1 << 32, stride, dtype=np.uint64).astype(np.uint32)).view(np.float32)
+
+
+def hashed_doubles(count: int, seed: int = 11) -> np.ndarray:
+    """Doubles from hashed 64-bit patterns, half of them any pattern, half in each code's ordinary range."""
+    rng = np.random.default_rng(seed)
+    out = rng.integers(0, 1 << 63, count, dtype=np.int64).view(np.float64).copy()
+    out[1::4] = rng.uniform(-750, 750, out[1::4].size)
+    out[2::4] = rng.uniform(0, 1e6, out[2::4].size)
+    out[3::4] = rng.uniform(-2.2e6, 2.2e6, out[3::4].size)
+    return out
+
+
+@pytest.mark.parametrize("code", EXACT_UNARY)
+def test_oracle_matches_the_reference_across_the_float_range(oracle, reference, code):
+    """The exact codes on every 257th float bit pattern (16.7 M values: all exponents, both signs,
+    subnormals, infinities and NaNs) and on 2^22 hashed doubles."""
+    for x in (spread_floats(), hashed_doubles(1 << 22)):
+        n = x.size
+        chunk = C.record_output(C.Node(code, [C.Reference(x.ctypes.data, n, x.dtype)]))
+        mine = _oracle.execute(oracle, chunk, n, x.dtype)
+        theirs = _oracle.execute(reference, chunk, n, x.dtype)
+        bad = _oracle.mismatches(mine, theirs)
+        assert bad.size == 0, f"{code} ({x.dtype}): {bad.size} of {n} differ, first input {x[bad[0]]!r}"
