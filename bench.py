@@ -737,9 +737,91 @@ def run_solves(args) -> int:
     return 0
 
 
+def run_creation(args) -> int:
+    """Arrays made on the device (include/operations/creation.hpp): full, linspace, range and eye of
+    2^28 float32 elements (1 GiB each) and grid of 16384 x 16384 (two 1 GiB outputs), one step = all
+    five. Bound by HBM writes: 4 B/element, 8 for grid. Beside them: the reference's own creation
+    functions (libsci's host loops) on a 2^24-element sample."""
+    import torch
+
+    from libsci_b200.device import Device
+    from libsci_b200.native import check, lib
+    from tests import _oracle
+    from tests.test_oracle import creation_functions
+
+    count, side = 1 << 28, 1 << 14
+    peak, peak_source = measured_peaks()
+    device = Device(0)
+    stream = torch.cuda.ExternalStream(device.stream)
+    out = device.empty(count)
+    second = device.empty(count)
+    x, y = device.linspace(-1.0, 1.0, side), device.linspace(0.0, 5.0, side)
+    steps = {
+        "full": (lambda: check(lib.sci_cuda_fill(device.handle, 0, out.pointer, count, 2.5), device.handle), 4 * count),
+        "linspace": (lambda: check(lib.sci_cuda_linspace(device.handle, 0, out.pointer, count, -3.0, 7.0), device.handle),
+                     4 * count),
+        "range": (lambda: check(lib.sci_cuda_range(device.handle, 0, out.pointer, count, -1.0, 0.25), device.handle),
+                  4 * count),
+        "eye": (lambda: check(lib.sci_cuda_eye(device.handle, 0, out.pointer, side, side), device.handle), 4 * count),
+        "grid": (lambda: check(lib.sci_cuda_grid(device.handle, 0, x.pointer, side, y.pointer, side, out.pointer,
+                                                 second.pointer), device.handle), 8 * count),
+    }
+    for _ in range(args.warmup):
+        for launch, _bytes in steps.values():
+            launch()
+    device.synchronize()
+    kernels = {name: [] for name in steps}
+    totals = []
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            marks = [torch.cuda.Event(enable_timing=True) for _ in range(len(steps) + 1)]
+            marks[0].record(stream)
+            for index, (launch, _bytes) in enumerate(steps.values()):
+                launch()
+                marks[index + 1].record(stream)
+            marks[-1].synchronize()
+            for index, name in enumerate(steps):
+                kernels[name].append(marks[index].elapsed_time(marks[index + 1]))
+            totals.append(marks[0].elapsed_time(marks[-1]))
+    ms = statistics.median(totals)
+    moved = sum(b for _launch, b in steps.values())
+    per = {name: {"ms": statistics.median(t), "GB/s": steps[name][1] / (statistics.median(t) * 1e-3) / 1e9,
+                  "frac": steps[name][1] / (statistics.median(t) * 1e-3) / 1e9 / peak} for name, t in kernels.items()}
+    top = max(per, key=lambda name: per[name]["ms"])
+
+    ref = None if args.no_cpu else _oracle.reference()
+    cpu = None
+    if ref is not None:
+        theirs = creation_functions(ref, "sci_ref")
+        sample = 1 << 24
+        host = np.empty(sample, np.float32)
+        started = time.perf_counter()
+        theirs["full"](0, host.ctypes.data, sample, 2.5)
+        theirs["linspace"](0, host.ctypes.data, sample, -3.0, 7.0)
+        theirs["range"](0, host.ctypes.data, sample, -1.0, -1.0 + 0.25 * sample, 0.25)
+        theirs["eye"](0, host.ctypes.data, 1 << 12, 1 << 12)
+        seconds = time.perf_counter() - started
+        cpu = {"value": 4 * 4 * sample / seconds / 1e9, "unit": "GB/s", "cores": 1, "kind": "reference",
+               "sample": "2^24 elements of full, linspace, range and eye each through libsci's own creation "
+                         "functions (host loops, one thread)"}
+    line = {"metric": "device creation GB/s written vs HBM peak", "value": moved / (ms * 1e-3) / 1e9, "unit": "GB/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "full, linspace, range, eye of 2^28 floats; grid 16384 x 16384",
+                       "bytes_written": moved, "l2": "each output 1 GiB, above L2"},
+            "kernels": per,
+            "roofline": {"bound": "hbm", "achieved": per[top]["GB/s"], "peak": peak, "unit": "GB/s",
+                         "frac": per[top]["frac"], "traffic": None, "kernel": top, "peak_source": peak_source},
+            "cpu_baseline": cpu, "gpu_launches": len(steps) * args.steps, "clocks": clocks.summary()}
+    print(json.dumps(line))
+    device.close()
+    return 0
+
+
 def main() -> int:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--workload", default="chunks", choices=["chunks", "product", "solve", "gradient", "batch", "solves"])
+    parser.add_argument("--workload", default="chunks",
+                        choices=["chunks", "product", "solve", "gradient", "batch", "solves", "creation"])
     parser.add_argument("--size", type=int, default=8192)
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=20)
@@ -766,6 +848,8 @@ def main() -> int:
         return run_gradient(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "creation":
+        return run_creation(args)
     if args.workload == "solves":
         return run_solves(args)
 

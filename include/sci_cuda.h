@@ -283,6 +283,26 @@ int sci_cuda_solve_batch_destroy(sci_cuda_solve_batch *batch);
  * failure a message is written to `message` (may be null). */
 int sci_cuda_reduce_noalloc(const sci_chunk *chunk, uint32_t fold, uint64_t count, double *device_result,
                             void *stream, uint32_t blocks, char *message, size_t message_length);
+/* ---- arrays made on the device (include/operations/creation.hpp) ----------------------------
+ * The element values of libsci's creation functions, computed where the array lives, on the
+ * context's stream (asynchronous). `output` (and grid's operands) must be device memory of the
+ * context; `precision` is SCI_PRECISION_SINGLE (float) or SCI_PRECISION_WIDE (double). */
+/* zeros / ones / full (creation.hpp:34-58): output[0, count) := value, cast to the element type. */
+int sci_cuda_fill(sci_cuda_context *context, uint32_t precision, void *output, uint64_t count, double value);
+/* linspace (creation.hpp:66-84): count values from start to stop, both included; start and stop
+ * are elements (their difference is taken in the element type, the rest in double). */
+int sci_cuda_linspace(sci_cuda_context *context, uint32_t precision, void *output, uint64_t count, double start,
+                      double stop);
+/* range (creation.hpp:157-168): the count of start, start + step, ... below stop (host only). */
+uint64_t sci_cuda_range_count(uint32_t precision, double start, double stop, double step);
+/* range: output[i] = start + element(i) * step in the element type, for that count. */
+int sci_cuda_range(sci_cuda_context *context, uint32_t precision, void *output, uint64_t count, double start,
+                   double step);
+/* eye (creation.hpp:91-106): a rows x columns row-major matrix with ones on the main diagonal. */
+int sci_cuda_eye(sci_cuda_context *context, uint32_t precision, void *output, uint64_t rows, uint64_t columns);
+/* grid (creation.hpp:120-140, numpy.meshgrid): xx[i][j] = x[j], yy[i][j] = y[i], both ny x nx. */
+int sci_cuda_grid(sci_cuda_context *context, uint32_t precision, const void *x, uint64_t nx, const void *y, uint64_t ny,
+                  void *xx, void *yy);
 /* Waits until every queued NVRTC specialisation has been compiled and loaded
  * (vulkan::Compiler::loop, src/core/drivers/vulkan/compiler.cpp:184-222, compiles in the
  * background the same way; a chunk runs on the interpreter until its kernel is ready).

@@ -80,6 +80,64 @@ class Device:
         out.upload(host)
         return out
 
+    # -- creation on the device (include/operations/creation.hpp) ---------------------------------
+    @staticmethod
+    def _precision(dtype) -> int:
+        dtype = np.dtype(dtype)
+        if dtype == np.float32:
+            return C.SINGLE
+        if dtype == np.float64:
+            return C.WIDE
+        raise TypeError(f"device arrays are float32 or float64, not {dtype}")
+
+    def full(self, count: int, value: float, dtype=np.float32) -> "DeviceArray":
+        """full (creation.hpp:52-58), filled on the device."""
+        out = self.empty(count, dtype)
+        check(lib.sci_cuda_fill(self.handle, self._precision(dtype), out.pointer, count, float(value)), self.handle)
+        return out
+
+    def zeros(self, count: int, dtype=np.float32) -> "DeviceArray":
+        """zeros (creation.hpp:34-38)."""
+        return self.full(count, 0.0, dtype)
+
+    def ones(self, count: int, dtype=np.float32) -> "DeviceArray":
+        """ones (creation.hpp:44-47)."""
+        return self.full(count, 1.0, dtype)
+
+    def linspace(self, start: float, stop: float, count: int, dtype=np.float32) -> "DeviceArray":
+        """linspace (creation.hpp:66-84): count values from start to stop, both included."""
+        out = self.empty(count, dtype)
+        check(lib.sci_cuda_linspace(self.handle, self._precision(dtype), out.pointer, count, float(start), float(stop)),
+              self.handle)
+        return out
+
+    def range(self, start: float, stop: float | None = None, step: float = 1.0, dtype=np.float32) -> "DeviceArray":
+        """range (creation.hpp:157-176, numpy.arange): start, start + step, ... below stop;
+        range(stop) counts from 0."""
+        if stop is None:
+            start, stop = 0.0, start
+        precision = self._precision(dtype)
+        count = int(lib.sci_cuda_range_count(precision, float(start), float(stop), float(step)))
+        out = self.empty(count, dtype)
+        check(lib.sci_cuda_range(self.handle, precision, out.pointer, count, float(start), float(step)), self.handle)
+        return out
+
+    def eye(self, rows: int, columns: int | None = None, dtype=np.float32) -> "DeviceArray":
+        """eye (creation.hpp:91-117): a rows x columns row-major matrix, ones on the diagonal."""
+        columns = rows if columns is None else columns
+        out = self.empty(rows * columns, dtype)
+        check(lib.sci_cuda_eye(self.handle, self._precision(dtype), out.pointer, rows, columns), self.handle)
+        return out
+
+    def grid(self, x: "DeviceArray", y: "DeviceArray"):
+        """grid (creation.hpp:120-140, numpy.meshgrid): (xx, yy), each len(y) x len(x), row-major."""
+        if x.dtype != y.dtype:
+            raise TypeError("grid: x and y differ in type")
+        xx, yy = self.empty(x.count * y.count, x.dtype), self.empty(x.count * y.count, x.dtype)
+        check(lib.sci_cuda_grid(self.handle, self._precision(x.dtype), x.pointer, x.count, y.pointer, y.count,
+                                xx.pointer, yy.pointer), self.handle)
+        return xx, yy
+
     # -- chunks ---------------------------------------------------------------------------------
     def execute(self, chunk: C.Chunk, output: int, count: int) -> None:
         check(lib.sci_cuda_execute(self.handle, ctypes.byref(chunk), output, count), self.handle)

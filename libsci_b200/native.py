@@ -88,6 +88,13 @@ def _load() -> ctypes.CDLL:
     sig["sci_cuda_solve_batch_launch"] = (ctypes.c_int, [ctypes.c_void_p])
     sig["sci_cuda_solve_batch_shapes"] = (ctypes.c_int, [ctypes.c_void_p, P(ctypes.c_uint32)])
     sig["sci_cuda_solve_batch_destroy"] = (ctypes.c_int, [ctypes.c_void_p])
+    U64, F64, U32, VP = ctypes.c_uint64, ctypes.c_double, ctypes.c_uint32, ctypes.c_void_p
+    sig["sci_cuda_fill"] = (ctypes.c_int, [c_ctx, U32, VP, U64, F64])
+    sig["sci_cuda_linspace"] = (ctypes.c_int, [c_ctx, U32, VP, U64, F64, F64])
+    sig["sci_cuda_range_count"] = (U64, [U32, F64, F64, F64])
+    sig["sci_cuda_range"] = (ctypes.c_int, [c_ctx, U32, VP, U64, F64, F64])
+    sig["sci_cuda_eye"] = (ctypes.c_int, [c_ctx, U32, VP, U64, U64])
+    sig["sci_cuda_grid"] = (ctypes.c_int, [c_ctx, U32, VP, U64, VP, U64, VP, VP])
     optional = {}
     sig["sci_cuda_factor"] = (ctypes.c_int, [c_ctx, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                              ctypes.c_uint64])

@@ -221,4 +221,49 @@ const float *sci_ref_workload_output(void *handle, const int which) {
 
 void sci_ref_workload_destroy(void *handle) { delete static_cast<sci_ref_workload *>(handle); }
 
+// ---- creation: the reference's own functions (include/operations/creation.hpp) -----------------
+void sci_ref_full(uint32_t precision, void *out, uint64_t count, double value) {  // creation.hpp:52-58
+    if (precision == SCI_PRECISION_WIDE) {
+        const auto made = sci::operations::full<double>({count}, value);
+        std::memcpy(out, made.data(), count * sizeof(double));
+    } else {
+        const auto made = sci::operations::full<float>({count}, static_cast<float>(value));
+        std::memcpy(out, made.data(), count * sizeof(float));
+    }
+}
+
+void sci_ref_linspace(uint32_t precision, void *out, uint64_t count, double start, double stop) {  // :66-84
+    if (precision == SCI_PRECISION_WIDE) {
+        const auto made = sci::operations::linspace<double>(start, stop, count);
+        if (count) std::memcpy(out, made.data(), count * sizeof(double));
+    } else {
+        const auto made = sci::operations::linspace<float>(static_cast<float>(start), static_cast<float>(stop), count);
+        if (count) std::memcpy(out, made.data(), count * sizeof(float));
+    }
+}
+
+// range (creation.hpp:157-168): fills `out` (room for `capacity` values) and returns the count.
+uint64_t sci_ref_range(uint32_t precision, void *out, uint64_t capacity, double start, double stop, double step) {
+    if (precision == SCI_PRECISION_WIDE) {
+        const auto made = sci::operations::range<double>(start, stop, step);
+        const uint64_t count = made.shape()[0];
+        if (count && count <= capacity) std::memcpy(out, made.data(), count * sizeof(double));
+        return count;
+    }
+    const auto made = sci::operations::range<float>(static_cast<float>(start), static_cast<float>(stop), static_cast<float>(step));
+    const uint64_t count = made.shape()[0];
+    if (count && count <= capacity) std::memcpy(out, made.data(), count * sizeof(float));
+    return count;
+}
+
+void sci_ref_eye(uint32_t precision, void *out, uint64_t rows, uint64_t columns) {  // creation.hpp:91-106
+    if (precision == SCI_PRECISION_WIDE) {
+        const auto made = sci::operations::eye<double>({rows, columns});
+        std::memcpy(out, made.data(), rows * columns * sizeof(double));
+    } else {
+        const auto made = sci::operations::eye<float>({rows, columns});
+        std::memcpy(out, made.data(), rows * columns * sizeof(float));
+    }
+}
+
 } // extern "C"

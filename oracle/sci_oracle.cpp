@@ -15,7 +15,9 @@
 //    calling the same C library (glibc) functions;
 //  - reductions folded in double with numpy NaN rules (accumulator.hpp:17-48,
 //    dispatch.cpp:106-165), as the FP64 oracle the GPU reductions are held to;
-//  - linear::factor / substitute (include/linear/decompose.hpp:29-72, solve.hpp:25-52).
+//  - linear::factor / substitute (include/linear/decompose.hpp:29-72, solve.hpp:25-52);
+//  - the element values of the creation functions full / linspace / range / eye / grid
+//    (include/operations/creation.hpp:34-168).
 // Parity is pinned against the reference itself: tests compare this file's outputs with
 // oracle/_ref/libsci_ref.so (the reference's own CPU path) and with tests/golden fixtures.
 //
@@ -465,6 +467,40 @@ namespace {
 
 } // namespace
 
+// ---- creation (include/operations/creation.hpp) -----------------------------------------------
+namespace {
+    template <typename T> void fill_values(T *out, uint64_t count, T value) {  // creation.hpp:34-58
+        for (uint64_t i = 0; i < count; ++i) out[i] = value;
+    }
+    template <typename T> void linspace_values(T *out, uint64_t count, T start, T stop) {  // creation.hpp:66-84
+        if (count == 0) return;
+        if (count == 1) {
+            out[0] = start;
+            return;
+        }
+        const double step = static_cast<double>(stop - start) / (static_cast<double>(count) - 1.0);
+        for (uint64_t i = 0; i < count; ++i) out[i] = static_cast<T>(static_cast<double>(start) + static_cast<double>(i) * step);
+    }
+    template <typename T> uint64_t range_count(T start, T stop, T step) {  // creation.hpp:159-161
+        const double span = std::ceil((static_cast<double>(stop) - static_cast<double>(start)) / static_cast<double>(step));
+        return span > 0 ? static_cast<uint64_t>(span) : 0;
+    }
+    template <typename T> void range_values(T *out, uint64_t count, T start, T step) {  // creation.hpp:163-165
+        for (uint64_t i = 0; i < count; ++i) out[i] = static_cast<T>(start + static_cast<T>(i) * step);
+    }
+    template <typename T> void eye_values(T *out, uint64_t rows, uint64_t columns) {  // creation.hpp:91-106
+        for (uint64_t i = 0; i < rows * columns; ++i) out[i] = T(0);
+        for (uint64_t i = 0; i < (rows < columns ? rows : columns); ++i) out[i * columns + i] = T(1);
+    }
+    template <typename T> void grid_values(const T *x, uint64_t nx, const T *y, uint64_t ny, T *xx, T *yy) {  // :120-140
+        for (uint64_t i = 0; i < ny; ++i)
+            for (uint64_t j = 0; j < nx; ++j) {
+                xx[i * nx + j] = x[j];
+                yy[i * nx + j] = y[i];
+            }
+    }
+} // namespace
+
 extern "C" {
 
 // The pack width whose loop tails take the Scalar forms: 16 floats / 8 doubles for AVX-512.
@@ -513,6 +549,36 @@ void sci_oracle_product_rows(const float *a, const float *b, double *c, uint64_t
             std::copy(row.begin(), row.end(), c + (r - first) * n);
         }
     });
+}
+
+
+void sci_oracle_fill(uint32_t precision, void *out, uint64_t count, double value) {
+    if (precision == SCI_PRECISION_WIDE) fill_values(static_cast<double *>(out), count, value);
+    else fill_values(static_cast<float *>(out), count, static_cast<float>(value));
+}
+void sci_oracle_linspace(uint32_t precision, void *out, uint64_t count, double start, double stop) {
+    if (precision == SCI_PRECISION_WIDE) linspace_values(static_cast<double *>(out), count, start, stop);
+    else linspace_values(static_cast<float *>(out), count, static_cast<float>(start), static_cast<float>(stop));
+}
+uint64_t sci_oracle_range_count(uint32_t precision, double start, double stop, double step) {
+    if (precision == SCI_PRECISION_WIDE) return range_count(start, stop, step);
+    return range_count(static_cast<float>(start), static_cast<float>(stop), static_cast<float>(step));
+}
+void sci_oracle_range(uint32_t precision, void *out, uint64_t count, double start, double step) {
+    if (precision == SCI_PRECISION_WIDE) range_values(static_cast<double *>(out), count, start, step);
+    else range_values(static_cast<float *>(out), count, static_cast<float>(start), static_cast<float>(step));
+}
+void sci_oracle_eye(uint32_t precision, void *out, uint64_t rows, uint64_t columns) {
+    if (precision == SCI_PRECISION_WIDE) eye_values(static_cast<double *>(out), rows, columns);
+    else eye_values(static_cast<float *>(out), rows, columns);
+}
+void sci_oracle_grid(uint32_t precision, const void *x, uint64_t nx, const void *y, uint64_t ny, void *xx, void *yy) {
+    if (precision == SCI_PRECISION_WIDE)
+        grid_values(static_cast<const double *>(x), nx, static_cast<const double *>(y), ny, static_cast<double *>(xx),
+                    static_cast<double *>(yy));
+    else
+        grid_values(static_cast<const float *>(x), nx, static_cast<const float *>(y), ny, static_cast<float *>(xx),
+                    static_cast<float *>(yy));
 }
 
 } // extern "C"

@@ -177,3 +177,62 @@ def test_oracle_matches_the_reference_across_the_float_range(oracle, reference, 
         theirs = _oracle.execute(reference, chunk, n, x.dtype)
         bad = _oracle.mismatches(mine, theirs)
         assert bad.size == 0, f"{code} ({x.dtype}): {bad.size} of {n} differ, first input {x[bad[0]]!r}"
+
+
+# ---- creation (include/operations/creation.hpp) -------------------------------------------------
+def creation_functions(lib, prefix):
+    """ctypes signatures of the creation functions of the oracle or of the reference bridge."""
+    U32, U64, F64, VP = ctypes.c_uint32, ctypes.c_uint64, ctypes.c_double, ctypes.c_void_p
+    table = {"fill": [U32, VP, U64, F64], "full": [U32, VP, U64, F64], "linspace": [U32, VP, U64, F64, F64],
+             "range_count": [U32, F64, F64, F64], "range": [U32, VP, U64, F64, F64], "eye": [U32, VP, U64, U64],
+             "grid": [U32, VP, U64, VP, U64, VP, VP]}
+    out = {}
+    for name, args in table.items():
+        fn = getattr(lib, f"{prefix}_{name}", None)
+        if fn is None:
+            continue
+        fn.argtypes = args
+        fn.restype = U64 if name == "range_count" else None
+        out[name] = fn
+    if prefix == "sci_ref":
+        out["range"].argtypes = [U32, VP, U64, F64, F64, F64]
+        out["range"].restype = U64
+    return out
+
+
+LINSPACES = [(0.0, 1.0, 5), (-3.7, 11.2, 1001), (1e-30, 1e30, 257), (5.0, 5.0, 10), (-0.0, 3.0, 1), (2.5, -7.25, 100003),
+             (0.1, 0.7, 2), (0.0, 1.0, 0), (-1.0, 1.0, (1 << 20) + 3)]
+RANGES = [(0.0, 10.0, 1.0), (-5.5, 17.25, 0.37), (10.0, 0.0, -0.3), (0.0, 3e7, 1.0), (1.0, 1.0, 1.0), (0.0, 1.0, 3.0),
+          (0.1, 100.1, 0.01)]
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_creation_oracle_matches_the_reference(oracle, reference, dtype):
+    mine, theirs = creation_functions(oracle, "sci_oracle"), creation_functions(reference, "sci_ref")
+    precision = 1 if dtype == np.float64 else 0
+    for value in (0.0, 1.0, 2.5, -0.0, float("inf"), float("nan"), 1e40):
+        a, b = np.empty(1003, dtype), np.empty(1003, dtype)
+        mine["fill"](precision, a.ctypes.data, a.size, value)
+        theirs["full"](precision, b.ctypes.data, b.size, value)
+        assert _oracle.mismatches(a, b).size == 0, value
+    for start, stop, count in LINSPACES:
+        a, b = np.empty(max(count, 1), dtype), np.empty(max(count, 1), dtype)
+        mine["linspace"](precision, a.ctypes.data, count, start, stop)
+        theirs["linspace"](precision, b.ctypes.data, count, start, stop)
+        assert _oracle.mismatches(a[:count], b[:count]).size == 0, (start, stop, count)
+    for start, stop, step in RANGES:
+        count = mine["range_count"](precision, start, stop, step)
+        a, b = np.empty(max(count, 1), dtype), np.empty(max(count, 1), dtype)
+        mine["range"](precision, a.ctypes.data, count, start, step)
+        assert theirs["range"](precision, b.ctypes.data, b.size, start, stop, step) == count, (start, stop, step)
+        assert _oracle.mismatches(a[:count], b[:count]).size == 0, (start, stop, step)
+    for rows, columns in ((3, 3), (4, 7), (7, 4), (1, 1), (1000, 999)):
+        a, b = np.empty(rows * columns, dtype), np.empty(rows * columns, dtype)
+        mine["eye"](precision, a.ctypes.data, rows, columns)
+        theirs["eye"](precision, b.ctypes.data, rows, columns)
+        assert _oracle.mismatches(a, b).size == 0, (rows, columns)
+    x, y = np.arange(7, dtype=dtype) * 0.5, np.arange(5, dtype=dtype) - 2
+    xx, yy = np.empty(35, dtype), np.empty(35, dtype)
+    mine["grid"](precision, x.ctypes.data, 7, y.ctypes.data, 5, xx.ctypes.data, yy.ctypes.data)
+    gx, gy = np.meshgrid(x, y)  # numpy.meshgrid, which grid is named after
+    assert np.array_equal(xx.reshape(5, 7), gx) and np.array_equal(yy.reshape(5, 7), gy)
