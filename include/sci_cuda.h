@@ -303,6 +303,17 @@ int sci_cuda_eye(sci_cuda_context *context, uint32_t precision, void *output, ui
 /* grid (creation.hpp:120-140, numpy.meshgrid): xx[i][j] = x[j], yy[i][j] = y[i], both ny x nx. */
 int sci_cuda_grid(sci_cuda_context *context, uint32_t precision, const void *x, uint64_t nx, const void *y, uint64_t ny,
                   void *xx, void *yy);
+/* decompose (include/linear/decompose.hpp:77-103, scipy.linalg.lu): A = P L U with the
+ * factorisation (mode as sci_cuda_factor: SCI_FACTOR_PLAIN follows the reference's pivot order
+ * step for step) and the split into dense factors on the device. matrix (unchanged) and the three
+ * order x order outputs are device memory of the context; permutation[rows[c]][c] = 1. Waits. */
+int sci_cuda_decompose(sci_cuda_context *context, uint32_t precision, uint32_t mode, const void *matrix,
+                       void *permutation, void *lower, void *upper, uint64_t order);
+/* transpose (include/operations/manipulations.hpp:33-62, numpy.transpose): output (extents in
+ * reverse order) [j_{r-1}, ..., j_0] = input[j_0, ..., j_{r-1}], row-major, rank 1 to 8; output
+ * must not be the input. */
+int sci_cuda_transpose(sci_cuda_context *context, uint32_t precision, const void *input, uint32_t rank,
+                       const uint64_t *shape, void *output);
 /* Waits until every queued NVRTC specialisation has been compiled and loaded
  * (vulkan::Compiler::loop, src/core/drivers/vulkan/compiler.cpp:184-222, compiles in the
  * background the same way; a chunk runs on the interpreter until its kernel is ready).

@@ -1742,6 +1742,25 @@ namespace sci_cuda {
         }
 
         // out (n x n) = in^T, 32 x 32 tiles through shared memory.
+        // decompose's split of the packed factors (decompose.hpp:86-97): lower takes the strict lower
+        // part and a unit diagonal, upper keeps the rest (in place: it holds the packed factors on
+        // entry), and permutation[rows[c]][c] = 1.
+        template <typename T>
+        __global__ void split_factors(T *upper, T *lower, T *permutation, const unsigned *rows, unsigned long long n) {
+            const unsigned long long count = n * n, stride = 1ull * gridDim.x * blockDim.x;
+            for (unsigned long long i = 1ull * blockIdx.x * blockDim.x + threadIdx.x; i < count; i += stride) {
+                const unsigned long long r = i / n, c = i - r * n;
+                const T v = upper[i];
+                if (c < r) {
+                    lower[i] = v;
+                    upper[i] = T(0);
+                } else {
+                    lower[i] = c == r ? T(1) : T(0);
+                }
+                permutation[i] = rows[c] == r ? T(1) : T(0);
+            }
+        }
+
         template <typename T> __global__ void transpose_square(const T *in, T *out, unsigned long long n) {
             __shared__ T tile[32][33];
             const unsigned long long r0 = blockIdx.y * 32ull, c0 = blockIdx.x * 32ull;
@@ -1812,6 +1831,47 @@ extern "C" int sci_cuda_factor(sci_cuda_context *context, uint32_t precision, ui
     for (uint64_t i = 0; i < order; ++i) rows[i] = i;
     for (uint64_t i = 0; i < order; ++i) std::swap(rows[i], rows[static_cast<uint64_t>(host[i])]);
     return SCI_CUDA_OK;
+}
+
+// decompose (decompose.hpp:77-103) with the factorisation and the split on the device.
+extern "C" int sci_cuda_decompose(sci_cuda_context *context, uint32_t precision, uint32_t mode, const void *matrix,
+                                  void *permutation, void *lower, void *upper, uint64_t order) {
+    if (!context) return SCI_CUDA_ERROR_INVALID;
+    std::lock_guard<std::recursive_mutex> lock(context->guard);
+    if (precision > SCI_PRECISION_WIDE || mode > SCI_FACTOR_PLAIN)
+        return context->fail(SCI_CUDA_ERROR_INVALID, "unknown precision %u or mode %u", precision, mode);
+    if (order == 0) return SCI_CUDA_OK;
+    if (order > kPanelRows) return context->fail(SCI_CUDA_ERROR_UNSUPPORTED, "decompose: order %llu above %llu",
+                                                 static_cast<unsigned long long>(order), kPanelRows);
+    for (const void *p : {static_cast<const void *>(matrix), static_cast<const void *>(permutation),
+                          static_cast<const void *>(lower), static_cast<const void *>(upper)})
+        if (!p || !reachable(*context, p)) return context->fail(SCI_CUDA_ERROR_INVALID, "decompose: %p is not device memory", p);
+    cudaSetDevice(context->device);
+    const size_t element = precision == SCI_PRECISION_WIDE ? 8 : 4;
+    if (int code = context->check(context->solver->reserve(order * 12 + kMovements * sizeof(Movement) + 2048), "pivot storage"))
+        return code;
+    Carve carve{static_cast<unsigned char *>(context->solver->memory)};
+    long long *piv = carve.take<long long>(order);
+    Movement *moved = carve.take<Movement>(kMovements);
+    unsigned *rows = carve.take<unsigned>(order);
+    if (int code = context->check(cudaMemcpyAsync(upper, matrix, order * order * element, cudaMemcpyDeviceToDevice, context->stream),
+                                  "copying the matrix"))
+        return code;
+    int code = precision == SCI_PRECISION_WIDE
+                       ? factor_device<double>(*context, static_cast<double *>(upper), order, piv, moved, false, false)
+                       : factor_device<float>(*context, static_cast<float *>(upper), order, piv, moved,
+                                              mode != SCI_FACTOR_PLAIN, true);
+    if (code) return code;
+    if (int c = row_order(*context, piv, rows, order)) return c;
+    const unsigned grid = static_cast<unsigned>(std::min<unsigned long long>((order * order + 255) / 256, 8ull * context->sms));
+    if (precision == SCI_PRECISION_WIDE)
+        split_factors<double><<<grid, 256, 0, context->stream>>>(static_cast<double *>(upper), static_cast<double *>(lower),
+                                                                static_cast<double *>(permutation), rows, order);
+    else
+        split_factors<float><<<grid, 256, 0, context->stream>>>(static_cast<float *>(upper), static_cast<float *>(lower),
+                                                               static_cast<float *>(permutation), rows, order);
+    if (int c = context->check(cudaGetLastError(), "splitting the factors")) return c;
+    return context->drain();
 }
 
 namespace {

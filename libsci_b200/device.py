@@ -138,6 +138,26 @@ class Device:
                                 xx.pointer, yy.pointer), self.handle)
         return xx, yy
 
+    def transpose(self, array: "DeviceArray", shape) -> "DeviceArray":
+        """transpose (manipulations.hpp:33-62): `array` read with `shape` (row-major), the result
+        with the extents reversed."""
+        shape = [int(v) for v in shape]
+        if int(np.prod(shape)) != array.count:
+            raise ValueError("transpose: the shape does not cover the array")
+        out = self.empty(array.count, array.dtype)
+        extents = (ctypes.c_uint64 * len(shape))(*shape)
+        check(lib.sci_cuda_transpose(self.handle, self._precision(array.dtype), array.pointer, len(shape), extents,
+                                     out.pointer), self.handle)
+        return out
+
+    def decompose(self, matrix: "DeviceArray", order: int, plain: bool = False):
+        """decompose (decompose.hpp:77-103): (P, L, U) with A = P L U, each order x order, made on the
+        device."""
+        p, l, u = (self.empty(order * order, matrix.dtype) for _ in range(3))
+        check(lib.sci_cuda_decompose(self.handle, self._precision(matrix.dtype), 1 if plain else 0,
+                                     matrix.pointer, p.pointer, l.pointer, u.pointer, order), self.handle)
+        return p, l, u
+
     # -- chunks ---------------------------------------------------------------------------------
     def execute(self, chunk: C.Chunk, output: int, count: int) -> None:
         check(lib.sci_cuda_execute(self.handle, ctypes.byref(chunk), output, count), self.handle)
