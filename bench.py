@@ -739,8 +739,9 @@ def run_solves(args) -> int:
 
 def run_creation(args) -> int:
     """Arrays made on the device (include/operations/creation.hpp): full, linspace, range and eye of
-    2^28 float32 elements (1 GiB each) and grid of 16384 x 16384 (two 1 GiB outputs), one step = all
-    five. Bound by HBM writes: 4 B/element, 8 for grid. Beside them: the reference's own creation
+    2^28 float32 elements (1 GiB each), grid of 16384 x 16384 (two 1 GiB outputs), and transpose
+    (manipulations.hpp) of a 16384 x 16384 matrix; one step = all six. Bound by HBM: 4 B/element
+    written, 8 for grid and for transpose (read + write). Beside them: the reference's own creation
     functions (libsci's host loops) on a 2^24-element sample."""
     import torch
 
@@ -756,6 +757,7 @@ def run_creation(args) -> int:
     out = device.empty(count)
     second = device.empty(count)
     x, y = device.linspace(-1.0, 1.0, side), device.linspace(0.0, 5.0, side)
+    extents = (ctypes.c_uint64 * 2)(side, side)
     steps = {
         "full": (lambda: check(lib.sci_cuda_fill(device.handle, 0, out.pointer, count, 2.5), device.handle), 4 * count),
         "linspace": (lambda: check(lib.sci_cuda_linspace(device.handle, 0, out.pointer, count, -3.0, 7.0), device.handle),
@@ -765,6 +767,9 @@ def run_creation(args) -> int:
         "eye": (lambda: check(lib.sci_cuda_eye(device.handle, 0, out.pointer, side, side), device.handle), 4 * count),
         "grid": (lambda: check(lib.sci_cuda_grid(device.handle, 0, x.pointer, side, y.pointer, side, out.pointer,
                                                  second.pointer), device.handle), 8 * count),
+        # transpose (manipulations.hpp:33-62) of the 16384 x 16384 grid output: read + write
+        "transpose": (lambda: check(lib.sci_cuda_transpose(device.handle, 0, out.pointer, 2, extents, second.pointer),
+                                    device.handle), 8 * count),
     }
     for _ in range(args.warmup):
         for launch, _bytes in steps.values():
@@ -807,7 +812,7 @@ def run_creation(args) -> int:
     line = {"metric": "device creation GB/s written vs HBM peak", "value": moved / (ms * 1e-3) / 1e9, "unit": "GB/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "full, linspace, range, eye of 2^28 floats; grid 16384 x 16384",
+            "config": {"workload": "full, linspace, range, eye of 2^28 floats; grid and transpose 16384 x 16384",
                        "bytes_written": moved, "l2": "each output 1 GiB, above L2"},
             "kernels": per,
             "roofline": {"bound": "hbm", "achieved": per[top]["GB/s"], "peak": peak, "unit": "GB/s",

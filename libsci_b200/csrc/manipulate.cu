@@ -2,7 +2,7 @@
 // dimensions in reverse order, output[j_{r-1}, ..., j_0] = input[j_0, ..., j_{r-1}], for row-major
 // arrays of rank 1 to 8. The reference copies element by element on the host.
 //
-// Rank 2 goes through 32 x 32 tiles in shared memory (pitch 33), so both the reads and the writes
+// Rank 2 goes through 64 x 64 tiles in shared memory (pitch 65), so both the reads and the writes
 // are coalesced; other ranks map each output element to its input element. A copy either way: the
 // values are the input's bits. Bound by HBM: 2 x element size bytes per element.
 #include "context.hpp"
@@ -22,22 +22,32 @@ namespace sci_cuda {
             int rank;
         };
 
+        // 64 x 64 tiles, 256 threads (32 x 8): each thread loads its 16 elements of the tile before
+        // storing any (16 loads in flight per thread), then writes 16 of the transposed tile.
+        constexpr int kTile = 64;
         template <typename T>
         __global__ void __launch_bounds__(256) transpose_tiles(const T *in, T *out, unsigned long long rows,
                                                                unsigned long long columns) {
-            __shared__ T tile[32][33];
-            const unsigned long long tiles_x = (columns + 31) / 32, tiles = tiles_x * ((rows + 31) / 32);
+            __shared__ T tile[kTile][kTile + 1];
+            const unsigned long long tiles_x = (columns + kTile - 1) / kTile, tiles = tiles_x * ((rows + kTile - 1) / kTile);
             for (unsigned long long t = blockIdx.x; t < tiles; t += gridDim.x) {
-                const unsigned long long r0 = (t / tiles_x) * 32, c0 = (t % tiles_x) * 32;
-                for (int k = threadIdx.y; k < 32; k += 8) {
-                    const unsigned long long r = r0 + k, c = c0 + threadIdx.x;
-                    if (r < rows && c < columns) tile[k][threadIdx.x] = in[r * columns + c];
+                const unsigned long long r0 = (t / tiles_x) * kTile, c0 = (t % tiles_x) * kTile;
+                T staged[16];
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const int k = threadIdx.y + 8 * (q / 2), x = threadIdx.x + 32 * (q % 2);
+                    const unsigned long long r = r0 + k, c = c0 + x;
+                    staged[q] = (r < rows && c < columns) ? in[r * columns + c] : T(0);
                 }
+#pragma unroll
+                for (int q = 0; q < 16; ++q) tile[threadIdx.y + 8 * (q / 2)][threadIdx.x + 32 * (q % 2)] = staged[q];
                 __syncthreads();
                 // out is columns x rows: out[c][r] = in[r][c]
-                for (int k = threadIdx.y; k < 32; k += 8) {
-                    const unsigned long long c = c0 + k, r = r0 + threadIdx.x;
-                    if (c < columns && r < rows) out[c * rows + r] = tile[threadIdx.x][k];
+#pragma unroll
+                for (int q = 0; q < 16; ++q) {
+                    const int k = threadIdx.y + 8 * (q / 2), x = threadIdx.x + 32 * (q % 2);
+                    const unsigned long long c = c0 + k, r = r0 + x;
+                    if (c < columns && r < rows) out[c * rows + r] = tile[x][k];
                 }
                 __syncthreads();
             }
@@ -62,7 +72,7 @@ namespace sci_cuda {
         template <typename T>
         int launch(Context &ctx, const T *in, T *out, const Dims &d, unsigned long long count) {
             if (d.rank == 2) {
-                const unsigned long long tiles = ((d.extent[0] + 31) / 32) * ((d.extent[1] + 31) / 32);
+                const unsigned long long tiles = ((d.extent[0] + kTile - 1) / kTile) * ((d.extent[1] + kTile - 1) / kTile);
                 const unsigned grid = static_cast<unsigned>(tiles < 8ull * ctx.sms ? tiles : 8ull * ctx.sms);
                 transpose_tiles<T><<<grid, dim3(32, 8), 0, ctx.stream>>>(in, out, d.extent[0], d.extent[1]);
             } else {
