@@ -823,10 +823,111 @@ def run_creation(args) -> int:
     return 0
 
 
+def run_elements(args) -> int:
+    """Integer-element chunks (sci_cuda_execute_elements / reduce_elements), the expressions libsci
+    evaluates on the host for non-native element types (include/array/expression.hpp:178-184,
+    203-220): int32 t = a*b + c, maximum(a, c) / b and sum(a*b) over 2^28 elements (1 GiB per
+    array), int8 t = a*b + c over 2^30 and int64 t = a*b + c over 2^27 (1 GiB per array each); one
+    step = all five. HBM-bound: bytes = inputs read + output written per element. Beside them: the
+    reference's own host loop (array::calculate) for int32 a*b + c on a 2^24-element sample."""
+    import torch
+
+    from libsci_b200 import chunk as C
+    from libsci_b200.device import Device
+    from tests import _oracle
+
+    peak, peak_source = measured_peaks()
+    device = Device(0)
+    stream = torch.cuda.ExternalStream(device.stream)
+
+    def operands(dtype, count):
+        # a 2^24-element hashed pattern per operand (no zeros, so b is a divisor), uploaded slice by
+        # slice into 1 GiB device arrays
+        piece = 1 << 24
+        index = np.arange(piece, dtype=np.uint64)
+        made = []
+        for salt in (0x9E3779B97F4A7C15, 0xC2B2AE3D27D4EB4F, 0x165667B19E3779F9):
+            values = ((index * np.uint64(salt)) >> np.uint64(40)).astype(dtype)
+            values[values == 0] = 1
+            array = device.empty(count, dtype)
+            for start in range(0, count, piece):
+                array.offset(start, piece).upload(values)
+            made.append(array)
+        return made
+
+    steps = {}
+    for dtype, count in ((np.int32, 1 << 28), (np.int8, 1 << 30), (np.int64, 1 << 27)):
+        a, b, c = operands(dtype, count)
+        out = device.empty(count, dtype)
+        size = np.dtype(dtype).itemsize
+        x, y, z = a.expression(), b.expression(), c.expression()
+        name = np.dtype(dtype).name
+        fused = C.record_output(x * y + z)
+        steps[f"{name} a*b+c"] = (lambda ch=fused, o=out, n=count, d=dtype: device.execute_elements(d, ch, o.pointer, n),
+                                  4 * size * count)
+        if dtype == np.int32:
+            divided = C.record_output(C.binary("maximum", x, z) / y)
+            steps[f"{name} maximum(a,c)/b"] = (
+                lambda ch=divided, o=out, n=count, d=dtype: device.execute_elements(d, ch, o.pointer, n), 4 * size * count)
+            summed = C.record_reduce(x * y)
+            steps[f"{name} sum(a*b)"] = (lambda ch=summed, n=count, d=dtype: device.reduce_elements(d, ch, C.SUM, n),
+                                         2 * size * count)
+    for _ in range(args.warmup):
+        for launch, _bytes in steps.values():
+            launch()
+    device.synchronize()
+    kernels = {name: [] for name in steps}
+    totals = []
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            marks = [torch.cuda.Event(enable_timing=True) for _ in range(len(steps) + 1)]
+            marks[0].record(stream)
+            for index, (launch, _bytes) in enumerate(steps.values()):
+                launch()
+                marks[index + 1].record(stream)
+            marks[-1].synchronize()
+            for index, name in enumerate(steps):
+                kernels[name].append(marks[index].elapsed_time(marks[index + 1]))
+            totals.append(marks[0].elapsed_time(marks[-1]))
+    ms = statistics.median(totals)
+    moved = sum(b for _launch, b in steps.values())
+    per = {name: {"ms": statistics.median(t), "GB/s": steps[name][1] / (statistics.median(t) * 1e-3) / 1e9,
+                  "frac": steps[name][1] / (statistics.median(t) * 1e-3) / 1e9 / peak} for name, t in kernels.items()}
+    top = max(per, key=lambda name: per[name]["ms"])
+
+    ref = None if args.no_cpu else _oracle.reference()
+    cpu = None
+    if ref is not None:
+        sample = 1 << 24
+        rng = np.random.default_rng(1)
+        host = [rng.integers(-1000, 1000, sample, dtype=np.int32) for _ in range(3)]
+        result = np.empty(sample, np.int32)
+        started = time.perf_counter()
+        ref.sci_ref_elements(0, C.ELEMENT[np.dtype(np.int32)], host[0].ctypes.data, host[1].ctypes.data,
+                             host[2].ctypes.data, sample, result.ctypes.data)
+        seconds = time.perf_counter() - started
+        cpu = {"value": 16 * sample / seconds / 1e9, "unit": "GB/s", "cores": 1, "kind": "reference",
+               "sample": "int32 a*b + c over 2^24 elements through libsci's own assign() host loop "
+                         "(array::calculate, one thread)"}
+    line = {"metric": "integer-element chunk GB/s vs HBM peak", "value": moved / (ms * 1e-3) / 1e9, "unit": "GB/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int8/int32/int64", "data": "synthetic",
+            "config": {"workload": "int32 a*b+c, maximum(a,c)/b, sum(a*b) over 2^28; int8 a*b+c over 2^30; "
+                                   "int64 a*b+c over 2^27", "bytes": moved, "l2": "every array 1 GiB, above L2"},
+            "kernels": per,
+            "roofline": {"bound": "hbm", "achieved": per[top]["GB/s"], "peak": peak, "unit": "GB/s",
+                         "frac": per[top]["frac"], "traffic": None, "kernel": top, "peak_source": peak_source},
+            "cpu_baseline": cpu, "gpu_launches": (len(steps) + 1) * args.steps, "clocks": clocks.summary()}
+    print(json.dumps(line))
+    device.close()
+    return 0
+
+
 def main() -> int:
     parser = argparse.ArgumentParser()
     parser.add_argument("--workload", default="chunks",
-                        choices=["chunks", "product", "solve", "gradient", "batch", "solves", "creation"])
+                        choices=["chunks", "product", "solve", "gradient", "batch", "solves", "creation",
+                                 "elements"])
     parser.add_argument("--size", type=int, default=8192)
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=20)
@@ -853,6 +954,8 @@ def main() -> int:
         return run_gradient(args)
     if args.workload == "batch":
         return run_batch(args)
+    if args.workload == "elements":
+        return run_elements(args)
     if args.workload == "creation":
         return run_creation(args)
     if args.workload == "solves":

@@ -131,6 +131,30 @@ int sci_cuda_reduce(sci_cuda_context *context, const sci_chunk *chunk, uint32_t 
 /* The same reduction, queued: the double result is written to device memory `device_result`. */
 int sci_cuda_reduce_async(sci_cuda_context *context, const sci_chunk *chunk, uint32_t fold, uint64_t count,
                           double *device_result);
+
+/* ---- chunks over other element types ------------------------------------------------------- */
+/* The reference records chunks for float and double only (core::native, traits.hpp:26); any other
+ * element type evaluates its expression tree on the host, element by element, with the scalar
+ * semantics of array::calculate (calculate.hpp:17-93) in assign() (expression.hpp:178-184) and
+ * reduce() (expression.hpp:203-220). These entry points run the same expression, recorded into the
+ * same bytecode (the chunk's precision field is ignored), on the device. FLOAT32 / FLOAT64 go to
+ * sci_cuda_execute / sci_cuda_reduce. Integer arithmetic wraps in the element's width; a zero
+ * divisor gives 0; a real function's NaN converts to 0 and out-of-range values saturate (the cases
+ * C++ leaves undefined). */
+enum {
+    SCI_ELEMENT_FLOAT32 = 0, SCI_ELEMENT_FLOAT64 = 1, /* = SCI_PRECISION_SINGLE / _WIDE */
+    SCI_ELEMENT_INT8 = 2, SCI_ELEMENT_INT16 = 3, SCI_ELEMENT_INT32 = 4, SCI_ELEMENT_INT64 = 5,
+    SCI_ELEMENT_UINT8 = 6, SCI_ELEMENT_UINT16 = 7, SCI_ELEMENT_UINT32 = 8, SCI_ELEMENT_UINT64 = 9
+};
+/* Bytes per element, 0 for an unknown type. */
+uint64_t sci_cuda_element_size(uint32_t element);
+/* assign(target, expression) for an array of `element` (expression.hpp:158-185), queued. */
+int sci_cuda_execute_elements(sci_cuda_context *context, uint32_t element, const sci_chunk *chunk, void *output,
+                              uint64_t count);
+/* reduce(expression, fold) (expression.hpp:191-221): writes one element (its own size) to the host
+ * pointer `result`; an empty reduction is element{} = 0 for every fold (expression.hpp:205). Waits. */
+int sci_cuda_reduce_elements(sci_cuda_context *context, uint32_t element, const sci_chunk *chunk, uint32_t fold,
+                             uint64_t count, void *result);
 /* ---- matrix product ------------------------------------------------------------------------ */
 enum {
     SCI_PRODUCT_BF16 = 0,       /* bf16 operands on tcgen05 tensor cores, FP32 accumulation           */

@@ -46,6 +46,12 @@ BINARY = ["add", "subtract", "multiply", "divide", "minimum", "maximum"]
 SUM, MINIMUM, MAXIMUM = 0, 1, 2  # fold.hpp:11
 SINGLE, WIDE = 0, 1  # precision.hpp:12
 
+# element types of sci_cuda_execute_elements / sci_cuda_reduce_elements (SCI_ELEMENT_*): float and
+# double are libsci's native types (traits.hpp:26); the integer types run the same bytecode with
+# array::calculate's scalar semantics (calculate.hpp:17-93).
+ELEMENT = {np.dtype(t): code for code, t in enumerate(
+    [np.float32, np.float64, np.int8, np.int16, np.int32, np.int64, np.uint8, np.uint16, np.uint32, np.uint64])}
+
 
 class Instruction(ctypes.Structure):
     """core::Instruction (instruction.hpp:28-35)."""

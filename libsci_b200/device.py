@@ -167,6 +167,19 @@ class Device:
         check(lib.sci_cuda_reduce(self.handle, ctypes.byref(chunk), fold, count, ctypes.byref(result)), self.handle)
         return result.value
 
+    def execute_elements(self, dtype, chunk: C.Chunk, output: int, count: int) -> None:
+        """assign() for any element type (expression.hpp:158-185), integers included."""
+        check(lib.sci_cuda_execute_elements(self.handle, C.ELEMENT[np.dtype(dtype)], ctypes.byref(chunk), output, count),
+              self.handle)
+
+    def reduce_elements(self, dtype, chunk: C.Chunk, fold: int, count: int):
+        """reduce() for any element type (expression.hpp:191-221): one element of `dtype`."""
+        dtype = np.dtype(dtype)
+        result = np.zeros(1, dtype)
+        check(lib.sci_cuda_reduce_elements(self.handle, C.ELEMENT[dtype], ctypes.byref(chunk), fold, count,
+                                           result.ctypes.data), self.handle)
+        return result[0]
+
     def reduce_async(self, chunk: C.Chunk, fold: int, count: int, device_result: int) -> None:
         check(lib.sci_cuda_reduce_async(self.handle, ctypes.byref(chunk), fold, count, device_result), self.handle)
 
@@ -214,7 +227,10 @@ class Device:
         chunk = C.record_output(expr)
         if not chunk.valid():
             raise SciCudaError(1, "expression outgrew the 64-entry chunk")
-        self.execute(chunk, out.pointer, expr.count)
+        if expr.dtype.kind in "iu":
+            self.execute_elements(expr.dtype, chunk, out.pointer, expr.count)
+        else:
+            self.execute(chunk, out.pointer, expr.count)
         return out
 
     def reduce(self, expression, fold: int) -> float:
@@ -222,6 +238,8 @@ class Device:
         chunk = C.record_reduce(expr)
         if not chunk.valid():
             raise SciCudaError(1, "expression outgrew the 64-entry chunk")
+        if expr.dtype.kind in "iu":
+            return self.reduce_elements(expr.dtype, chunk, fold, expr.count)
         value = self.reduce_chunk(chunk, fold, expr.count)
         return float(expr.dtype.type(value))  # static_cast<element>(device->reduce(...)) (expression.hpp:198)
 
@@ -472,10 +490,18 @@ def sum(item):  # noqa: A001 - numpy name
 
 
 def mean(item):
-    """reduce.hpp:24-28: sum / count in the element type."""
+    """reduce.hpp:24-28: sum / count in the element type (for integers: the wrapped sum divided by
+    the count converted to the element type, truncating toward zero)."""
     expr = C._operand(item, None)
     if expr.count == 0:
-        return 0.0
+        return expr.dtype.type(0) if expr.dtype.kind in "iu" else 0.0
+    if expr.dtype.kind in "iu":
+        total = int(sum(item))
+        count = int(np.array(expr.count, np.uint64).astype(expr.dtype))  # static_cast<element>(count)
+        if count == 0:
+            raise ZeroDivisionError("the count converts to 0 in the element type")
+        quotient = abs(total) // abs(count) * (1 if (total < 0) == (count < 0) else -1)
+        return np.array(quotient).astype(expr.dtype)[()]
     total = expr.dtype.type(sum(item))
     return float(total / expr.dtype.type(expr.count))
 

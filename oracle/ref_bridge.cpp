@@ -266,4 +266,51 @@ void sci_ref_eye(uint32_t precision, void *out, uint64_t rows, uint64_t columns)
     }
 }
 
+// ---- integer elements: the reference's own host loop (expression.hpp:178-184,203-220) ----------
+// Named expressions over three arrays of one integer element type, written the way a libsci user
+// writes them; the reference evaluates them element by element through array::calculate
+// (calculate.hpp:17-93). Evaluations (which < 10) fill `out` with `count` elements; reductions
+// (which >= 10) write one element. Returns 1 for an unknown name or element type.
+int sci_ref_elements(const int which, const uint32_t element, const void *a, const void *b, const void *c,
+                     const uint64_t count, void *out) {
+    auto run = [&](auto tag) -> int {
+        using T = decltype(tag);
+        sci::Array<T, 1> x(sci::Shape<1>{count}, sci::array::Uninitialized{});
+        sci::Array<T, 1> y(sci::Shape<1>{count}, sci::array::Uninitialized{});
+        sci::Array<T, 1> z(sci::Shape<1>{count}, sci::array::Uninitialized{});
+        sci::Array<T, 1> r(sci::Shape<1>{count}, sci::array::Uninitialized{});
+        std::memcpy(x.data(), a, count * sizeof(T));
+        std::memcpy(y.data(), b, count * sizeof(T));
+        std::memcpy(z.data(), c, count * sizeof(T));
+        T folded{};
+        switch (which) {
+        case 0: r = x * y + z; break;
+        case 1: r = -x + y * T(3); break;
+        case 2: r = sci::absolute(x) - sci::minimum(y, z); break;
+        case 3: r = sci::maximum(x, z) / y; break;
+        case 4: r = sci::root(sci::absolute(x)) + y; break;
+        case 5: r = sci::atan(x) * y + sci::cos(z); break;
+        case 6: r = sci::logarithm(sci::absolute(x) + T(1)) * T(2) - sci::tanh(y); break;
+        case 10: folded = sci::sum(x * y); break;
+        case 11: folded = sci::minimum(x - z); break;
+        case 12: folded = sci::maximum(sci::absolute(y) + x); break;
+        default: return 1;
+        }
+        if (which >= 10) std::memcpy(out, &folded, sizeof(T));
+        else std::memcpy(out, r.data(), count * sizeof(T));
+        return 0;
+    };
+    switch (element) {
+    case SCI_ELEMENT_INT8: return run(int8_t{});
+    case SCI_ELEMENT_INT16: return run(int16_t{});
+    case SCI_ELEMENT_INT32: return run(int32_t{});
+    case SCI_ELEMENT_INT64: return run(int64_t{});
+    case SCI_ELEMENT_UINT8: return run(uint8_t{});
+    case SCI_ELEMENT_UINT16: return run(uint16_t{});
+    case SCI_ELEMENT_UINT32: return run(uint32_t{});
+    case SCI_ELEMENT_UINT64: return run(uint64_t{});
+    default: return 1;
+    }
+}
+
 } // extern "C"

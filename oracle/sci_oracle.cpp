@@ -17,7 +17,12 @@
 //    dispatch.cpp:106-165), as the FP64 oracle the GPU reductions are held to;
 //  - linear::factor / substitute (include/linear/decompose.hpp:29-72, solve.hpp:25-52);
 //  - the element values of the creation functions full / linspace / range / eye / grid
-//    (include/operations/creation.hpp:34-168).
+//    (include/operations/creation.hpp:34-168);
+//  - integer-element expressions, element by element: array::calculate<code, element>
+//    (include/array/calculate.hpp:17-93) as assign() and reduce() run it for non-native element
+//    types (include/array/expression.hpp:178-184,203-220), with the cases C++ leaves undefined
+//    (signed overflow, a zero divisor, MIN / -1, a real result that is NaN or out of range) given
+//    the definitions the CUDA backend documents: wrap, 0, MIN, 0 / saturate.
 // Parity is pinned against the reference itself: tests compare this file's outputs with
 // oracle/_ref/libsci_ref.so (the reference's own CPU path) and with tests/golden fixtures.
 //
@@ -32,6 +37,7 @@
 #include <cstring>
 #include <limits>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 namespace {
@@ -492,6 +498,128 @@ namespace {
         for (uint64_t i = 0; i < rows * columns; ++i) out[i] = T(0);
         for (uint64_t i = 0; i < (rows < columns ? rows : columns); ++i) out[i * columns + i] = T(1);
     }
+    // ---- integer elements (calculate.hpp:17-93, expression.hpp:178-184,203-220) ----------------
+    template <typename T> using IntWord = std::conditional_t<sizeof(T) <= 4, uint32_t, uint64_t>;
+
+    template <typename T> T int_from_real(double x) {
+        constexpr T lo = std::numeric_limits<T>::min(), hi = std::numeric_limits<T>::max();
+        if (std::isnan(x)) return T(0);
+        if (x <= static_cast<double>(lo)) return lo;
+        if (x >= static_cast<double>(hi)) return hi;
+        return static_cast<T>(x);
+    }
+
+    double int_real(int code, double x) {  // calculate.hpp:25-80, in double
+        switch (code) {
+        case SCI_CODE_ROOT: return std::sqrt(x);
+        case SCI_CODE_EXPONENTIAL: return std::exp(x);
+        case SCI_CODE_LOGARITHM: return std::log(x);
+        case SCI_CODE_SIN: return std::sin(x);
+        case SCI_CODE_COS: return std::cos(x);
+        case SCI_CODE_TAN: return std::tan(x);
+        case SCI_CODE_ASIN: return std::asin(x);
+        case SCI_CODE_ACOS: return std::acos(x);
+        case SCI_CODE_ATAN: return std::atan(x);
+        case SCI_CODE_CSC: return 1.0 / std::sin(x);
+        case SCI_CODE_SEC: return 1.0 / std::cos(x);
+        case SCI_CODE_COT: return 1.0 / std::tan(x);
+        case SCI_CODE_ACSC: return std::asin(1.0 / x);
+        case SCI_CODE_ASEC: return std::acos(1.0 / x);
+        case SCI_CODE_ACOT: return std::atan(1.0 / x);
+        case SCI_CODE_SINH: return std::sinh(x);
+        case SCI_CODE_COSH: return std::cosh(x);
+        case SCI_CODE_TANH: return std::tanh(x);
+        case SCI_CODE_ASINH: return std::asinh(x);
+        case SCI_CODE_ACOSH: return std::acosh(x);
+        case SCI_CODE_ATANH: return std::atanh(x);
+        case SCI_CODE_CSCH: return 1.0 / std::sinh(x);
+        case SCI_CODE_SECH: return 1.0 / std::cosh(x);
+        case SCI_CODE_COTH: return 1.0 / std::tanh(x);
+        case SCI_CODE_ACSCH: return std::asinh(1.0 / x);
+        case SCI_CODE_ASECH: return std::acosh(1.0 / x);
+        default: return std::atanh(1.0 / x);
+        }
+    }
+
+    template <typename T> T int_apply(int code, T a, T b, T c) {
+        using W = IntWord<T>;
+        switch (code) {
+        case SCI_CODE_COPY: return a;
+        case SCI_CODE_NEGATE: return T(W(0) - W(a));
+        case SCI_CODE_ABSOLUTE:
+            if constexpr (std::is_signed_v<T>) return a < T(0) ? T(W(0) - W(a)) : a;
+            else return a;
+        case SCI_CODE_ADD: return T(W(a) + W(b));
+        case SCI_CODE_SUBTRACT: return T(W(a) - W(b));
+        case SCI_CODE_MULTIPLY: return T(W(a) * W(b));
+        case SCI_CODE_DIVIDE:
+            if (b == T(0)) return T(0);
+            if constexpr (std::is_signed_v<T>) {
+                if (b == T(-1)) return T(W(0) - W(a));
+            }
+            return T(a / b);
+        case SCI_CODE_MINIMUM: return b < a ? b : a;
+        case SCI_CODE_MAXIMUM: return b > a ? b : a;
+        case SCI_CODE_FUSE: return T(W(a) * W(b) + W(c));
+        default: return int_from_real<T>(int_real(code, static_cast<double>(a)));
+        }
+    }
+
+    // One element through the chunk: value ids as in instruction.hpp:12-25.
+    template <typename T> T int_element(const sci_chunk &chunk, uint64_t i, T *temporaries, T &out, unsigned wanted) {
+        auto value = [&](unsigned id) -> T {
+            const unsigned kind = id & SCI_SLOT_TYPES, slot = id & 63;
+            if (id == SCI_SLOT_NONE) return T(0);
+            if (kind == SCI_SLOT_INPUT) return static_cast<const T *>(chunk.inputs[slot])[i];
+            if (kind == SCI_SLOT_LITERAL) return static_cast<T>(chunk.constants[slot]);
+            if (kind == SCI_SLOT_TEMPORARY) return temporaries[slot];
+            return out;
+        };
+        for (int k = 0; k < chunk.length; ++k) {
+            const sci_instruction &ins = chunk.instructions[k];
+            const T r = int_apply<T>(ins.code, value(ins.sources[0]), value(ins.sources[1]), value(ins.sources[2]));
+            if (ins.target == SCI_SLOT_OUTPUT) out = r;
+            else temporaries[ins.target & 63] = r;
+        }
+        return value(wanted);
+    }
+
+    template <typename T> void int_execute(const sci_chunk &chunk, T *output, uint64_t count) {
+        T temporaries[SCI_CHUNK_CAPACITY] = {};
+        for (uint64_t i = 0; i < count; ++i) {
+            T out{};
+            output[i] = int_element<T>(chunk, i, temporaries, out, SCI_SLOT_OUTPUT);
+        }
+    }
+
+    template <typename T> T int_reduce(const sci_chunk &chunk, int fold, uint64_t count) {
+        if (count == 0) return T{};
+        T temporaries[SCI_CHUNK_CAPACITY] = {};
+        T out{};
+        T result = int_element<T>(chunk, 0, temporaries, out, chunk.result);
+        for (uint64_t i = 1; i < count; ++i) {
+            const T v = int_element<T>(chunk, i, temporaries, out, chunk.result);
+            if (fold == SCI_FOLD_SUM) result = T(IntWord<T>(result) + IntWord<T>(v));
+            else if (fold == SCI_FOLD_MINIMUM) result = v < result ? v : result;
+            else result = v > result ? v : result;
+        }
+        return result;
+    }
+
+    template <typename F> int by_int_element(uint32_t element, F &&f) {
+        switch (element) {
+        case SCI_ELEMENT_INT8: return f(int8_t{});
+        case SCI_ELEMENT_INT16: return f(int16_t{});
+        case SCI_ELEMENT_INT32: return f(int32_t{});
+        case SCI_ELEMENT_INT64: return f(int64_t{});
+        case SCI_ELEMENT_UINT8: return f(uint8_t{});
+        case SCI_ELEMENT_UINT16: return f(uint16_t{});
+        case SCI_ELEMENT_UINT32: return f(uint32_t{});
+        case SCI_ELEMENT_UINT64: return f(uint64_t{});
+        default: return SCI_CUDA_ERROR_INVALID;
+        }
+    }
+
     template <typename T> void grid_values(const T *x, uint64_t nx, const T *y, uint64_t ny, T *xx, T *yy) {  // :120-140
         for (uint64_t i = 0; i < ny; ++i)
             for (uint64_t j = 0; j < nx; ++j) {
@@ -579,6 +707,27 @@ void sci_oracle_grid(uint32_t precision, const void *x, uint64_t nx, const void 
     else
         grid_values(static_cast<const float *>(x), nx, static_cast<const float *>(y), ny, static_cast<float *>(xx),
                     static_cast<float *>(yy));
+}
+
+// Integer-element expressions (calculate.hpp, expression.hpp:178-184,203-220); element is a
+// SCI_ELEMENT_INT* / UINT* code. reduce writes one element to `result`.
+int sci_oracle_execute_elements(uint32_t element, const sci_chunk *chunk, void *output, uint64_t count) {
+    if (!chunk || !valid(*chunk)) return SCI_CUDA_ERROR_INVALID;
+    return by_int_element(element, [&](auto tag) {
+        using T = decltype(tag);
+        int_execute<T>(*chunk, static_cast<T *>(output), count);
+        return 0;
+    });
+}
+
+int sci_oracle_reduce_elements(uint32_t element, const sci_chunk *chunk, uint32_t fold, uint64_t count, void *result) {
+    if (!chunk || !valid(*chunk) || fold > SCI_FOLD_MAXIMUM || !result) return SCI_CUDA_ERROR_INVALID;
+    return by_int_element(element, [&](auto tag) {
+        using T = decltype(tag);
+        const T value = int_reduce<T>(*chunk, int(fold), count);
+        std::memcpy(result, &value, sizeof(T));
+        return 0;
+    });
 }
 
 } // extern "C"

@@ -39,6 +39,9 @@ def port() -> ctypes.CDLL:
     lib.sci_oracle_substitute_f64.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_uint64, ctypes.c_uint64]
     lib.sci_oracle_product_rows.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_uint64] * 5
     lib.sci_oracle_tail_width.restype = ctypes.c_uint64
+    lib.sci_oracle_execute_elements.argtypes = [ctypes.c_uint32, P(ChunkStruct), ctypes.c_void_p, ctypes.c_uint64]
+    lib.sci_oracle_reduce_elements.argtypes = [ctypes.c_uint32, P(ChunkStruct), ctypes.c_uint32, ctypes.c_uint64,
+                                               ctypes.c_void_p]
     _cache["port"] = lib
     return lib
 
@@ -67,6 +70,8 @@ def reference() -> ctypes.CDLL | None:
     lib.sci_ref_workload_output.restype = ctypes.c_void_p
     lib.sci_ref_workload_output.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.sci_ref_workload_destroy.argtypes = [ctypes.c_void_p]
+    lib.sci_ref_elements.argtypes = [ctypes.c_int, ctypes.c_uint32] + [ctypes.c_void_p] * 3 + [ctypes.c_uint64,
+                                                                                            ctypes.c_void_p]
     _cache["ref"] = lib
     return lib
 
