@@ -923,11 +923,119 @@ def run_elements(args) -> int:
     return 0
 
 
+def run_shapes(args) -> int:
+    """Broadcasting, the roadmap's elementwise functions and axis reductions (libsci's README.md:
+    149-152, numpy's rules): over 16384 x 16384 float32 (1 GiB per full array), one step =
+    (16384,1) + (1,16384); where((16384,1), x, y); clip(x, -1, 1); power(x, 2.5); floor(x); sum of
+    x over axis 0 and over axis 1. HBM-bound: bytes = full operands read + output written (a
+    broadcast operand is 64 KiB). Beside them: numpy on the host (one thread) on a 2048 x 16384
+    sample of the same steps."""
+    import torch
+
+    from libsci_b200 import chunk as C
+    from libsci_b200.device import Device
+    from libsci_b200.native import check, lib
+
+    side = 1 << 14
+    count = side * side
+    peak, peak_source = measured_peaks()
+    device = Device(0)
+    stream = torch.cuda.ExternalStream(device.stream)
+    full = (side, side)
+    x = device.range(-2.0, -2.0 + count * (4.0 / count), 4.0 / count)
+    y = device.full(count, 0.5)
+    column = device.linspace(-1.0, 1.0, side)
+    row = device.linspace(0.0, 3.0, side)
+    out = device.empty(count)
+    reduced = device.empty(side)
+    scalars = {v: device.full(1, v) for v in (-1.0, 1.0, 2.5)}
+
+    def apply(code, operands):
+        # straight through the C ABI into a preallocated output: nothing allocates in the timed region
+        number = C.EXTRA[code] if code in C.EXTRA else C.CODE[code]
+        inputs = (ctypes.c_void_p * len(operands))(*[array.pointer for array, _ in operands])
+        extents = (ctypes.c_uint64 * (2 * len(operands)))(*[e for _, shape in operands for e in shape])
+        check(lib.sci_cuda_broadcast(device.handle, 0, number, 2, (ctypes.c_uint64 * 2)(*full), len(operands), inputs,
+                                     extents, out.pointer), device.handle)
+
+    def axis_sum(axis):
+        check(lib.sci_cuda_reduce_axis(device.handle, 0, C.SUM, x.pointer, 2, (ctypes.c_uint64 * 2)(*full), axis,
+                                       reduced.pointer), device.handle)
+
+    one = (1, 1)
+    steps = {
+        "broadcast add (16384,1)+(1,16384)": (lambda: apply("add", [(column, (side, 1)), (row, (1, side))]), 4 * count),
+        "where((16384,1), x, y)": (lambda: apply("where", [(column, (side, 1)), (x, full), (y, full)]), 12 * count),
+        "clip(x, -1, 1)": (lambda: apply("clip", [(x, full), (scalars[-1.0], one), (scalars[1.0], one)]), 8 * count),
+        "power(x, 2.5)": (lambda: apply("power", [(x, full), (scalars[2.5], one)]), 8 * count),
+        "floor(x)": (lambda: apply("floor", [(x, full)]), 8 * count),
+        "sum(x, axis=0)": (lambda: axis_sum(0), 4 * count),
+        "sum(x, axis=1)": (lambda: axis_sum(1), 4 * count),
+    }
+
+    for _ in range(args.warmup):
+        for launch, _bytes in steps.values():
+            launch()
+    device.synchronize()
+    kernels = {name: [] for name in steps}
+    totals = []
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            marks = [torch.cuda.Event(enable_timing=True) for _ in range(len(steps) + 1)]
+            marks[0].record(stream)
+            for index, (launch, _bytes) in enumerate(steps.values()):
+                launch()
+                marks[index + 1].record(stream)
+            marks[-1].synchronize()
+            for index, name in enumerate(steps):
+                kernels[name].append(marks[index].elapsed_time(marks[index + 1]))
+            totals.append(marks[0].elapsed_time(marks[-1]))
+    ms = statistics.median(totals)
+    moved = sum(b for _launch, b in steps.values())
+    per = {name: {"ms": statistics.median(t), "GB/s": steps[name][1] / (statistics.median(t) * 1e-3) / 1e9,
+                  "frac": steps[name][1] / (statistics.median(t) * 1e-3) / 1e9 / peak} for name, t in kernels.items()}
+    top = max(per, key=lambda name: per[name]["ms"])
+
+    cpu = None
+    if not args.no_cpu:
+        rows = 2048
+        hx = np.linspace(-2.0, 2.0, rows * side, dtype=np.float32).reshape(rows, side)
+        hy = np.full((rows, side), 0.5, np.float32)
+        hc = np.linspace(-1.0, 1.0, rows, dtype=np.float32).reshape(rows, 1)
+        hr = np.linspace(0.0, 3.0, side, dtype=np.float32).reshape(1, side)
+        started = time.perf_counter()
+        with np.errstate(all="ignore"):
+            _ = hc + hr
+            _ = np.where(hc != 0, hx, hy)
+            _ = np.clip(hx, np.float32(-1), np.float32(1))
+            _ = np.power(hx, np.float32(2.5))
+            _ = np.floor(hx)
+            _ = hx.sum(axis=0, dtype=np.float64)
+            _ = hx.sum(axis=1, dtype=np.float64)
+        seconds = time.perf_counter() - started
+        cpu = {"value": moved * rows / side / seconds / 1e9, "unit": "GB/s", "cores": 1, "kind": "port",
+               "sample": "the seven steps over 2048 x 16384 floats in numpy on the host (the rules these "
+                         "follow; libsci has no implementation of them)"}
+    line = {"metric": "broadcast / roadmap elementwise / axis-reduction GB/s vs HBM peak",
+            "value": moved / (ms * 1e-3) / 1e9, "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "16384 x 16384 float32: broadcast add, where, clip, power, floor, sum over "
+                                   "axis 0 and axis 1", "bytes": moved, "l2": "every full array 1 GiB, above L2"},
+            "kernels": per,
+            "roofline": {"bound": "hbm", "achieved": per[top]["GB/s"], "peak": peak, "unit": "GB/s",
+                         "frac": per[top]["frac"], "traffic": None, "kernel": top, "peak_source": peak_source},
+            "cpu_baseline": cpu, "gpu_launches": 8 * args.steps, "clocks": clocks.summary()}
+    print(json.dumps(line))
+    device.close()
+    return 0
+
+
 def main() -> int:
     parser = argparse.ArgumentParser()
     parser.add_argument("--workload", default="chunks",
                         choices=["chunks", "product", "solve", "gradient", "batch", "solves", "creation",
-                                 "elements"])
+                                 "elements", "shapes"])
     parser.add_argument("--size", type=int, default=8192)
     parser.add_argument("--gpus", type=int, default=1)
     parser.add_argument("--steps", type=int, default=20)
@@ -956,6 +1064,8 @@ def main() -> int:
         return run_batch(args)
     if args.workload == "elements":
         return run_elements(args)
+    if args.workload == "shapes":
+        return run_shapes(args)
     if args.workload == "creation":
         return run_creation(args)
     if args.workload == "solves":

@@ -132,6 +132,31 @@ int sci_cuda_reduce(sci_cuda_context *context, const sci_chunk *chunk, uint32_t 
 int sci_cuda_reduce_async(sci_cuda_context *context, const sci_chunk *chunk, uint32_t fold, uint64_t count,
                           double *device_result);
 
+/* ---- shapes: broadcasting, the roadmap's elementwise functions, axis reductions ------------- */
+/* libsci lists these as next (README.md:149-152) and has no implementation yet; the rules are
+ * numpy's, which its operations are named after (reduce.hpp:8-9). */
+enum { /* codes beyond core::Code, for sci_cuda_broadcast only */
+    SCI_EXTRA_FLOOR = 64, SCI_EXTRA_CEIL = 65, SCI_EXTRA_ROUND = 66, /* round: halves to even (numpy.round) */
+    SCI_EXTRA_POWER = 67,                                            /* C pow; float raised in double */
+    SCI_EXTRA_CLIP = 68,                                             /* minimum(maximum(x, lo), hi) */
+    SCI_EXTRA_WHERE = 69                                             /* condition != 0 ? x : y */
+};
+/* output = code(operands...) over the output `shape` (rank 1 to 8). Every operand has `rank`
+ * extents in input_shapes[k * rank + axis], each equal to the output's or 1 (broadcast: the caller
+ * prepends 1s, as numpy aligns shapes on the right). Codes: SCI_CODE_COPY (broadcast_to), ADD,
+ * SUBTRACT, MULTIPLY, DIVIDE, MINIMUM, MAXIMUM (NaN propagates, numpy.minimum / maximum) and the
+ * SCI_EXTRA codes; 1, 2 or 3 operands by code. Queued. */
+int sci_cuda_broadcast(sci_cuda_context *context, uint32_t precision, uint32_t code, uint32_t rank,
+                       const uint64_t *shape, uint32_t operands, const void *const *inputs,
+                       const uint64_t *input_shapes, void *output);
+enum { SCI_AXIS_MEAN = 3 }; /* beside SCI_FOLD_SUM / MINIMUM / MAXIMUM */
+/* sum(a, axis) and the rest: folds `input` (row-major, `shape`, rank 1 to 8) over `axis` into
+ * `output` (the shape without that axis). Folds in double, NaN propagates, one cast to the element
+ * type; mean = sum / count in the element type (reduce.hpp:24-28); an empty axis gives 0 for sum
+ * and mean, NaN for minimum and maximum. Queued. */
+int sci_cuda_reduce_axis(sci_cuda_context *context, uint32_t precision, uint32_t fold, const void *input,
+                         uint32_t rank, const uint64_t *shape, uint32_t axis, void *output);
+
 /* ---- chunks over other element types ------------------------------------------------------- */
 /* The reference records chunks for float and double only (core::native, traits.hpp:26); any other
  * element type evaluates its expression tree on the host, element by element, with the scalar

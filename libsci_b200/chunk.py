@@ -46,6 +46,11 @@ BINARY = ["add", "subtract", "multiply", "divide", "minimum", "maximum"]
 SUM, MINIMUM, MAXIMUM = 0, 1, 2  # fold.hpp:11
 SINGLE, WIDE = 0, 1  # precision.hpp:12
 
+# codes beyond core::Code for sci_cuda_broadcast (libsci's roadmap functions, README.md:149-152),
+# and the mean fold of sci_cuda_reduce_axis
+EXTRA = {"floor": 64, "ceil": 65, "round": 66, "power": 67, "clip": 68, "where": 69}
+AXIS_MEAN = 3
+
 # element types of sci_cuda_execute_elements / sci_cuda_reduce_elements (SCI_ELEMENT_*): float and
 # double are libsci's native types (traits.hpp:26); the integer types run the same bytecode with
 # array::calculate's scalar semantics (calculate.hpp:17-93).

@@ -158,6 +158,45 @@ class Device:
                                      matrix.pointer, p.pointer, l.pointer, u.pointer, order), self.handle)
         return p, l, u
 
+    # -- shapes: broadcasting, the roadmap's elementwise functions, axis reductions --------------
+    def broadcast(self, code, operands, shape=()):
+        """code(operands...) with numpy broadcasting (libsci's roadmap, README.md:149-152).
+
+        `code` is a name ("add", "minimum", "power", "clip", "where", "copy", ...) and `operands`
+        a list of (DeviceArray, shape) pairs of one element type; shapes align on the right as in
+        numpy, and the result has their broadcast shape (with `shape` broadcast in too).
+        Returns (DeviceArray, shape)."""
+        number = C.EXTRA[code] if code in C.EXTRA else C.CODE[code]
+        dtype = operands[0][0].dtype
+        shapes = [tuple(int(e) for e in shape) for _, shape in operands]
+        for (array, _), own in zip(operands, shapes):
+            if array.dtype != dtype or array.count != int(np.prod(own, dtype=np.int64)):
+                raise ValueError(f"operand of {array.count} {array.dtype} elements does not have shape {own}")
+        shape = tuple(int(e) for e in np.broadcast_shapes(*shapes, tuple(shape)))
+        rank = max(len(shape), 1)
+        aligned = [(1,) * (rank - len(s)) + s for s in shapes]
+        out = self.empty(int(np.prod(shape, dtype=np.int64)), dtype)
+        inputs = (ctypes.c_void_p * len(operands))(*[array.pointer for array, _ in operands])
+        extents = (ctypes.c_uint64 * (len(operands) * rank))(*[e for s in aligned for e in s])
+        out_extents = (ctypes.c_uint64 * rank)(*(shape or (1,)))
+        check(lib.sci_cuda_broadcast(self.handle, self._precision(dtype), number, rank, out_extents, len(operands),
+                                     inputs, extents, out.pointer), self.handle)
+        return out, shape
+
+    def reduce_axis(self, array: "DeviceArray", shape, axis: int, fold: int):
+        """sum / minimum / maximum / mean (C.AXIS_MEAN) of a row-major array along `axis`
+        (negative counts from the end). Returns (DeviceArray, shape without that axis)."""
+        shape = tuple(int(e) for e in shape)
+        axis = axis + len(shape) if axis < 0 else axis
+        if not 0 <= axis < len(shape):
+            raise ValueError(f"axis {axis} of a rank-{len(shape)} array")
+        kept = shape[:axis] + shape[axis + 1:]
+        out = self.empty(int(np.prod(kept, dtype=np.int64)), array.dtype)
+        extents = (ctypes.c_uint64 * len(shape))(*shape)
+        check(lib.sci_cuda_reduce_axis(self.handle, self._precision(array.dtype), fold, array.pointer, len(shape), extents,
+                                       axis, out.pointer), self.handle)
+        return out, kept
+
     # -- chunks ---------------------------------------------------------------------------------
     def execute(self, chunk: C.Chunk, output: int, count: int) -> None:
         check(lib.sci_cuda_execute(self.handle, ctypes.byref(chunk), output, count), self.handle)
@@ -511,6 +550,79 @@ def dot(first, second):
     return _device_of(first).reduce(C.binary("multiply", first, second), C.SUM)
 
 
+def _shaped(item, device=None, dtype=None):
+    """(DeviceArray, shape) from a pair, a DeviceArray (one axis) or a scalar (shape ())."""
+    if isinstance(item, tuple) and len(item) == 2 and isinstance(item[0], DeviceArray):
+        return item
+    if isinstance(item, DeviceArray):
+        return item, (item.count,)
+    return device.full(1, float(item), dtype), ()
+
+
+def _broadcast(code, *items):
+    anchor = next(i for i in items if isinstance(i, DeviceArray) or isinstance(i, tuple))
+    array = anchor[0] if isinstance(anchor, tuple) else anchor
+    operands = [_shaped(item, array.device, array.dtype) for item in items]
+    return array.device.broadcast(code, operands)
+
+
+def power(x, y):
+    """numpy.power with broadcasting; returns (DeviceArray, shape)."""
+    return _broadcast("power", x, y)
+
+
+def floor(x):
+    return _broadcast("floor", x)
+
+
+def ceil(x):
+    return _broadcast("ceil", x)
+
+
+def round(x):  # noqa: A001 - numpy name
+    """numpy.round: halves to even."""
+    return _broadcast("round", x)
+
+
+def clip(x, lower, upper):
+    """numpy.clip: minimum(maximum(x, lower), upper); bounds may be arrays or scalars."""
+    return _broadcast("clip", x, lower, upper)
+
+
+def where(condition, x, y):
+    """numpy.where(condition != 0, x, y) with broadcasting."""
+    return _broadcast("where", condition, x, y)
+
+
+def broadcast_to(x, shape):
+    """numpy.broadcast_to, materialised (a copy): (DeviceArray, shape)."""
+    array, own = _shaped(x)
+    shape = tuple(int(e) for e in shape)
+    if np.broadcast_shapes(tuple(own), shape) != shape:
+        raise ValueError(f"cannot broadcast {tuple(own)} to {shape}")
+    return array.device.broadcast("copy", [(array, own)], shape)
+
+
+def sum_axis(x, axis):
+    array, shape = _shaped(x)
+    return array.device.reduce_axis(array, shape, axis, C.SUM)
+
+
+def mean_axis(x, axis):
+    array, shape = _shaped(x)
+    return array.device.reduce_axis(array, shape, axis, C.AXIS_MEAN)
+
+
+def minimum_axis(x, axis):
+    array, shape = _shaped(x)
+    return array.device.reduce_axis(array, shape, axis, C.MINIMUM)
+
+
+def maximum_axis(x, axis):
+    array, shape = _shaped(x)
+    return array.device.reduce_axis(array, shape, axis, C.MAXIMUM)
+
+
 def _device_of(item) -> Device:
     if isinstance(item, DeviceArray):
         return item.device
@@ -522,4 +634,5 @@ def _device_of(item) -> Device:
 
 
 __all__ = ["Device", "DeviceArray", "minimum", "maximum", "add", "subtract", "multiply", "divide", "sum", "mean",
-           "dot", "negate"] + list(C.UNARY)
+           "dot", "negate", "power", "floor", "ceil", "round", "clip", "where", "broadcast_to", "sum_axis",
+           "mean_axis", "minimum_axis", "maximum_axis"] + list(C.UNARY)

@@ -97,6 +97,8 @@ def _load() -> ctypes.CDLL:
     sig["sci_cuda_grid"] = (ctypes.c_int, [c_ctx, U32, VP, U64, VP, U64, VP, VP])
     sig["sci_cuda_decompose"] = (ctypes.c_int, [c_ctx, U32, U32, VP, VP, VP, VP, U64])
     sig["sci_cuda_transpose"] = (ctypes.c_int, [c_ctx, U32, VP, U32, P(U64), VP])
+    sig["sci_cuda_broadcast"] = (ctypes.c_int, [c_ctx, U32, U32, U32, P(U64), U32, P(VP), P(U64), VP])
+    sig["sci_cuda_reduce_axis"] = (ctypes.c_int, [c_ctx, U32, U32, VP, U32, P(U64), U32, VP])
     sig["sci_cuda_element_size"] = (U64, [U32])
     sig["sci_cuda_execute_elements"] = (ctypes.c_int, [c_ctx, U32, P(ChunkStruct), VP, U64])
     sig["sci_cuda_reduce_elements"] = (ctypes.c_int, [c_ctx, U32, P(ChunkStruct), U32, U64, VP])
