@@ -57,6 +57,16 @@ def generate(count: int, seed: int = 0):
     return x, y, z
 
 
+def measured_traffic(section: str, step: str, elements: int):
+    """DRAM bytes of one launch of `step` from the committed ncu figures (profiles/traffic.json,
+    bytes per element of one capture, scaled to `elements`), or None."""
+    path = ROOT / "profiles" / "traffic.json"
+    if not path.exists():
+        return None
+    entry = json.loads(path.read_text()).get(section, {}).get(step)
+    return entry["bytes_per_element"] * elements if entry else None
+
+
 def measured_peaks():
     path = ROOT / "MEASURED_PEAKS.json"
     if path.exists():
@@ -856,13 +866,15 @@ def run_elements(args) -> int:
         return made
 
     steps = {}
-    for dtype, count in ((np.int32, 1 << 28), (np.int8, 1 << 30), (np.int64, 1 << 27)):
+    shrink = 2 if args.small else 0  # --small: a quarter of each size, for profiler captures
+    for dtype, count in ((np.int32, 1 << (28 - shrink)), (np.int8, 1 << (30 - shrink)), (np.int64, 1 << (27 - shrink))):
         a, b, c = operands(dtype, count)
         out = device.empty(count, dtype)
         size = np.dtype(dtype).itemsize
         x, y, z = a.expression(), b.expression(), c.expression()
         name = np.dtype(dtype).name
         fused = C.record_output(x * y + z)
+        counts.update({f"{name} a*b+c": count, f"{name} maximum(a,c)/b": count, f"{name} sum(a*b)": count})
         steps[f"{name} a*b+c"] = (lambda ch=fused, o=out, n=count, d=dtype: device.execute_elements(d, ch, o.pointer, n),
                                   4 * size * count)
         if dtype == np.int32:
@@ -894,6 +906,7 @@ def run_elements(args) -> int:
     per = {name: {"ms": statistics.median(t), "GB/s": steps[name][1] / (statistics.median(t) * 1e-3) / 1e9,
                   "frac": steps[name][1] / (statistics.median(t) * 1e-3) / 1e9 / peak} for name, t in kernels.items()}
     top = max(per, key=lambda name: per[name]["ms"])
+    top_elements = {name: n for name, n in counts.items()}[top]
 
     ref = None if args.no_cpu else _oracle.reference()
     cpu = None
@@ -912,11 +925,13 @@ def run_elements(args) -> int:
     line = {"metric": "integer-element chunk GB/s vs HBM peak", "value": moved / (ms * 1e-3) / 1e9, "unit": "GB/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int8/int32/int64", "data": "synthetic",
-            "config": {"workload": "int32 a*b+c, maximum(a,c)/b, sum(a*b) over 2^28; int8 a*b+c over 2^30; "
-                                   "int64 a*b+c over 2^27", "bytes": moved, "l2": "every array 1 GiB, above L2"},
+            "config": {"workload": f"int32 a*b+c, maximum(a,c)/b, sum(a*b) over 2^{28 - shrink}; int8 a*b+c over "
+                                   f"2^{30 - shrink}; int64 a*b+c over 2^{27 - shrink}", "bytes": moved,
+                       "l2": "every array above L2"},
             "kernels": per,
             "roofline": {"bound": "hbm", "achieved": per[top]["GB/s"], "peak": peak, "unit": "GB/s",
-                         "frac": per[top]["frac"], "traffic": None, "kernel": top, "peak_source": peak_source},
+                         "frac": per[top]["frac"], "traffic": measured_traffic("elements", top, top_elements),
+                         "kernel": f"element_stream ({top})", "peak_source": peak_source},
             "cpu_baseline": cpu, "gpu_launches": (len(steps) + 1) * args.steps, "clocks": clocks.summary()}
     print(json.dumps(line))
     device.close()
@@ -936,7 +951,7 @@ def run_shapes(args) -> int:
     from libsci_b200.device import Device
     from libsci_b200.native import check, lib
 
-    side = 1 << 14
+    side = 1 << (13 if args.small else 14)
     count = side * side
     peak, peak_source = measured_peaks()
     device = Device(0)
@@ -994,7 +1009,9 @@ def run_shapes(args) -> int:
     moved = sum(b for _launch, b in steps.values())
     per = {name: {"ms": statistics.median(t), "GB/s": steps[name][1] / (statistics.median(t) * 1e-3) / 1e9,
                   "frac": steps[name][1] / (statistics.median(t) * 1e-3) / 1e9 / peak} for name, t in kernels.items()}
-    top = max(per, key=lambda name: per[name]["ms"])
+    # power spends its time in the FP64 pipe (a double pow per element): the roofline names the
+    # slowest HBM-bound step, power is reported beside it
+    top = max((name for name in per if not name.startswith("power")), key=lambda name: per[name]["ms"])
 
     cpu = None
     if not args.no_cpu:
@@ -1020,11 +1037,14 @@ def run_shapes(args) -> int:
             "value": moved / (ms * 1e-3) / 1e9, "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "16384 x 16384 float32: broadcast add, where, clip, power, floor, sum over "
-                                   "axis 0 and axis 1", "bytes": moved, "l2": "every full array 1 GiB, above L2"},
+            "config": {"workload": f"{side} x {side} float32: broadcast add, where, clip, power, floor, sum over "
+                                   "axis 0 and axis 1", "bytes": moved, "l2": "every full array above L2"},
             "kernels": per,
             "roofline": {"bound": "hbm", "achieved": per[top]["GB/s"], "peak": peak, "unit": "GB/s",
-                         "frac": per[top]["frac"], "traffic": None, "kernel": top, "peak_source": peak_source},
+                         "frac": per[top]["frac"], "traffic": measured_traffic("shapes", top, count), "kernel": top,
+                         "peak_source": peak_source},
+            "fp64_bound": {"step": "power(x, 2.5)", "ms": per["power(x, 2.5)"]["ms"],
+                           "note": "a double-precision pow per element; bound by the FP64 pipe, not HBM"},
             "cpu_baseline": cpu, "gpu_launches": 8 * args.steps, "clocks": clocks.summary()}
     print(json.dumps(line))
     device.close()
@@ -1044,6 +1064,8 @@ def main() -> int:
     parser.add_argument("--elements", type=int, default=1 << 28)
     parser.add_argument("--e2e-steps", type=int, default=3)
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    parser.add_argument("--small", action="store_true",
+                        help="elements / shapes workloads at a quarter size (for profiler captures)")
     parser.add_argument("--items", type=int, default=8192, help="batch workload: instances")
     parser.add_argument("--gradient-elements", type=int, default=1 << 26, help="gradient workload: elements per array")
     args = parser.parse_args()

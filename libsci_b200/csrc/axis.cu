@@ -145,8 +145,12 @@ namespace sci_cuda {
         }
 
         template <typename T> int launch_axis(Context &ctx, const T *in, T *out, AxisShape s) {
-            const unsigned long long target = 148ull * 64 * 32;  // threads wanted in flight
-            const unsigned long long most = 16ull * ctx.sms;    // blocks of 256
+            // Work units for four resident waves of threads, run by one persistent wave, so the last
+            // units do not leave most of the GPU idle.
+            const void *kernel = s.inner == 1 && s.extent >= 64 ? reinterpret_cast<const void *>(&axis_rows<T>)
+                                                                : reinterpret_cast<const void *>(&axis_column_vectors<T>);
+            const unsigned long long most = 1ull * ctx.sms * ctx.blocks_per_sm(kernel, 256, 0);  // blocks of 256
+            const unsigned long long target = 4 * most * 256;                                     // threads' worth of units
             // short rows go a thread per row (the column form with inner = 1)
             const bool rows = s.inner == 1 && s.extent >= 64;
             constexpr unsigned long long V = 16 / sizeof(T);

@@ -35,6 +35,7 @@ namespace sci_cuda {
 
         constexpr int kMaxAxes = 8;
         constexpr unsigned kPiece = 1024;
+        constexpr int kVectorsPerThread = 2;  // 16-byte vectors per thread per piece (vector form)
 
         template <typename T> struct ApplyLaunch {
             int code;
@@ -126,7 +127,7 @@ namespace sci_cuda {
         // broadcast along the last axis is one value per row. The code is a template argument.
         template <typename T, int CODE>
         __global__ void __launch_bounds__(256) apply_vectors(const __grid_constant__ ApplyLaunch<T> L) {
-            constexpr int V = 16 / sizeof(T), U = 2;
+            constexpr int V = 16 / sizeof(T), U = kVectorsPerThread;
             const int last = L.rank - 1;
             const unsigned long long columns = L.extent[last];
             const unsigned long long span = 1ull * blockDim.x * V * U;
@@ -172,7 +173,7 @@ namespace sci_cuda {
 
         template <typename T, int CODE> void launch_vectors(Context &ctx, const ApplyLaunch<T> &L) {
             constexpr int V = 16 / sizeof(T);
-            const unsigned long long columns = L.extent[L.rank - 1], span = 256ull * V * 2;
+            const unsigned long long columns = L.extent[L.rank - 1], span = 256ull * V * kVectorsPerThread;
             const unsigned long long pieces = (L.count / columns) * ((columns + span - 1) / span);
             // one wave: as many blocks as stay resident
             const unsigned long long most =
