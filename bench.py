@@ -865,7 +865,7 @@ def run_elements(args) -> int:
             made.append(array)
         return made
 
-    steps = {}
+    steps, counts = {}, {}
     shrink = 2 if args.small else 0  # --small: a quarter of each size, for profiler captures
     for dtype, count in ((np.int32, 1 << (28 - shrink)), (np.int8, 1 << (30 - shrink)), (np.int64, 1 << (27 - shrink))):
         a, b, c = operands(dtype, count)
