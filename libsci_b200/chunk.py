@@ -283,8 +283,13 @@ class Node(Expression):
     def __init__(self, code: str, children):
         self.code = CODE[code]
         self.children = children
-        self.dtype = next(c.dtype for c in children if not isinstance(c, Literal))
-        self.count = next(c.count for c in children if not isinstance(c, Literal))
+        arrays = [c for c in children if not isinstance(c, Literal)]
+        self.dtype = arrays[0].dtype
+        self.count = arrays[0].count
+        # node.hpp:32-33: every operand has the node's element type (a compile-time error there)
+        for other in arrays[1:]:
+            if other.dtype != self.dtype:
+                raise TypeError(f"operands must share an element type: {self.dtype} and {other.dtype}")
 
     def record(self, chunk: Chunk) -> int:
         slots = [child.record(chunk) for child in self.children]

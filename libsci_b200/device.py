@@ -535,14 +535,22 @@ def mean(item):
     if expr.count == 0:
         return expr.dtype.type(0) if expr.dtype.kind in "iu" else 0.0
     if expr.dtype.kind in "iu":
-        total = int(sum(item))
-        count = int(np.array(expr.count, np.uint64).astype(expr.dtype))  # static_cast<element>(count)
-        if count == 0:
-            raise ZeroDivisionError("the count converts to 0 in the element type")
-        quotient = abs(total) // abs(count) * (1 if (total < 0) == (count < 0) else -1)
-        return np.array(quotient).astype(expr.dtype)[()]
+        return integer_mean(sum(item), expr.count, expr.dtype)
     total = expr.dtype.type(sum(item))
     return float(total / expr.dtype.type(expr.count))
+
+
+def integer_mean(total, count: int, dtype):
+    """reduce.hpp:27 for an integer element: sum / static_cast<element>(count), the sum already
+    wrapped in the element's width, the count converted (wrapping) to the element type, and the
+    division truncating toward zero (wrapping for MIN / -1)."""
+    dtype = np.dtype(dtype)
+    divisor = int(np.array(count, np.uint64).astype(dtype))
+    if divisor == 0:
+        raise ZeroDivisionError("the count converts to 0 in the element type")
+    total = int(total)
+    quotient = abs(total) // abs(divisor) * (1 if (total < 0) == (divisor < 0) else -1)
+    return np.array(quotient).astype(dtype)[()]
 
 
 def dot(first, second):

@@ -294,6 +294,7 @@ int sci_ref_elements(const int which, const uint32_t element, const void *a, con
         case 10: folded = sci::sum(x * y); break;
         case 11: folded = sci::minimum(x - z); break;
         case 12: folded = sci::maximum(sci::absolute(y) + x); break;
+        case 13: folded = sci::mean(x * y); break;
         default: return 1;
         }
         if (which >= 10) std::memcpy(out, &folded, sizeof(T));

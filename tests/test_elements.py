@@ -135,3 +135,17 @@ def test_elements_recorder_uses_float_bytecode_layout():
     chunk = C.record_output(a * b + 3)
     assert [step[0] for step in chunk.listing()] == ["fuse"]
     assert chunk.literals == 1 and chunk.constants[0] == 3.0
+
+
+@pytest.mark.parametrize("dtype", [np.int8, np.int16, np.int32, np.uint8, np.uint32])
+def test_integer_mean_matches_reference(oracle, reference, dtype):
+    # sci::mean (reduce.hpp:24-28) over int arrays: the wrapped sum divided by the count converted to
+    # the element type; the host side of libsci_b200.device.mean does that division on the device's
+    # sum (here the oracle's)
+    from libsci_b200.device import integer_mean
+
+    for count in (1, 7, 100, 4099):
+        arrays = operands(dtype, count, seed=count)
+        total = oracle_elements(oracle, 10, arrays, dtype)[0]  # sum(x * y)
+        want = reference_elements(reference, 13, arrays, dtype)[0]  # mean(x * y)
+        assert integer_mean(total, count, dtype) == want, (np.dtype(dtype).name, count, total, want)

@@ -58,3 +58,13 @@ def test_recorder_rules():
     for k in range(70):
         e = e + float(k)
     assert not C.record_output(e).valid()
+
+
+def test_operands_must_share_an_element_type():
+    # node.hpp:32-33 rejects a node over arrays of different element types at compile time; the
+    # recorder raises instead of recording one of them under the other's type
+    a = C.Reference(16, 8, np.float32)
+    b = C.Reference(32, 8, np.int32)
+    with pytest.raises(TypeError):
+        C.binary("add", a, b)
+    assert C.binary("add", a, 2).dtype == np.float32  # a literal takes the array's type
