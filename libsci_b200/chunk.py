@@ -83,9 +83,12 @@ class ChunkStruct(ctypes.Structure):
 class Chunk(ChunkStruct):
     """A chunk being recorded; the recording rules follow chunk.hpp line by line (see module doc)."""
 
-    def __init__(self, precision: int = SINGLE):
+    def __init__(self, precision: int = SINGLE, element: int | None = None):
         super().__init__()
         self.precision = precision
+        # SCI_ELEMENT_* of the arrays the chunk reads (not part of the C struct): the float kernels
+        # take only float / double chunks, the element kernels any
+        self.element = precision if element is None else element
         self.result = NONE
         self._busy = 0
         self._overflow = False
@@ -320,15 +323,29 @@ def unary(code: str, item) -> Node:
     return Node(code, [_operand(item, None)])
 
 
+def _new_chunk(dtype) -> Chunk:
+    dtype = np.dtype(dtype)
+    if dtype not in ELEMENT:
+        raise TypeError(f"no device chunks over {dtype} elements (float32, float64 and the integer types)")
+    return Chunk(WIDE if dtype == np.float64 else SINGLE, ELEMENT[dtype])
+
+
 def record_output(expression: Expression) -> Chunk:
     """assign(): chunk.output(item.record(chunk)) (expression.hpp:162-163)."""
-    chunk = Chunk(WIDE if expression.dtype == np.float64 else SINGLE)
+    chunk = _new_chunk(expression.dtype)
     chunk.output(expression.record(chunk))
     return chunk
 
 
 def record_reduce(expression: Expression) -> Chunk:
     """reduce(): chunk.reduce(item.record(chunk)) (expression.hpp:194-195)."""
-    chunk = Chunk(WIDE if expression.dtype == np.float64 else SINGLE)
+    chunk = _new_chunk(expression.dtype)
     chunk.reduce(expression.record(chunk))
     return chunk
+
+
+def require_float(chunk) -> None:
+    """The float kernels (execute, reduce, gradients, batches) read float or double lanes: a chunk
+    recorded over another element type would be read at the wrong width."""
+    if getattr(chunk, "element", chunk.precision) not in (SINGLE, WIDE):
+        raise TypeError("an integer-element chunk runs through execute_elements / reduce_elements")

@@ -199,27 +199,32 @@ class Device:
 
     # -- chunks ---------------------------------------------------------------------------------
     def execute(self, chunk: C.Chunk, output: int, count: int) -> None:
+        C.require_float(chunk)
         check(lib.sci_cuda_execute(self.handle, ctypes.byref(chunk), output, count), self.handle)
 
     def reduce_chunk(self, chunk: C.Chunk, fold: int, count: int) -> float:
+        C.require_float(chunk)
         result = ctypes.c_double()
         check(lib.sci_cuda_reduce(self.handle, ctypes.byref(chunk), fold, count, ctypes.byref(result)), self.handle)
         return result.value
 
     def execute_elements(self, dtype, chunk: C.Chunk, output: int, count: int) -> None:
         """assign() for any element type (expression.hpp:158-185), integers included."""
+        _same_element(chunk, dtype)
         check(lib.sci_cuda_execute_elements(self.handle, C.ELEMENT[np.dtype(dtype)], ctypes.byref(chunk), output, count),
               self.handle)
 
     def reduce_elements(self, dtype, chunk: C.Chunk, fold: int, count: int):
         """reduce() for any element type (expression.hpp:191-221): one element of `dtype`."""
         dtype = np.dtype(dtype)
+        _same_element(chunk, dtype)
         result = np.zeros(1, dtype)
         check(lib.sci_cuda_reduce_elements(self.handle, C.ELEMENT[dtype], ctypes.byref(chunk), fold, count,
                                            result.ctypes.data), self.handle)
         return result[0]
 
     def reduce_async(self, chunk: C.Chunk, fold: int, count: int, device_result: int) -> None:
+        C.require_float(chunk)
         check(lib.sci_cuda_reduce_async(self.handle, ctypes.byref(chunk), fold, count, device_result), self.handle)
 
     def product(self, left: "DeviceArray", right: "DeviceArray", rows: int, columns: int, depth: int,
@@ -263,6 +268,11 @@ class Device:
         expr = C._operand(expression, None)
         if out is None:
             out = self.empty(expr.count, expr.dtype)
+        elif out.dtype != expr.dtype or out.count != expr.count:
+            # assign's ASSERT(target.shape() == item.shape()) (expression.hpp:160), and the element
+            # types match by construction there
+            raise ValueError(f"target of {out.count} {out.dtype} elements for an expression of {expr.count} "
+                             f"{expr.dtype} elements")
         chunk = C.record_output(expr)
         if not chunk.valid():
             raise SciCudaError(1, "expression outgrew the 64-entry chunk")
@@ -289,6 +299,7 @@ class Device:
         the temporary-storing comparison form instead of the recomputing adjoint."""
         expr = C._operand(expression, None)
         chunk = C.record_reduce(expr)
+        C.require_float(chunk)
         if not chunk.valid():
             raise SciCudaError(1, "expression outgrew the 64-entry chunk")
         wanted = {int(w.pointer): i for i, w in enumerate(wrt)}
@@ -338,6 +349,7 @@ class Device:
         dispatches into Vulkan command buffers). inputs: items x arguments device pointers; counts:
         items element counts; outputs: items device pointers or None; results: a float64
         DeviceArray of items values, or None."""
+        C.require_float(chunk)
         return Batch(self, chunk, fold, inputs, counts, outputs, results)
 
 
@@ -556,6 +568,12 @@ def integer_mean(total, count: int, dtype):
 def dot(first, second):
     """linear::dot: reduce(first * second, sum) (product.hpp:72-76), contracted on the device."""
     return _device_of(first).reduce(C.binary("multiply", first, second), C.SUM)
+
+
+def _same_element(chunk, dtype) -> None:
+    element = getattr(chunk, "element", None)
+    if element is not None and element != C.ELEMENT[np.dtype(dtype)]:
+        raise TypeError(f"the chunk was recorded over another element type than {np.dtype(dtype)}")
 
 
 def _shaped(item, device=None, dtype=None):

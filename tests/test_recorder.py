@@ -68,3 +68,17 @@ def test_operands_must_share_an_element_type():
     with pytest.raises(TypeError):
         C.binary("add", a, b)
     assert C.binary("add", a, 2).dtype == np.float32  # a literal takes the array's type
+
+
+def test_unsupported_and_integer_chunks_stay_off_the_float_kernels():
+    # a float16 or bool array has no device chunk; an integer chunk is refused by the float entry
+    # points (which would read its lanes at the float width) before anything launches
+    with pytest.raises(TypeError):
+        C.record_output(C.Reference(16, 8, np.float16) * 2)
+    with pytest.raises(TypeError):
+        C.record_reduce(C.Reference(16, 8, np.bool_) + 1)
+    integer = C.record_output(C.Reference(16, 8, np.int8) * 2)
+    assert integer.element == C.ELEMENT[np.dtype(np.int8)]
+    with pytest.raises(TypeError):
+        C.require_float(integer)
+    C.require_float(C.record_output(C.Reference(16, 8, np.float64) * 2))
