@@ -153,6 +153,7 @@ class Device:
     def decompose(self, matrix: "DeviceArray", order: int, plain: bool = False):
         """decompose (decompose.hpp:77-103): (P, L, U) with A = P L U, each order x order, made on the
         device."""
+        _require(matrix, order * order, matrix.dtype, "decompose")
         p, l, u = (self.empty(order * order, matrix.dtype) for _ in range(3))
         check(lib.sci_cuda_decompose(self.handle, self._precision(matrix.dtype), 1 if plain else 0,
                                      matrix.pointer, p.pointer, l.pointer, u.pointer, order), self.handle)
@@ -191,6 +192,8 @@ class Device:
         if not 0 <= axis < len(shape):
             raise ValueError(f"axis {axis} of a rank-{len(shape)} array")
         kept = shape[:axis] + shape[axis + 1:]
+        if array.count != int(np.prod(shape, dtype=np.int64)):
+            raise ValueError(f"reduce_axis: {array.count} elements do not have shape {shape}")
         out = self.empty(int(np.prod(kept, dtype=np.int64)), array.dtype)
         extents = (ctypes.c_uint64 * len(shape))(*shape)
         check(lib.sci_cuda_reduce_axis(self.handle, self._precision(array.dtype), fold, array.pointer, len(shape), extents,
@@ -236,7 +239,10 @@ class Device:
         dtype = left.dtype
         if out is None:
             out = self.empty(rows * columns, dtype)
-        precision = C.WIDE if dtype == np.float64 else C.SINGLE
+        precision = self._precision(dtype)
+        _require(left, rows * depth, dtype, "product left")
+        _require(right, depth * columns, dtype, "product right")
+        _require(out, rows * columns, dtype, "product output")
         check(lib.sci_cuda_product(self.handle, precision, mode, left.pointer, right.pointer, out.pointer, rows, columns,
                                    depth), self.handle)
         return out
@@ -244,7 +250,8 @@ class Device:
     def factor(self, matrix: "DeviceArray", order: int, plain: bool = False) -> np.ndarray:
         """linear::factor (decompose.hpp:29-72) in place; returns rows[] (original row at each position)."""
         rows = np.zeros(order, np.uint64)
-        precision = C.WIDE if matrix.dtype == np.float64 else C.SINGLE
+        precision = self._precision(matrix.dtype)
+        _require(matrix, order * order, matrix.dtype, "factor")
         check(lib.sci_cuda_factor(self.handle, precision, 1 if plain else 0, matrix.pointer, rows.ctypes.data, order),
               self.handle)
         return rows
@@ -257,7 +264,10 @@ class Device:
 
         if out is None:
             out = self.empty(order * width, right.dtype)
-        precision = C.WIDE if matrix.dtype == np.float64 else C.SINGLE
+        precision = self._precision(matrix.dtype)
+        _require(matrix, order * order, matrix.dtype, "solve matrix")
+        _require(right, order * width, matrix.dtype, "solve right-hand side")
+        _require(out, order * width, matrix.dtype, "solve output")
         report = SolveReport()
         check(lib.sci_cuda_solve(self.handle, precision, 1 if refine else 0, matrix.pointer, right.pointer, out.pointer,
                                  order, width, ctypes.byref(report)), self.handle)
@@ -322,8 +332,11 @@ class Device:
                          columns: int, depth: int, mode: int = 0):
         """Adjoints of product (new): (upstream @ right.T, left.T @ upstream) as DeviceArrays."""
         dtype = left.dtype
+        precision = self._precision(dtype)
+        _require(left, rows * depth, dtype, "product_gradient left")
+        _require(right, depth * columns, dtype, "product_gradient right")
+        _require(upstream, rows * columns, dtype, "product_gradient upstream")
         dl, dr = self.empty(rows * depth, dtype), self.empty(depth * columns, dtype)
-        precision = C.WIDE if dtype == np.float64 else C.SINGLE
         check(lib.sci_cuda_product_gradient(self.handle, precision, mode, left.pointer, right.pointer, upstream.pointer,
                                             dl.pointer, dr.pointer, rows, columns, depth), self.handle)
         return dl, dr
@@ -334,8 +347,11 @@ class Device:
         from .native import SolveReport
 
         dtype = matrix.dtype
+        precision = self._precision(dtype)
+        _require(matrix, order * order, dtype, "solve_gradient matrix")
+        _require(right, order * width, dtype, "solve_gradient right-hand side")
+        _require(upstream, order * width, dtype, "solve_gradient upstream")
         x, dm, db = self.empty(order * width, dtype), self.empty(order * order, dtype), self.empty(order * width, dtype)
-        precision = C.WIDE if dtype == np.float64 else C.SINGLE
         report = SolveReport()
         check(lib.sci_cuda_solve_gradient(self.handle, precision, 1 if refine else 0, matrix.pointer, right.pointer,
                                           upstream.pointer, x.pointer, dm.pointer, db.pointer, order, width,
@@ -568,6 +584,15 @@ def integer_mean(total, count: int, dtype):
 def dot(first, second):
     """linear::dot: reduce(first * second, sum) (product.hpp:72-76), contracted on the device."""
     return _device_of(first).reduce(C.binary("multiply", first, second), C.SUM)
+
+
+def _require(array: "DeviceArray", count: int, dtype, what: str) -> None:
+    """The C ABI sees raw pointers: the host checks that each operand holds what the call reads or
+    writes, in the call's element type, before anything launches."""
+    if array.dtype != np.dtype(dtype):
+        raise TypeError(f"{what}: {array.dtype} elements where {np.dtype(dtype)} is needed")
+    if array.count < count:
+        raise ValueError(f"{what}: {array.count} elements where the call uses {count}")
 
 
 def _same_element(chunk, dtype) -> None:
