@@ -8,6 +8,10 @@ codes.npz      for float32 and float64: inputs x, y (1031 values with specials) 
 workloads.npz  the plain fused workload at 4099 elements (a = linspace(0,1), b ~ U[-1,1) seed 0,
                c = 1): t = a*b + c*2, e = exp(t)*0.5, s = sum(sin(t)); and a seeded 64x64 float32
                matrix with its LU factors and row order from linear::factor.
+elements.npz   for the eight integer element types: operands x, y, z (129 values inside the ranges
+               where C++ defines every step) and the reference's host-loop results of the named
+               integer expressions of oracle/ref_bridge.cpp (sci_ref_elements 0-6, 10-13).
+               Written alone by: python tests/golden/make_golden.py elements
 """
 import sys
 from pathlib import Path
@@ -74,5 +78,25 @@ def main():
     print("wrote tests/golden/codes.npz and tests/golden/workloads.npz")
 
 
+def elements():
+    from tests.test_elements import INTEGERS, operands, reference_elements
+
+    ref = _oracle.reference()
+    if ref is None:
+        raise SystemExit("build oracle/_ref first: make -C oracle ref")
+    out = {}
+    for dtype in INTEGERS:
+        name = np.dtype(dtype).name
+        x, y, z = operands(dtype, 129, seed=29)
+        out[f"x_{name}"], out[f"y_{name}"], out[f"z_{name}"] = x, y, z
+        for which in list(range(7)) + [10, 11, 12, 13]:
+            out[f"{which}_{name}"] = reference_elements(ref, which, (x, y, z), dtype)
+    np.savez_compressed(ROOT / "tests" / "golden" / "elements.npz", **out)
+    print("wrote tests/golden/elements.npz")
+
+
 if __name__ == "__main__":
-    main()
+    if len(sys.argv) > 1 and sys.argv[1] == "elements":
+        elements()
+    else:
+        main()

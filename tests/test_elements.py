@@ -94,7 +94,7 @@ def oracle_elements(oracle, which, arrays, dtype):
 def reference_elements(reference, which, arrays, dtype):
     dtype = np.dtype(dtype)
     count = arrays[0].size
-    out = np.zeros(1 if which in REDUCTIONS else count, dtype)
+    out = np.zeros(1 if which in REDUCTIONS or which == 13 else count, dtype)
     x, y, z = arrays
     assert reference.sci_ref_elements(which, C.ELEMENT[dtype], x.ctypes.data, y.ctypes.data, z.ctypes.data, count,
                                       out.ctypes.data) == 0
@@ -149,3 +149,22 @@ def test_integer_mean_matches_reference(oracle, reference, dtype):
         total = oracle_elements(oracle, 10, arrays, dtype)[0]  # sum(x * y)
         want = reference_elements(reference, 13, arrays, dtype)[0]  # mean(x * y)
         assert integer_mean(total, count, dtype) == want, (np.dtype(dtype).name, count, total, want)
+
+
+def test_golden_elements(oracle):
+    """The reference's host-loop results committed by tests/golden/make_golden.py (elements.npz):
+    the oracle matches them without oracle/_ref present, and its integer mean with the host-side
+    division matches sci::mean."""
+    from pathlib import Path
+
+    from libsci_b200.device import integer_mean
+
+    data = np.load(Path(__file__).resolve().parent / "golden" / "elements.npz")
+    for dtype in INTEGERS:
+        name = np.dtype(dtype).name
+        arrays = tuple(np.ascontiguousarray(data[f"{v}_{name}"]) for v in "xyz")
+        for which in EVALUATIONS + list(REDUCTIONS):
+            got = oracle_elements(oracle, which, arrays, dtype)
+            assert np.array_equal(got, data[f"{which}_{name}"]), (name, which)
+        total = oracle_elements(oracle, 10, arrays, dtype)[0]
+        assert integer_mean(total, arrays[0].size, dtype) == data[f"13_{name}"][0], name
