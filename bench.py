@@ -15,7 +15,8 @@ operations a libsci user writes for it, each one kernel launch through the C ABI
 library's stream, max over ranks). Inputs are 1 GiB each, far larger than the 126 MB L2, so no
 flush is needed between steps. `e2e` runs the same step through the C ABI from pinned host buffers:
 the three inputs are uploaded and the three stored outputs and three reductions downloaded inside
-the timed region. `roofline` is the dominant kernel's achieved GB/s over the measured copy peak.
+the timed region, the step streamed in pieces through the copy lanes so that uploads, kernels and
+downloads overlap. `roofline` is the dominant kernel's achieved GB/s over the measured copy peak.
 `cpu_baseline` times libsci's own CPU path (oracle/_ref/libsci_ref.so, all host cores) on a
 2^24-element sample of the same workload.
 
@@ -29,6 +30,7 @@ from __future__ import annotations
 import argparse
 import ctypes
 import json
+import math
 import os
 import statistics
 import sys
@@ -1063,6 +1065,8 @@ def main() -> int:
     parser.add_argument("--impl", default="b200", choices=["b200", "reference"])
     parser.add_argument("--elements", type=int, default=1 << 28)
     parser.add_argument("--e2e-steps", type=int, default=3)
+    parser.add_argument("--e2e-pieces", type=int, default=8,
+                        help="pieces the end-to-end step streams through the copy lanes")
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     parser.add_argument("--small", action="store_true",
                         help="elements / shapes workloads at a quarter size (for profiler captures)")
@@ -1205,13 +1209,49 @@ def main() -> int:
     host_results = torch.zeros(3, dtype=torch.float64).pin_memory()
     from libsci_b200.native import check, lib
 
+    # The step in pieces through the copy lanes: the upload of piece p+1, the six chunks over piece p
+    # and the download of piece p-1 overlap (PCIe carries both directions at once). Each piece's
+    # three reductions land in its own slots and are folded into `results` on the main stream.
+    pieces = args.e2e_pieces if n % args.e2e_pieces == 0 else 1
+    span = n // pieces
+    piece_results = torch.zeros(pieces, 3, dtype=torch.float64, device=f"cuda:{local}")
+    piece_chunks = []
+    for p in range(pieces):
+        o = p * span
+        pa, pb, pc = (v.offset(o, span).expression() for v in (dx, dy, dz))
+        piece_chunks.append([
+            (C.record_output(C.unary("root", C.unary("absolute", pa)) * C.unary("logarithm", pb) + C.unary("tanh", pc)),
+             stored.pointer + 4 * o),
+            (C.record_output(C.binary("minimum", pa, pc)), lower.pointer + 4 * o),
+            (C.record_output(C.binary("maximum", pa, pc)), upper.pointer + 4 * o),
+            (C.record_reduce(C.unary("exponential", -pa * pa)), C.SUM),
+            (C.record_reduce(C.unary("sin", pa) * C.unary("cos", pc)), C.MAXIMUM),
+            (C.record_reduce(pa * pc), C.SUM),
+        ])
+
     def e2e_step():
-        for host, dev in ((hx, dx), (hy, dy), (hz, dz)):
-            check(lib.sci_cuda_upload(device.handle, dev.pointer, host.data_ptr(), n * 4), device.handle)
-        step()
-        for host, dev in zip(outs, (stored, lower, upper)):
-            check(lib.sci_cuda_download(device.handle, host.data_ptr(), dev.pointer, n * 4), device.handle)
-        check(lib.sci_cuda_download(device.handle, host_results.data_ptr(), results.data_ptr(), 24), device.handle)
+        check(lib.sci_cuda_join(device.handle), device.handle)  # lanes start after the main stream's work
+        for p in range(pieces):
+            o = p * span
+            for host, dev in ((hx, dx), (hy, dy), (hz, dz)):
+                check(lib.sci_cuda_upload_lane(device.handle, dev.pointer + 4 * o, host.data_ptr() + 4 * o, 4 * span),
+                      device.handle)
+            for i, (chunk, target) in enumerate(piece_chunks[p]):
+                if i < 3:
+                    device.execute(chunk, target, span)
+                else:
+                    device.reduce_async(chunk, target, span, piece_results.data_ptr() + 8 * (3 * p + i - 3))
+            for host, dev in zip(outs, (stored, lower, upper)):
+                check(lib.sci_cuda_download_lane(device.handle, host.data_ptr() + 4 * o, dev.pointer + 4 * o, 4 * span),
+                      device.handle)
+        with torch.cuda.stream(stream):
+            results[0] = piece_results[:, 0].sum()
+            results[1] = piece_results[:, 1].max()  # NaN propagates
+            results[2] = piece_results[:, 2].sum()
+            if dist is not None:
+                results.copy_(combine(results, (C.SUM, C.MAXIMUM, C.SUM)))
+        check(lib.sci_cuda_download_lane(device.handle, host_results.data_ptr(), results.data_ptr(), 24), device.handle)
+        check(lib.sci_cuda_join(device.handle), device.handle)
 
     e2e_step()
     device.synchronize()
@@ -1229,6 +1269,17 @@ def main() -> int:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
     e2e_value = STEP_BYTES_PER_ELEMENT * n * world / (e2e_ms * 1e-3) / 1e9
+    # the pieces reproduce the single-pass step: elementwise outputs bit for bit, reductions to FP64
+    # rounding
+    device.synchronize()
+    piecewise = host_results.clone()
+    step()
+    device.synchronize()
+    whole = results.cpu()
+    for slot in range(3):
+        a_, b_ = float(piecewise[slot]), float(whole[slot])
+        if not ((math.isnan(a_) and math.isnan(b_)) or abs(a_ - b_) <= 1e-9 * max(abs(b_), 1e-300)):
+            raise RuntimeError(f"pipelined reduction {slot} = {a_} differs from the single pass {b_}")
 
     # a correctness spot check of the step just run: the stored chunk against the CPU oracle
     cpu = None

@@ -115,6 +115,17 @@ int sci_cuda_dispose(sci_cuda_context *context, void *memory);
 /* Array::to(device) / Array::host() transfers (array.hpp:223-237), queued on the stream. */
 int sci_cuda_upload(sci_cuda_context *context, void *device, const void *host, uint64_t bytes);
 int sci_cuda_download(sci_cuda_context *context, void *host, const void *device, uint64_t bytes);
+/* Copy lanes (new; the reference copies through the host pointer): the same copies on two more
+ * streams, so that uploads, kernels and downloads of different pieces overlap. An upload on the
+ * lane starts without waiting for queued work, and work queued after it waits for it; a download
+ * on the lane waits for the work queued before it and delays nothing queued after it. Host memory
+ * should be pinned for the copies to overlap. sci_cuda_join is a barrier between the lanes and the
+ * main stream: work queued after it waits for every lane copy queued before it, and lane copies
+ * queued after it wait for the main stream's work queued before it. sci_cuda_synchronize waits for
+ * the lanes too. */
+int sci_cuda_upload_lane(sci_cuda_context *context, void *device, const void *host, uint64_t bytes);
+int sci_cuda_download_lane(sci_cuda_context *context, void *host, const void *device, uint64_t bytes);
+int sci_cuda_join(sci_cuda_context *context);
 
 /* ---- chunks ------------------------------------------------------------------------------ */
 /* Device::execute(chunk, output, count) (device.hpp:63, device.cpp:235-263): output[i] =

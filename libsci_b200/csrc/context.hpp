@@ -92,6 +92,11 @@ namespace sci_cuda {
         cudaEvent_t side_done{nullptr};         // the side stream's queued work has finished
         cudaEvent_t main_ready{nullptr};        // the main stream reached the point the side waits for
         std::unique_ptr<Workspace> side_space;  // the side stream's product operands
+        cudaStream_t upload_lane{nullptr};    // host-to-device copies that overlap the main stream
+        cudaStream_t download_lane{nullptr};  // device-to-host copies that overlap the main stream
+        cudaEvent_t uploaded{nullptr};        // the upload lane's last queued copy
+        cudaEvent_t downloaded{nullptr};      // the download lane's last queued copy
+        cudaEvent_t main_point{nullptr};      // where the main stream was when a download was queued
         unsigned *sweep_flags{nullptr};  // progress marks of the persistent substitution sweeps
         size_t sweep_capacity{0};        // flags allocated
         unsigned sweep_epoch{0};         // the value that marks a flag as set by the current sweep

@@ -319,6 +319,15 @@ int sci_cuda_close(sci_cuda_context *context) {
         if (context->side_done) cudaEventDestroy(context->side_done);
         if (context->main_ready) cudaEventDestroy(context->main_ready);
         if (context->side_space) context->side_space->release();
+        if (context->upload_lane) {
+            cudaStreamSynchronize(context->upload_lane);
+            cudaStreamSynchronize(context->download_lane);
+            cudaStreamDestroy(context->upload_lane);
+            cudaStreamDestroy(context->download_lane);
+            cudaEventDestroy(context->uploaded);
+            cudaEventDestroy(context->downloaded);
+            cudaEventDestroy(context->main_point);
+        }
         cudaFreeHost(context->host_result);
         cudaFreeHost(context->host_status);
         cudaStreamDestroy(context->stream);
@@ -339,6 +348,11 @@ int sci_cuda_synchronize(sci_cuda_context *context) {
     if (!context) return SCI_CUDA_ERROR_INVALID;
     std::lock_guard<std::recursive_mutex> lock(context->guard);
     cudaSetDevice(context->device);
+    if (context->upload_lane) {
+        if (int code = context->check(cudaStreamSynchronize(context->upload_lane), "synchronizing the upload lane")) return code;
+        if (int code = context->check(cudaStreamSynchronize(context->download_lane), "synchronizing the download lane"))
+            return code;
+    }
     return context->drain();
 }
 
@@ -401,6 +415,66 @@ int sci_cuda_download(sci_cuda_context *context, void *host, const void *device,
     std::lock_guard<std::recursive_mutex> lock(context->guard);
     cudaSetDevice(context->device);
     return context->check(cudaMemcpyAsync(host, device, bytes, cudaMemcpyDeviceToHost, context->stream), "download");
+}
+
+// ---- copy lanes: host <-> device copies that overlap the main stream's work -------------------
+// Two more streams per context, made on first use. An upload on the lane starts at once (it does
+// not wait for queued kernels) and everything queued on the main stream after it waits for it; a
+// download on the lane waits for everything queued on the main stream before it and delays nothing
+// queued after it. PCIe carries both directions at once, so a caller that splits its arrays into
+// pieces overlaps the upload of one piece, the kernels of the previous and the download of the one
+// before that. The caller keeps a buffer out of a lane copy while earlier queued work still uses it,
+// or calls sci_cuda_join, a barrier between the lanes and the main stream in both directions.
+namespace {
+    int open_lanes(Context &ctx) {
+        if (ctx.upload_lane) return SCI_CUDA_OK;
+        if (int code = ctx.check(cudaStreamCreateWithFlags(&ctx.upload_lane, cudaStreamNonBlocking), "upload lane")) return code;
+        if (int code = ctx.check(cudaStreamCreateWithFlags(&ctx.download_lane, cudaStreamNonBlocking), "download lane"))
+            return code;
+        for (cudaEvent_t *event : {&ctx.uploaded, &ctx.downloaded, &ctx.main_point})
+            if (int code = ctx.check(cudaEventCreateWithFlags(event, cudaEventDisableTiming), "lane event")) return code;
+        return SCI_CUDA_OK;
+    }
+} // namespace
+
+int sci_cuda_upload_lane(sci_cuda_context *context, void *device, const void *host, uint64_t bytes) {
+    if (!context || (!device && bytes) || (!host && bytes)) return SCI_CUDA_ERROR_INVALID;
+    std::lock_guard<std::recursive_mutex> lock(context->guard);
+    cudaSetDevice(context->device);
+    if (int code = open_lanes(*context)) return code;
+    if (int code = context->check(cudaMemcpyAsync(device, host, bytes, cudaMemcpyHostToDevice, context->upload_lane),
+                                  "lane upload"))
+        return code;
+    if (int code = context->check(cudaEventRecord(context->uploaded, context->upload_lane), "lane upload event")) return code;
+    return context->check(cudaStreamWaitEvent(context->stream, context->uploaded, 0), "main stream waits for the upload");
+}
+
+int sci_cuda_download_lane(sci_cuda_context *context, void *host, const void *device, uint64_t bytes) {
+    if (!context || (!device && bytes) || (!host && bytes)) return SCI_CUDA_ERROR_INVALID;
+    std::lock_guard<std::recursive_mutex> lock(context->guard);
+    cudaSetDevice(context->device);
+    if (int code = open_lanes(*context)) return code;
+    if (int code = context->check(cudaEventRecord(context->main_point, context->stream), "main stream point")) return code;
+    if (int code = context->check(cudaStreamWaitEvent(context->download_lane, context->main_point, 0), "download lane waits"))
+        return code;
+    if (int code = context->check(cudaMemcpyAsync(host, device, bytes, cudaMemcpyDeviceToHost, context->download_lane),
+                                  "lane download"))
+        return code;
+    return context->check(cudaEventRecord(context->downloaded, context->download_lane), "lane download event");
+}
+
+int sci_cuda_join(sci_cuda_context *context) {
+    if (!context) return SCI_CUDA_ERROR_INVALID;
+    std::lock_guard<std::recursive_mutex> lock(context->guard);
+    if (!context->upload_lane) return SCI_CUDA_OK;
+    cudaSetDevice(context->device);
+    if (int code = context->check(cudaStreamWaitEvent(context->stream, context->uploaded, 0), "join uploads")) return code;
+    if (int code = context->check(cudaStreamWaitEvent(context->stream, context->downloaded, 0), "join downloads")) return code;
+    // and the other way: lane copies queued after the join wait for the main stream's work before it
+    if (int code = context->check(cudaEventRecord(context->main_point, context->stream), "join point")) return code;
+    if (int code = context->check(cudaStreamWaitEvent(context->upload_lane, context->main_point, 0), "join upload lane"))
+        return code;
+    return context->check(cudaStreamWaitEvent(context->download_lane, context->main_point, 0), "join download lane");
 }
 
 int sci_cuda_execute(sci_cuda_context *context, const sci_chunk *chunk, void *output, uint64_t count) {

@@ -97,6 +97,9 @@ def _load() -> ctypes.CDLL:
     sig["sci_cuda_grid"] = (ctypes.c_int, [c_ctx, U32, VP, U64, VP, U64, VP, VP])
     sig["sci_cuda_decompose"] = (ctypes.c_int, [c_ctx, U32, U32, VP, VP, VP, VP, U64])
     sig["sci_cuda_transpose"] = (ctypes.c_int, [c_ctx, U32, VP, U32, P(U64), VP])
+    sig["sci_cuda_upload_lane"] = (ctypes.c_int, [c_ctx, VP, VP, U64])
+    sig["sci_cuda_download_lane"] = (ctypes.c_int, [c_ctx, VP, VP, U64])
+    sig["sci_cuda_join"] = (ctypes.c_int, [c_ctx])
     sig["sci_cuda_broadcast"] = (ctypes.c_int, [c_ctx, U32, U32, U32, P(U64), U32, P(VP), P(U64), VP])
     sig["sci_cuda_reduce_axis"] = (ctypes.c_int, [c_ctx, U32, U32, VP, U32, P(U64), U32, VP])
     sig["sci_cuda_element_size"] = (U64, [U32])
