@@ -168,3 +168,28 @@ def test_golden_elements(oracle):
             assert np.array_equal(got, data[f"{which}_{name}"]), (name, which)
         total = oracle_elements(oracle, 10, arrays, dtype)[0]
         assert integer_mean(total, arrays[0].size, dtype) == data[f"13_{name}"][0], name
+
+
+def test_oracle_defines_the_undefined_cases(oracle):
+    """Where C++ leaves the host loop undefined, the backend defines the result (and the device is
+    held to the oracle there): division by zero gives 0, MIN / -1 wraps to MIN, signed overflow
+    wraps, a NaN real result converts to 0 and out-of-range real results saturate."""
+    def run(expression, arrays, dtype):
+        chunk = C.record_output(expression)
+        out = np.empty(arrays[0].size, dtype)
+        assert oracle.sci_oracle_execute_elements(C.ELEMENT[np.dtype(dtype)], ctypes.byref(chunk), out.ctypes.data,
+                                                  out.size) == 0
+        return out
+
+    for dtype in (np.int8, np.int32, np.int64):
+        info = np.iinfo(dtype)
+        x = np.array([7, info.min, info.max, -9, 0], dtype)
+        y = np.array([0, -1, 2, 0, 0], dtype)
+        a, b = leaves((x, y), dtype)
+        assert run(a / b, (x, y), dtype).tolist() == [0, info.min, info.max // 2, 0, 0]
+        wrapped = (x.astype(object) * 2 + 0)
+        want = [((int(v) - int(info.min)) % (1 << (8 * np.dtype(dtype).itemsize))) + int(info.min) for v in wrapped]
+        assert run(a * 2, (x, y), dtype).tolist() == want
+        assert run(C.unary("root", a), (x, y), dtype).tolist()[1] == 0            # sqrt(MIN) is NaN -> 0
+        assert run(C.unary("exponential", a), (x, y), dtype).tolist()[2] == info.max  # saturates
+        assert run(C.unary("logarithm", a), (x, y), dtype).tolist()[4] == info.min    # log(0) = -inf
