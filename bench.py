@@ -102,20 +102,30 @@ class ClockSampler:
             self.nvml = None
         self.thread = threading.Thread(target=self._run, daemon=True)
 
+    def _sample(self) -> bool:
+        try:
+            self.samples.append(self.nvml.nvmlDeviceGetClockInfo(self.handle, self.nvml.NVML_CLOCK_SM))
+            mask = self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+        except Exception:
+            return False
+        for bit, name in self.REASONS.items():
+            if mask & bit:
+                self.reasons.add(name)
+        return True
+
     def _run(self):
-        while not self._stop.is_set():
-            try:
-                self.samples.append(self.nvml.nvmlDeviceGetClockInfo(self.handle, self.nvml.NVML_CLOCK_SM))
-                mask = self.nvml.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
-                for bit, name in self.REASONS.items():
-                    if mask & bit:
-                        self.reasons.add(name)
-            except Exception:
+        # a fixed 5 ms period measured from the start, so a thread starved of the GIL for a while
+        # resumes on the next tick instead of drifting
+        start = time.perf_counter()
+        tick = 1
+        while not self._stop.wait(max(0.0, start + 0.005 * tick - time.perf_counter())):
+            if not self._sample():
                 break
-            time.sleep(0.002)
+            tick += 1
 
     def __enter__(self):
         if self.nvml:
+            self._sample()  # one sample as the region starts, whatever the thread manages
             self.thread.start()
         return self
 

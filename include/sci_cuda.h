@@ -334,13 +334,15 @@ int sci_cuda_solve_batch_destroy(sci_cuda_solve_batch *batch);
  * latency-critical thread where an allocation would synchronize the device). It needs no context:
  * it runs on the calling thread's current device and on `stream` (a cudaStream_t; 0 is the legacy
  * default stream), reads the chunk's inputs from device memory and writes the double result to
- * `device_result`, both on that device. Its scratch is one fixed 49,408-byte array compiled into
+ * `device_result`, both on that device. Its scratch is one fixed 49,664-byte array compiled into
  * the library, holding partials for at most 4096 blocks: `blocks` = 0 picks the launch width,
  * a larger value than 4096 is rejected with SCI_CUDA_ERROR_INVALID. It calls no cudaMalloc or
  * cudaFree. Every call on a device shares that array: calls whose kernels may overlap on the GPU
  * race and must be ordered by the caller (one stream, or events). The first call on a device
- * looks up the array's device address; make it before capturing the stream into a graph. On
- * failure a message is written to `message` (may be null). */
+ * looks up the array's device address; make it before capturing the stream into a graph. The
+ * call returns before the kernel runs, so a device-side failure cannot come back as a status: if
+ * a block's bounded wait on its input copies runs out, `device_result` receives a quiet NaN
+ * rather than a partial value. On failure a message is written to `message` (may be null). */
 int sci_cuda_reduce_noalloc(const sci_chunk *chunk, uint32_t fold, uint64_t count, double *device_result,
                             void *stream, uint32_t blocks, char *message, size_t message_length);
 /* ---- arrays made on the device (include/operations/creation.hpp) ----------------------------

@@ -497,7 +497,11 @@ namespace sci_cuda {
     // partials in block order and writes the value to `destination`. Every thread of the block
     // calls it.
     template <typename T>
-    __device__ __forceinline__ void finish_fold(Fold fold, unsigned op, ReduceState *state, double *destination) {
+    // `status`, when given, is the launch's error word: if a block gave up on its copies (its
+    // partial then covers only the tiles before it stopped), the result is a quiet NaN instead of a
+    // partial fold, so a caller that never reads the word still cannot take the value for a result.
+    __device__ __forceinline__ void finish_fold(Fold fold, unsigned op, ReduceState *state, double *destination,
+                                                const int *status = nullptr) {
         __shared__ double block_total[32];
         __shared__ unsigned block_magnitude[32];
         __shared__ bool last_block;
@@ -546,7 +550,9 @@ namespace sci_cuda {
                 poisoned |= __shfl_xor_sync(0xffffffffu, poisoned, offset);
             }
             if (t == 0) {
-                *destination = poisoned ? __longlong_as_double(0x7ff8000000000000ll) : total;
+                // every block's atomicOr on the word came before its ticket (fenced), so it is seen here
+                const bool gave_up = status != nullptr && (__ldcg(status) & kStatusTimeout) != 0;
+                *destination = poisoned || gave_up ? __longlong_as_double(0x7ff8000000000000ll) : total;
                 state->ticket = 0;
             }
         }
@@ -647,7 +653,7 @@ namespace sci_cuda {
             if constexpr (MODE != kEvaluate) fold_tile<T, MODE>(fold, op, value, second, w, false);
         }
 
-        if constexpr (MODE != kEvaluate) finish_fold<T>(fold, op, L.state, L.destination);
+        if constexpr (MODE != kEvaluate) finish_fold<T>(fold, op, L.state, L.destination, L.status);
     }
 
 } // namespace sci_cuda

@@ -135,6 +135,45 @@ namespace sci_cuda {
         int drain();
     };
 
+    // Block size, TMA ring depth and dynamic shared memory of a chunk launch: the widest tile whose
+    // temporaries (none for a specialised kernel, which keeps them in registers) and staged inputs
+    // fit in `budget` bytes. A chunk with transcendental codes is bound by instruction issue, not
+    // by HBM: a two-stage ring already covers its load latency, and the shared memory it frees buys
+    // more resident warps to hide its arithmetic latency; arithmetic-only chunks keep the deepest
+    // ring. threads = 0 when even a 32-thread tile does not fit.
+    struct ChunkShape {
+        int threads{0};
+        unsigned stages{0};
+        size_t smem{0};
+    };
+    inline ChunkShape chunk_shape(const Step *steps, unsigned length, unsigned arguments, unsigned temporaries,
+                                  size_t element, bool staged_ok, bool specialised, size_t budget) {
+        bool heavy = false;
+        for (unsigned s = 0; s < length; ++s) heavy = heavy || (steps[s].code >= kExponential && steps[s].code < kAdd);
+        const size_t ring = heavy ? 2u : static_cast<size_t>(kMaxStages);
+        ChunkShape shape;
+        for (int threads = 256; threads >= 32; threads /= 2) {
+            const size_t tile_bytes = size_t(32 / element) * threads * element;
+            const size_t temps = specialised ? 0 : size_t(temporaries) * tile_bytes;
+            if (temps > budget) continue;
+            unsigned stages = 0;
+            if (staged_ok && arguments > 0) {
+                const size_t fit = (budget - temps) / (size_t(arguments) * tile_bytes);
+                stages = static_cast<unsigned>(fit < ring ? fit : ring);
+            }
+            if (stages == 0 && staged_ok && arguments > 0 && threads > 32) continue;  // try a smaller tile
+            shape.threads = threads;
+            shape.stages = stages;
+            shape.smem = temps + size_t(stages) * arguments * tile_bytes;
+            break;
+        }
+        return shape;
+    }
+
+    // Without the opt-in, static plus dynamic shared memory must stay within 48 KB; the chunk
+    // kernel's static part (mbarriers, fold scratch) is under 4 KB.
+    constexpr size_t kChunkSharedOptIn = 44 * 1024;
+
     // The generic interpreter's kernels, compiled ahead of time (chunk_kernels_f32.cu / _f64.cu).
     const void *generic_chunk_kernel(bool wide, int mode);
     const void *generic_chunk_kernel_f32(int mode);

@@ -172,32 +172,12 @@ namespace sci_cuda {
         const Specialized *special = ctx.specializer ? ctx.specializer->find(ctx, chunk, mode) : nullptr;
         const void *kernel = special ? special->function : generic_chunk_kernel(sizeof(T) == 8, mode);
         const size_t budget = std::min<size_t>(ctx.shared_limit, 200 * 1024);
-        const bool staged_ok = aligned(L, mode);
-        // A chunk with transcendental codes is bound by instruction issue, not by HBM: a two-stage
-        // ring already covers its load latency, and the shared memory it frees buys more resident
-        // warps to hide its arithmetic latency. Arithmetic-only chunks keep the deepest ring.
-        bool heavy = false;
-        for (unsigned s = 0; s < L.length; ++s) heavy = heavy || (L.steps[s].code >= kExponential && L.steps[s].code < kAdd);
-        const unsigned ring = heavy ? 2u : static_cast<unsigned>(kMaxStages);
-        int threads = 256;
-        unsigned stages = 0;
-        size_t smem = 0;
-        for (; threads >= 32; threads /= 2) {
-            const size_t tile_bytes = size_t(Lanes<T>::count) * threads * sizeof(T);
-            const size_t temps = special ? 0 : size_t(L.temporaries) * tile_bytes;
-            if (temps > budget) continue;
-            stages = 0;
-            if (staged_ok && L.arguments > 0) {
-                const size_t per_stage = size_t(L.arguments) * tile_bytes;
-                const size_t fit = (budget - temps) / per_stage;
-                stages = static_cast<unsigned>(std::min<size_t>(fit, ring));
-            }
-            if (stages == 0 && staged_ok && L.arguments > 0 && threads > 32) continue;  // try a smaller tile
-            smem = temps + size_t(stages) * L.arguments * tile_bytes;
-            break;
-        }
-        if (threads < 32) return ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "chunk too wide for shared memory");
-        L.stages = stages;
+        const ChunkShape shape = chunk_shape(L.steps, L.length, L.arguments, L.temporaries, sizeof(T), aligned(L, mode),
+                                             special != nullptr, budget);
+        if (shape.threads < 32) return ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "chunk too wide for shared memory");
+        const int threads = shape.threads;
+        const size_t smem = shape.smem;
+        L.stages = shape.stages;
 
         const uint64_t tile = uint64_t(Lanes<T>::count) * threads;
         const uint64_t tiles = (L.count + tile - 1) / tile;
@@ -222,9 +202,7 @@ namespace sci_cuda {
             if (code != CUDA_SUCCESS) return ctx.fail(SCI_CUDA_ERROR_LAUNCH, "launching a specialised chunk kernel: %d", int(code));
             return SCI_CUDA_OK;
         }
-        // without the opt-in, static plus dynamic shared memory must stay within 48 KB; the
-        // kernel's static part (mbarriers, fold scratch) is under 4 KB
-        if (smem > 44 * 1024) {
+        if (smem > kChunkSharedOptIn) {
             cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         }
         const int per_sm = ctx.blocks_per_sm(kernel, threads, smem);

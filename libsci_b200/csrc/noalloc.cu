@@ -12,8 +12,12 @@
 // runs; only where its scratch lives differs.
 //
 // Limits and sharing:
-//  - the array holds partials for at most kNoAllocBlocks (4096) blocks, 48 KiB in all; a request
-//    for a wider launch is rejected with SCI_CUDA_ERROR_INVALID and a message;
+//  - the array holds partials for at most kNoAllocBlocks (4096) blocks, 49,664 bytes in all
+//    (sizeof(noalloc_scratch)); a request for a wider launch is rejected with
+//    SCI_CUDA_ERROR_INVALID and a message;
+//  - a block whose bounded wait on its copies runs out sets the error word; the last block then
+//    writes a quiet NaN as the result instead of a fold of what the blocks saw, so a timeout can
+//    never pass for a value (the call itself returned long before, with SCI_CUDA_OK);
 //  - every GPU that loads this library holds one copy of the array until the process exits;
 //  - every call on a device shares that device's copy, and it keeps whatever the last call left:
 //    the ticket and the error word are cleared on the stream before each launch, the partials are
@@ -31,7 +35,8 @@
 #include <mutex>
 
 // The scratch of every call on a device: a sci_cuda::ReduceState (block partials, NaN flags,
-// ticket) and, 256-byte aligned after it, the kernel's error word; 4096 partials, 49,408 bytes.
+// ticket; 49,156 bytes, padded to 49,408) and, 256-byte aligned after it, the kernel's error word
+// in a 256-byte slot: 49,664 bytes in all, partials for 4096 blocks.
 // On the host this name is only a stand-in for the device variable, never a device address:
 // passing it to a kernel would fault, or where the GPU can reach host memory, silently use the
 // wrong memory. Host code gets the device address from cudaGetSymbolAddress (below).
@@ -46,6 +51,7 @@ namespace sci_cuda {
         constexpr unsigned long long kNoAllocBytes = kStatusOffset + 256;
         constexpr int kMaxDevices = 64;
         static_assert(sizeof(noalloc_scratch) == kNoAllocBytes, "scratch layout");
+        static_assert(kNoAllocBytes == 49664, "the documented size of the fixed scratch");
 
         struct DeviceSetup {
             bool ready{false};
@@ -144,29 +150,19 @@ namespace sci_cuda {
             L.status = reinterpret_cast<int *>(setup.scratch + kStatusOffset);
             L.destination = result;
 
-            // Block size and TMA ring depth, as for sci_cuda_reduce: the widest tile whose
-            // temporaries and staged inputs fit in shared memory.
-            const unsigned long long budget = setup.shared_limit < 200 * 1024 ? setup.shared_limit : 200 * 1024;
-            int threads = 256;
-            unsigned stages = 0;
-            unsigned long long smem = 0;
-            for (; threads >= 32; threads /= 2) {
-                const unsigned long long tile_bytes = 1ull * Lanes<T>::count * threads * sizeof(T);
-                const unsigned long long temps = 1ull * L.temporaries * tile_bytes;
-                if (temps > budget) continue;
-                stages = 0;
-                if (aligned && L.arguments > 0) {
-                    const unsigned long long fit = (budget - temps) / (1ull * L.arguments * tile_bytes);
-                    stages = static_cast<unsigned>(fit < kMaxStages ? fit : kMaxStages);
-                }
-                if (stages == 0 && aligned && L.arguments > 0 && threads > 32) continue;
-                smem = temps + 1ull * stages * L.arguments * tile_bytes;
-                break;
-            }
-            if (threads < 32) return say(message, length, SCI_CUDA_ERROR_UNSUPPORTED, "chunk too wide for shared memory");
-            L.stages = stages;
+            // Block size and TMA ring depth chosen exactly as sci_cuda_reduce chooses them for the
+            // generic interpreter (chunk_shape), so both entry points fold in the same order.
+            const size_t budget = setup.shared_limit < 200 * 1024 ? size_t(setup.shared_limit) : size_t(200 * 1024);
+            const ChunkShape shape = chunk_shape(L.steps, L.length, L.arguments, L.temporaries, sizeof(T), aligned, false,
+                                                 budget);
+            if (shape.threads < 32) return say(message, length, SCI_CUDA_ERROR_UNSUPPORTED, "chunk too wide for shared memory");
+            const int threads = shape.threads;
+            const size_t smem = shape.smem;
+            L.stages = shape.stages;
             const void *kernel = generic_chunk_kernel(sizeof(T) == 8, mode);
-            if (smem > 48 * 1024 &&
+            // Static shared memory (mbarriers, fold scratch) counts against the 48 KB a launch gets
+            // without the opt-in, so the limit is raised from the same threshold sci_cuda_reduce uses.
+            if (smem > kChunkSharedOptIn &&
                 cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) != cudaSuccess)
                 return say(message, length, SCI_CUDA_ERROR_LAUNCH, "cannot raise the kernel's shared memory limit");
             int per_sm = 1;

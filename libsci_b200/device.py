@@ -231,11 +231,13 @@ class Device:
         check(lib.sci_cuda_reduce_async(self.handle, ctypes.byref(chunk), fold, count, device_result), self.handle)
 
     def product(self, left: "DeviceArray", right: "DeviceArray", rows: int, columns: int, depth: int,
-                mode: int = 0, out: "DeviceArray | None" = None) -> "DeviceArray":
+                mode: int = 3, out: "DeviceArray | None" = None) -> "DeviceArray":
         """linear::product (include/linear/product.hpp:22-65): row-major out = left @ right.
 
-        mode: 0 bf16 tensor cores, 1 split-bf16 (three tensor-core products), 2 plain FP32 SIMT;
-        double operands always multiply in plain FP64."""
+        mode: 3 (the default) split3-bf16, six tensor-core products that keep FP32 accuracy like the
+        reference's float product (dispatch.cpp:171-224); 0 bf16 tensor cores (about 8 bits per
+        operand, an explicit opt-in); 1 split-bf16 (three products, about 16 bits); 2 plain FP32
+        SIMT. Double operands always multiply in plain FP64."""
         dtype = left.dtype
         if out is None:
             out = self.empty(rows * columns, dtype)
@@ -329,7 +331,7 @@ class Device:
 
 
     def product_gradient(self, left: "DeviceArray", right: "DeviceArray", upstream: "DeviceArray", rows: int,
-                         columns: int, depth: int, mode: int = 0):
+                         columns: int, depth: int, mode: int = 3):
         """Adjoints of product (new): (upstream @ right.T, left.T @ upstream) as DeviceArrays."""
         dtype = left.dtype
         precision = self._precision(dtype)

@@ -75,3 +75,50 @@ def test_no_alloc_reduction_limits(device):
     assert fn(ctypes.byref(chunk), C.MINIMUM, 0, result.pointer, device.stream, 0, message, 256) == 0
     device.synchronize()
     assert np.isnan(result.numpy()[0])
+
+
+FRESH_PROCESS = r"""
+import ctypes, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from libsci_b200 import chunk as C
+from libsci_b200.device import Device
+from libsci_b200.native import lib
+
+fn = lib.sci_cuda_reduce_noalloc
+fn.restype = ctypes.c_int
+fn.argtypes = [ctypes.POINTER(C.ChunkStruct), ctypes.c_uint32, ctypes.c_uint64, ctypes.c_void_p, ctypes.c_void_p,
+               ctypes.c_uint32, ctypes.c_char_p, ctypes.c_size_t]
+device = Device(0)
+n = (1 << 22) + 5
+x = device.array(np.random.default_rng(3).uniform(2.0, 3.0, n).astype(np.float32))
+result = device.empty(1, np.float64)
+a = x.expression()
+# one input and two temporaries, arithmetic only: 16 KiB of temporaries and four 8 KiB ring stages
+# at 256 threads, exactly 48 KiB of dynamic shared memory, which needs the kernel's opt-in
+chunk = C.record_reduce((a - 1.0) / (a + 1.0))
+assert chunk.arguments == 1 and chunk.temporaries == 2
+message = ctypes.create_string_buffer(256)
+got = []
+for _ in range(2):
+    status = fn(ctypes.byref(chunk), C.SUM, n, result.pointer, device.stream, 0, message, 256)
+    assert status == 0, message.value
+    device.synchronize()
+    got.append(float(result.numpy()[0]))
+want = device.reduce_chunk(chunk, C.SUM, n)
+assert all(abs(g - want) <= 1e-9 * abs(want) for g in got), (got, want)
+print("fresh", got[0], want)
+"""
+
+
+def test_no_alloc_first_call_in_a_fresh_process():
+    """The first call of a process, with no earlier launch that could have raised the kernel's
+    shared-memory limit, on a chunk that needs exactly 48 KiB of dynamic shared memory."""
+    import subprocess
+    import sys
+    from pathlib import Path
+
+    root = str(Path(__file__).resolve().parent.parent)
+    run = subprocess.run([sys.executable, "-c", FRESH_PROCESS, root], capture_output=True, text=True, timeout=300)
+    assert run.returncode == 0, run.stdout + run.stderr
+    assert "fresh" in run.stdout
