@@ -69,6 +69,17 @@ def measured_traffic(section: str, step: str, elements: int):
     return entry["bytes_per_element"] * elements if entry else None
 
 
+def measured_tensor_peak(sustained: bool = True):
+    """The measured dense bf16 tensor peak in TFLOP/s (sustained for kernels inside a long step,
+    burst for one timed alone) and where it came from."""
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        key = "bf16_tflops_sustained" if sustained and "bf16_tflops_sustained" in data else "bf16_tflops"
+        return float(data[key]), f"measured {key}"
+    return (1400.0 if sustained else 1590.0), "fallback"
+
+
 def measured_peaks():
     path = ROOT / "MEASURED_PEAKS.json"
     if path.exists():
@@ -197,7 +208,124 @@ def run_reference_arm(args, rank: int) -> int:
     return 0
 
 
-def run_product(args) -> int:
+def run_plain(args, steps: int | None = None) -> dict:
+    """The plain fused expression, float32, n = 2^20 per array: a = linspace(0, 1, n), b ~ U[-1, 1)
+    (seed 0), c = ones; each step stores t = a*b + c*2.0f and e = exponential(t)*0.5f and reduces
+    s = sum(sin(t)): three C-ABI calls, 28 B/element of algorithmic traffic (29.4 MB), so the cost
+    is per-call latency, not HBM. Device-timed steps (inputs resident), an end-to-end step through
+    the C ABI (b uploaded from pinned host memory, a and c made on the device with the creation
+    entry points, t, e and s downloaded), the outputs checked against the oracle, and libsci's CPU
+    path on the same workload (oracle/_ref, all host threads)."""
+    import torch
+
+    from libsci_b200 import chunk as C
+    from libsci_b200.device import Device
+    from libsci_b200.native import check, lib
+    from tests import _oracle
+
+    n = 1 << 20
+    steps = steps or args.steps
+    device = Device(0)
+    stream = torch.cuda.ExternalStream(device.stream)
+    b = np.random.default_rng(0).uniform(-1, 1, n).astype(np.float32)
+    da, dc = device.linspace(0.0, 1.0, n), device.ones(n)
+    db = device.array(b)
+    dt, de = device.empty(n), device.empty(n)
+    s_out = torch.zeros(1, dtype=torch.float64, device="cuda")
+    t_chunk = C.record_output(da * db + dc * 2.0)
+    e_chunk = C.record_output(C.unary("exponential", dt.expression()) * 0.5)
+    s_chunk = C.record_reduce(C.unary("sin", dt.expression()))
+
+    def step():
+        device.execute(t_chunk, dt.pointer, n)
+        device.execute(e_chunk, de.pointer, n)
+        device.reduce_async(s_chunk, C.SUM, n, s_out.data_ptr())
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    device.jit_wait()
+    step()
+    device.synchronize()
+    with ClockSampler(0) as clocks:
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(steps):
+            step()
+        stop.record(stream)
+        stop.synchronize()
+    ms = start.elapsed_time(stop) / steps
+    bytes_per_step = 28.0 * n
+
+    # end to end: b up, a and c made on the device, t, e and s down, every step
+    hb = torch.from_numpy(b).pin_memory()
+    ht, he = torch.empty(n, dtype=torch.float32).pin_memory(), torch.empty(n, dtype=torch.float32).pin_memory()
+    hs = torch.zeros(1, dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        check(lib.sci_cuda_upload(device.handle, db.pointer, hb.data_ptr(), 4 * n), device.handle)
+        check(lib.sci_cuda_linspace(device.handle, 0, da.pointer, n, 0.0, 1.0), device.handle)
+        check(lib.sci_cuda_fill(device.handle, 0, dc.pointer, n, 1.0), device.handle)
+        step()
+        check(lib.sci_cuda_download(device.handle, ht.data_ptr(), dt.pointer, 4 * n), device.handle)
+        check(lib.sci_cuda_download(device.handle, he.data_ptr(), de.pointer, 4 * n), device.handle)
+        check(lib.sci_cuda_download(device.handle, hs.data_ptr(), s_out.data_ptr(), 8), device.handle)
+
+    for _ in range(3):
+        e2e_step()
+    device.synchronize()
+    e_start, e_stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e_start.record(stream)
+    for _ in range(steps):
+        e2e_step()
+    e_stop.record(stream)
+    e_stop.synchronize()
+    e2e_ms = e_start.elapsed_time(e_stop) / steps
+
+    # check: t and e bit for bit against the oracle, s within 1e-9 of its FP64 fold
+    oracle = _oracle.port()
+    a_host = da.numpy()
+    hosts = {da.pointer: a_host, db.pointer: b, dc.pointer: np.ones(n, np.float32)}
+    t_want = _oracle.execute(oracle, _oracle.on_host(t_chunk, hosts), n, np.float32)
+    e_want = _oracle.execute(oracle, _oracle.on_host(e_chunk, {dt.pointer: t_want}), n, np.float32)
+    s_want = _oracle.reduce(oracle, _oracle.on_host(s_chunk, {dt.pointer: t_want}), C.SUM, n)
+    mismatches = int(_oracle.mismatches(ht.numpy(), t_want).size + _oracle.mismatches(he.numpy(), e_want).size)
+    s_error = abs(float(hs[0]) - s_want) / abs(s_want)
+
+    cpu = None
+    ref = _oracle.reference()
+    if ref is not None and not args.no_cpu:
+        handle = ref.sci_ref_plain_create(b.ctypes.data, np.ones(n, np.float32).ctypes.data, n)
+        for _ in range(3):
+            ref.sci_ref_plain_step(handle)
+        started = time.perf_counter()
+        for _ in range(20):
+            ref.sci_ref_plain_step(handle)
+        seconds = (time.perf_counter() - started) / 20
+        ref.sci_ref_plain_destroy(handle)
+        cpu = {"value": bytes_per_step / seconds / 1e9, "unit": "GB/s", "cores": int(ref.sci_ref_threads()),
+               "kind": "reference", "ms_per_step": seconds * 1e3,
+               "sample": "the whole workload (2^20 elements), 20 steps after 3 warm-ups, libsci public API"}
+    peak, peak_source = measured_peaks()
+    value = bytes_per_step / (ms * 1e-3) / 1e9
+    line = {"metric": "plain fused expression GB/s (t, e stored; sum(sin t))", "value": value, "unit": "GB/s",
+            "n_gpus": 1, "steps": steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "plain fused expression, float32, n=2^20: t=a*b+c*2, e=exp(t)*0.5, s=sum(sin(t))",
+                       "elements": n, "bytes_per_element": 28,
+                       "l2": "29 MB per step fits in L2: latency-bound, no flush (the bound is per-call cost)"},
+            "us_per_call": ms * 1e3 / 3,
+            "check": {"t_e_mismatches_vs_oracle": mismatches, "s_rel_error_vs_fp64_fold": s_error},
+            "roofline": {"bound": "launch latency", "achieved": value, "peak": peak, "unit": "GB/s",
+                         "frac": value / peak, "traffic": None, "peak_source": f"{peak_source} hbm_gbs",
+                         "note": "29 MB of traffic takes 4.5 us at the HBM peak; three launches cost more"},
+            "e2e": {"value": bytes_per_step / (e2e_ms * 1e-3) / 1e9, "unit": "GB/s", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": 4 * n, "d2h_bytes_per_step": 8 * n + 8},
+            "cpu_baseline": cpu, "gpu_launches": 3 * steps, "clocks": clocks.summary()}
+    device.close()
+    return line
+
+
+def run_product(args) -> dict:
     """linear::product at M = N = K (default 8192), float32 inputs ~ U[-1,1): every mode timed on the
     device (conversion to bf16 included), error against FP64 rows, reference CPU multiply sampled."""
     import torch
@@ -220,23 +348,30 @@ def run_product(args) -> int:
     for i, r in enumerate(sample_rows):
         oracle.sci_oracle_product_rows(a.ctypes.data, b.ctypes.data, want[i].ctypes.data, size, size, size, int(r), int(r) + 1)
     modes = {}
-    for mode, name in ((0, "bf16"), (1, "split_bf16"), (3, "split3_bf16"), (2, "fp32")):
-        for _ in range(args.warmup):
-            device.product(da, db, size, size, size, mode=mode, out=dc)
-        device.synchronize()
-        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        steps = args.steps if mode != 2 else max(1, args.steps // 4)
-        start.record(stream)
-        for _ in range(steps):
-            device.product(da, db, size, size, size, mode=mode, out=dc)
-        stop.record(stream)
-        stop.synchronize()
-        ms = start.elapsed_time(stop) / steps
-        got = dc.numpy().reshape(size, size)[sample_rows]
-        err = np.abs(got - want)
-        modes[name] = {"ms": ms, "TFLOP/s": flops / (ms * 1e-3) / 1e12, "frac_of_bf16_peak": flops / (ms * 1e-3) / 1e12 / peak,
-                       "tensor_TFLOP/s": {0: 1, 1: 3, 3: 6}.get(mode, 0) * flops / (ms * 1e-3) / 1e12 if mode != 2 else None,
-                       "max_abs_err": float(err.max()), "rel_fro_err": float(np.linalg.norm(err) / np.linalg.norm(want))}
+    # |C - C64| <= (u_mode + k 2^-22) (|A| |B|) per element (tests/test_product_gpu.py)
+    scale = np.abs(a[sample_rows].astype(np.float64)) @ np.abs(b.astype(np.float64))
+    unit = {0: 2.0 ** -7, 1: 2.0 ** -14, 3: 2.0 ** -21, 2: 0.0}
+    with ClockSampler(0) as clocks:
+        for mode, name in ((0, "bf16"), (1, "split_bf16"), (3, "split3_bf16"), (2, "fp32")):
+            for _ in range(args.warmup):
+                device.product(da, db, size, size, size, mode=mode, out=dc)
+            device.synchronize()
+            start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            steps = args.steps if mode != 2 else max(1, args.steps // 4)
+            start.record(stream)
+            for _ in range(steps):
+                device.product(da, db, size, size, size, mode=mode, out=dc)
+            stop.record(stream)
+            stop.synchronize()
+            ms = start.elapsed_time(stop) / steps
+            got = dc.numpy().reshape(size, size)[sample_rows]
+            err = np.abs(got - want)
+            bound = (unit[mode] + (2.0 ** -23 if mode == 2 else 2.0 ** -22) * size) * scale
+            modes[name] = {"ms": ms, "TFLOP/s": flops / (ms * 1e-3) / 1e12,
+                           "frac_of_bf16_peak": flops / (ms * 1e-3) / 1e12 / peak,
+                           "tensor_TFLOP/s": {0: 1, 1: 3, 3: 6}.get(mode, 0) * flops / (ms * 1e-3) / 1e12 if mode != 2 else None,
+                           "max_abs_err": float(err.max()), "rel_fro_err": float(np.linalg.norm(err) / np.linalg.norm(want)),
+                           "within_bound": bool(np.all(err <= bound))}
     cpu = None
     ref = _oracle.reference()
     if ref is not None and not args.no_cpu:
@@ -257,10 +392,11 @@ def run_product(args) -> int:
             "modes": modes,
             "roofline": {"bound": "tensor", "achieved": best["TFLOP/s"], "peak": peak, "unit": "TFLOP/s",
                          "frac": best["TFLOP/s"] / peak, "traffic": None, "peak_source": "measured bf16_tflops (burst)"},
-            "cpu_baseline": cpu, "gpu_launches": 3 * args.steps}  # per bf16 product: two conversions + one GEMM
-    print(json.dumps(line))
+            "check": {name: {"within_bound": m["within_bound"], "rel_fro_err": m["rel_fro_err"]} for name, m in modes.items()},
+            "cpu_baseline": cpu, "gpu_launches": 3 * args.steps,  # per bf16 product: two conversions + one GEMM
+            "clocks": clocks.summary()}
     device.close()
-    return 0
+    return line
 
 
 def torch_solve(torch, a, b, args):
@@ -286,7 +422,7 @@ def torch_solve(torch, a, b, args):
     return {"ms": statistics.median(times), "backward_error": float(berr.max())}
 
 
-def run_solve(args) -> int:
+def run_solve(args) -> dict:
     """linear::solve at n = 8192 with 16 right-hand sides ~ N(0,1), for A = G + n I and A = G
     (G ~ N(0,1)): FP32 LU + FP64 refinement against plain FP64 LU on the same GPU, both to a
     normwise backward error <= 1e-14; libsci's CPU solve<double> timed once on a 2048 sample."""
@@ -300,6 +436,8 @@ def run_solve(args) -> int:
     stream = torch.cuda.ExternalStream(device.stream)
     flops = 2.0 / 3.0 * n ** 3 + 2.0 * n * n * width
     cases = {}
+    clocks = ClockSampler(0)
+    clocks.__enter__()
     for name, shift in (("G+nI", True), ("G", False)):
         rng = np.random.default_rng(17 + int(shift))
         a = rng.standard_normal((n, n)) + (n * np.eye(n) if shift else 0.0)
@@ -321,7 +459,10 @@ def run_solve(args) -> int:
             result[label] = {"ms": ms, "GFLOP/s": flops / (ms * 1e-3) / 1e9, "backward_error": berr,
                              "iterations": iterations}
         result["speedup_refined_vs_fp64"] = result["fp64_lu"]["ms"] / result["fp32_lu_fp64_refine"]["ms"]
-        result["external_torch_linalg_solve_fp64"] = torch_solve(torch, a, b, args)
+        result["check"] = {"backward_error_le_1e-14": bool(result["fp32_lu_fp64_refine"]["backward_error"] <= 1e-14
+                                                           and result["fp64_lu"]["backward_error"] <= 1e-14)}
+        if not getattr(args, "compact", False):
+            result["external_torch_linalg_solve_fp64"] = torch_solve(torch, a, b, args)
         cases[name] = result
         for arr in (da, db, dx):
             arr.free()
@@ -339,18 +480,30 @@ def run_solve(args) -> int:
         cpu = {"value": (2.0 / 3.0 * m ** 3 + 2.0 * m * m * width) / seconds / 1e9, "unit": "GFLOP/s",
                "cores": int(ref.sci_ref_threads()), "kind": "reference",
                "sample": "libsci solve<double> (factor + substitute) at n=2048, 16 RHS, timed once"}
+    clocks.__exit__(None, None, None)
     headline = cases["G+nI"]["fp32_lu_fp64_refine"]
+    # The refined solve's work rate against what its arithmetic can reach: the FP32 trailing
+    # updates run on the tensor cores as six bf16 products (split3), so the FP32-accurate tensor
+    # rate is the measured bf16 peak / 6; the rest (panels, substitutions, FP64 residuals) is
+    # latency-bound.
+    tensor_peak = measured_tensor_peak()
+    achieved = flops / (headline["ms"] * 1e-3) / 1e12
     line = {"metric": "solve speedup vs plain FP64 LU at equal backward error", "value": cases["G+nI"]["speedup_refined_vs_fp64"],
             "unit": "x", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": headline["ms"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 LU + f64 refinement",
             "data": "synthetic", "config": {"workload": f"solve n={n}, 16 RHS ~ N(0,1); A=G+nI and A=G"},
-            "cases": cases, "cpu_baseline": cpu}
-    print(json.dumps(line))
+            "cases": cases, "cpu_baseline": cpu,
+            "check": {name: case["check"] for name, case in cases.items()},
+            "roofline": {"bound": "tensor (split3 trailing update) + latency (panel chain)", "achieved": achieved,
+                         "peak": tensor_peak[0] / 6, "unit": "TFLOP/s", "frac": achieved / (tensor_peak[0] / 6),
+                         "traffic": None, "peak_source": f"{tensor_peak[1]} / 6 (six bf16 products per FP32-accurate one)",
+                         "work": "2/3 n^3 + 2 n^2 nrhs per factor + solve"},
+            "clocks": clocks.summary()}
     device.close()
-    return 0
+    return line
 
 
-def run_gradient(args) -> int:
+def run_gradient(args) -> dict:
     """sci::gradient workloads. Chunk: L = sum(exponential(-a*a)*sin(b) + logarithm(1+c*c)), float32,
     n = 2^26 per array, a,b,c ~ N(0,1): the recomputing adjoint against the temporary-storing one,
     each timed on the device (inputs 256 MiB each, above L2), gradients checked against the closed
@@ -497,9 +650,8 @@ def run_gradient(args) -> int:
                          "frac": chunk_result["recompute"]["frac_of_peak"], "traffic": None,
                          "peak_source": peak_source},
             "cpu_baseline": cpu, "gpu_launches": args.steps, "clocks": clocks.summary()}
-    print(json.dumps(line))
     device.close()
-    return 0
+    return line
 
 
 def batch_chunk(C, precision=0):
@@ -518,7 +670,7 @@ def batch_chunk(C, precision=0):
     return chunk
 
 
-def run_batch(args) -> int:
+def run_batch(args) -> dict:
     """Batching: 8192 float32 instances of t = a*b + c, r = sum(tanh(t)), lengths log-uniform in
     [256, 2^20] (seeded), a, b, c ~ N(0,1), in one persistent launch replayed from a CUDA graph.
     Beside it: the plain form, a loop of single calls through the C ABI (execute t, reduce
@@ -649,13 +801,12 @@ def run_batch(args) -> int:
             "roofline": {"bound": "hbm", "achieved": bytes_moved / (ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": bytes_moved / (ms * 1e-3) / 1e9 / peak, "traffic": None, "peak_source": peak_source},
             "cpu_baseline": cpu, "gpu_launches": args.steps, "clocks": clocks.summary()}
-    print(json.dumps(line))
     batch.close()
     device.close()
-    return 0
+    return line
 
 
-def run_solves(args) -> int:
+def run_solves(args) -> dict:
     """Batching of solves: 4096 independent systems, n ~ U[8, 256] (seeded), A = G + n I (G ~ N(0,1)),
     one right-hand side ~ N(0,1), FP32 LU + FP64 refinement, one graph replay (block size tuned per
     order bucket). Beside it: a loop of single sci_cuda_solve calls (the plain form, sampled) and
@@ -753,13 +904,12 @@ def run_solves(args) -> int:
                          "note": "A is read twice (FP32 copy + FP64 residuals from L2): "
                                  f"{2 * int(offsets_a[-1]) * 8 / (ms * 1e-3) / 1e9:.0f} GB/s of HBM for A"},
             "cpu_baseline": cpu, "gpu_launches": 4 * args.steps, "clocks": clocks.summary()}
-    print(json.dumps(line))
     batch.close()
     device.close()
-    return 0
+    return line
 
 
-def run_creation(args) -> int:
+def run_creation(args) -> dict:
     """Arrays made on the device (include/operations/creation.hpp): full, linspace, range and eye of
     2^28 float32 elements (1 GiB each), grid of 16384 x 16384 (two 1 GiB outputs), and transpose
     (manipulations.hpp) of a 16384 x 16384 matrix; one step = all six. Bound by HBM: 4 B/element
@@ -840,12 +990,11 @@ def run_creation(args) -> int:
             "roofline": {"bound": "hbm", "achieved": per[top]["GB/s"], "peak": peak, "unit": "GB/s",
                          "frac": per[top]["frac"], "traffic": None, "kernel": top, "peak_source": peak_source},
             "cpu_baseline": cpu, "gpu_launches": len(steps) * args.steps, "clocks": clocks.summary()}
-    print(json.dumps(line))
     device.close()
-    return 0
+    return line
 
 
-def run_elements(args) -> int:
+def run_elements(args) -> dict:
     """Integer-element chunks (sci_cuda_execute_elements / reduce_elements), the expressions libsci
     evaluates on the host for non-native element types (include/array/expression.hpp:178-184,
     203-220): int32 t = a*b + c, maximum(a, c) / b and sum(a*b) over 2^28 elements (1 GiB per
@@ -945,12 +1094,11 @@ def run_elements(args) -> int:
                          "frac": per[top]["frac"], "traffic": measured_traffic("elements", top, top_elements),
                          "kernel": f"element_stream ({top})", "peak_source": peak_source},
             "cpu_baseline": cpu, "gpu_launches": (len(steps) + 1) * args.steps, "clocks": clocks.summary()}
-    print(json.dumps(line))
     device.close()
-    return 0
+    return line
 
 
-def run_shapes(args) -> int:
+def run_shapes(args) -> dict:
     """Broadcasting, the roadmap's elementwise functions and axis reductions (libsci's README.md:
     149-152, numpy's rules): over 16384 x 16384 float32 (1 GiB per full array), one step =
     (16384,1) + (1,16384); where((16384,1), x, y); clip(x, -1, 1); power(x, 2.5); floor(x); sum of
@@ -1058,15 +1206,14 @@ def run_shapes(args) -> int:
             "fp64_bound": {"step": "power(x, 2.5)", "ms": per["power(x, 2.5)"]["ms"],
                            "note": "a double-precision pow per element; bound by the FP64 pipe, not HBM"},
             "cpu_baseline": cpu, "gpu_launches": 8 * args.steps, "clocks": clocks.summary()}
-    print(json.dumps(line))
     device.close()
-    return 0
+    return line
 
 
 def main() -> int:
     parser = argparse.ArgumentParser()
     parser.add_argument("--workload", default="chunks",
-                        choices=["chunks", "product", "solve", "gradient", "batch", "solves", "creation",
+                        choices=["chunks", "plain", "product", "solve", "gradient", "batch", "solves", "creation",
                                  "elements", "shapes"])
     parser.add_argument("--size", type=int, default=8192)
     parser.add_argument("--gpus", type=int, default=1)
@@ -1078,6 +1225,8 @@ def main() -> int:
     parser.add_argument("--e2e-pieces", type=int, default=8,
                         help="pieces the end-to-end step streams through the copy lanes")
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    parser.add_argument("--no-extras", action="store_true",
+                        help="default workload only: skip the other workloads' summaries in the line")
     parser.add_argument("--small", action="store_true",
                         help="elements / shapes workloads at a quarter size (for profiler captures)")
     parser.add_argument("--items", type=int, default=8192, help="batch workload: instances")
@@ -1090,22 +1239,12 @@ def main() -> int:
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference_arm(args, rank)
-    if args.workload == "product":
-        return run_product(args)
-    if args.workload == "solve":
-        return run_solve(args)
-    if args.workload == "gradient":
-        return run_gradient(args)
-    if args.workload == "batch":
-        return run_batch(args)
-    if args.workload == "elements":
-        return run_elements(args)
-    if args.workload == "shapes":
-        return run_shapes(args)
-    if args.workload == "creation":
-        return run_creation(args)
-    if args.workload == "solves":
-        return run_solves(args)
+    single = {"plain": run_plain, "product": run_product, "solve": run_solve, "gradient": run_gradient,
+              "batch": run_batch, "elements": run_elements, "shapes": run_shapes, "creation": run_creation,
+              "solves": run_solves}
+    if args.workload in single:
+        print(json.dumps(single[args.workload](args)))
+        return 0
 
     import torch
 
@@ -1315,11 +1454,57 @@ def main() -> int:
             "gpu_launches": len(names) * args.steps,
             "clocks": clocks.summary(),
         }
-        print(json.dumps(line))
     device.close()
+    del dx, dy, dz, stored, lower, upper
+    torch.cuda.empty_cache()
+    if rank == 0:
+        if world == 1 and not args.no_extras:
+            line["configs"] = run_extras(args)
+        print(json.dumps(line))
     if dist is not None:
         dist.destroy_process_group()
     return 0
+
+
+def compact(line: dict, *extra: str) -> dict:
+    """The keys of a workload's line that the default run carries for it."""
+    keys = ("metric", "value", "unit", "ms_per_step", "higher_is_better", "roofline", "check", "clocks", "e2e",
+            "gpu_launches") + extra
+    out = {k: line[k] for k in keys if k in line}
+    if line.get("cpu_baseline"):
+        out["cpu_baseline"] = {k: line["cpu_baseline"][k] for k in ("value", "unit", "cores", "kind", "sample")
+                               if k in line["cpu_baseline"]}
+    out["workload"] = line.get("config", {}).get("workload")
+    return out
+
+
+def run_extras(args) -> dict:
+    """Every other workload of the benchmark at its full size, with fewer timed steps: the plain
+    fused expression (n = 2^20), the product (8192^3, every mode), the solve (n = 8192, 16
+    right-hand sides, both matrices), the gradients (2^26; 4096 x 64 solve) and both batches, each
+    with its own device time, roofline, clocks and check against the oracle."""
+    import copy
+
+    import torch
+
+    extra = copy.copy(args)
+    extra.steps, extra.warmup, extra.compact = max(3, min(args.steps, 5)), 3, True
+    out = {}
+    for key, run, keep in (("plain_n2e20", run_plain, ("us_per_call",)),
+                           ("product_8192", run_product, ("modes",)),
+                           ("solve_8192", run_solve, ("cases",)),
+                           ("gradient", run_gradient, ("chunk", "solve")),
+                           ("batch_8192_items", run_batch, ("batch",)),
+                           ("solves_4096", run_solves, ("solves",))):
+        started = time.perf_counter()
+        try:
+            line = run(extra)
+            out[key] = compact(line, *keep)
+        except Exception as error:  # noqa: BLE001 - reported in the line, the headline stands
+            out[key] = {"error": f"{type(error).__name__}: {error}"}
+        out[key]["wall_s"] = time.perf_counter() - started
+        torch.cuda.empty_cache()
+    return out
 
 
 if __name__ == "__main__":

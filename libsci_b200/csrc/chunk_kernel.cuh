@@ -115,8 +115,27 @@ namespace sci_cuda {
     // it has a paired form), and a thread with any lane outside the fast form's inputs recomputes all
     // its lanes with the full form: one branch per thread, taken only for such inputs, and the same
     // values either way.
+    //
+    // Float tanh has a second fast form for |x| <= 1 (tanh_float_near: a polynomial instead of the
+    // exponential and the quotient), taken when every lane of every active thread of the warp is in
+    // that range (one vote, so a warp never runs both forms); its results are the same bits.
     template <int code, bool fast = false, typename T>
     __device__ __forceinline__ void apply_lanes(const T *a, const T *b, const T *c, T *r, const bool *tail) {
+        if constexpr (fast && code == kTanh && sizeof(T) == 4) {
+            bool near = true;
+#pragma unroll
+            for (int e = 0; e < Lanes<T>::count; ++e) near = near && fabsf(a[e]) <= 1.0f;  // false for NaN
+            if (__all_sync(__activemask(), near)) {
+                bool rare = false;
+#pragma unroll
+                for (int e = 0; e < Lanes<T>::count; ++e) r[e] = tanh_float_near(a[e], rare);
+                if (rare) {
+#pragma unroll
+                    for (int e = 0; e < Lanes<T>::count; ++e) r[e] = apply<code>(a[e], b[e], c[e], tail[e]);
+                }
+                return;
+            }
+        }
         if constexpr (fast && has_fast<code, T>()) {
             bool rare = false;
             if constexpr (has_pair<code, T>()) {

@@ -185,10 +185,12 @@ namespace sci_cuda {
     // Row-major GEMMs on submatrices (product.cu): C (pitch ldc) = A (pitch lda) * B (pitch ldb),
     // or C -= A * B with `subtract`. tensor_gemm splits each operand into `terms` (1-3) bf16 parts
     // and multiplies on the tensor cores; simt_gemm is the plain FP32 / FP64 form. Both queue on
-    // ctx.stream.
+    // ctx.stream. `whole_gpu`: the product has the GPU to itself, so products of 256 rows or more
+    // run on the persistent CTA-pair kernel (a static split of the tiles over every SM); the LU's
+    // updates, which share the GPU with the panels, keep the one-tile-per-CTA kernel.
     int tensor_gemm(Context &ctx, int terms, const float *a, unsigned long long lda, const float *b,
                     unsigned long long ldb, float *c, unsigned long long ldc, unsigned long long m, unsigned long long n,
-                    unsigned long long k, bool subtract);
+                    unsigned long long k, bool subtract, bool whole_gpu = false);
     template <typename T>
     int simt_gemm(Context &ctx, const T *a, unsigned long long lda, const T *b, unsigned long long ldb, T *c,
                   unsigned long long ldc, unsigned long long m, unsigned long long n, unsigned long long k, bool subtract);
@@ -196,7 +198,7 @@ namespace sci_cuda {
     // that B is stored n x k (pitch ldb).
     int tensor_gemm_t(Context &ctx, int terms, const float *a, unsigned long long lda, bool a_t, const float *b,
                       unsigned long long ldb, bool b_t, float *c, unsigned long long ldc, unsigned long long m,
-                      unsigned long long n, unsigned long long k, bool subtract);
+                      unsigned long long n, unsigned long long k, bool subtract, bool whole_gpu = false);
     template <typename T>
     int simt_gemm_t(Context &ctx, const T *a, unsigned long long lda, bool a_t, const T *b, unsigned long long ldb, bool b_t,
                     T *c, unsigned long long ldc, unsigned long long m, unsigned long long n, unsigned long long k,

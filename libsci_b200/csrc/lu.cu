@@ -142,18 +142,30 @@ namespace sci_cuda {
             static constexpr int value = N;
         };
 
-        // The panel runs on one thread-block cluster of CL CTAs (8, the portable size, or 16 where the
-        // GPU can co-schedule them) of 512 threads; CTA c holds rows [8192 c / CL, 8192 (c + 1) / CL)
-        // of the panel, 8192 / (512 CL) rows per thread.
+        // The panel runs on one thread-block cluster of CL CTAs of 512 threads covering ROWS rows from
+        // the panel's first: CTA c holds rows [ROWS c / CL, ROWS (c + 1) / CL), ROWS / (512 CL) rows
+        // per thread. The full panel (ROWS = 8192) takes 8 CTAs, the portable size, or 16 where the
+        // GPU can co-schedule them; a panel with fewer rows below its diagonal takes the smallest
+        // cluster of 1, 2, 4 or 8 CTAs that holds them at one row per thread, so its per-column
+        // exchange involves fewer CTAs (one CTA exchanges nothing across SMs).
         constexpr int kPanelBlock = 512;
-        template <int CL> struct PanelShape {
-            static constexpr int rows = static_cast<int>(kPanelRows) / CL;  // rows per CTA
+        template <int CL, int ROWS = static_cast<int>(kPanelRows)> struct PanelShape {
+            static constexpr int rows = ROWS / CL;  // rows per CTA
             static constexpr int per_thread = rows / kPanelBlock;
+            static_assert(per_thread >= 1 && rows % kPanelBlock == 0, "whole rows per thread");
         };
         // Dynamic shared memory of panel_factor: the staged multipliers, W x (rows per CTA + 1).
-        template <typename T, int CL> constexpr size_t panel_shared_bytes() {
-            return sizeof(T) * PanelWidth<T>::value * (PanelShape<CL>::rows + 1);
+        template <typename T, int CL, int ROWS = static_cast<int>(kPanelRows)> constexpr size_t panel_shared_bytes() {
+            return sizeof(T) * PanelWidth<T>::value * (PanelShape<CL, ROWS>::rows + 1);
         }
+
+        // Programmatic dependent launch along the factorisation's critical path: a kernel launched
+        // with programmatic stream serialization (launch_chained) may start while the kernel before
+        // it on the stream is still running; chain_wait() returns once that kernel has finished and
+        // its writes are visible, and chain_release() lets the kernel after this one start. Both are
+        // no-ops in a kernel launched the ordinary way.
+        __device__ __forceinline__ void chain_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+        __device__ __forceinline__ void chain_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
         __device__ __forceinline__ void named_sync(unsigned id, unsigned count) {
             asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
@@ -200,12 +212,12 @@ namespace sci_cuda {
         // to fill (a bounded wait), picks the pivot, and one CTA barrier hands it to every thread.
         // Inboxes alternate by column parity; a CTA sends into one again only after its own pivot
         // decision of the column in between, which needed every CTA's message of that column.
-        template <typename T, int CL>
+        template <typename T, int CL, int ROWS>
         __global__ void __launch_bounds__(kPanelBlock, 1)
                 panel_factor(T *a, unsigned long long n, unsigned long long j0, int width, long long *piv, Movement *moved,
                              int *status) {
-            constexpr int kClusterCtas = CL, kCtaRows = PanelShape<CL>::rows;
-            constexpr int W = PanelWidth<T>::value, R = PanelShape<CL>::per_thread, TH = kPanelBlock, WARPS = TH / 32;
+            constexpr int kClusterCtas = CL, kCtaRows = PanelShape<CL, ROWS>::rows;
+            constexpr int W = PanelWidth<T>::value, R = PanelShape<CL, ROWS>::per_thread, TH = kPanelBlock, WARPS = TH / 32;
             constexpr int P = kCtaRows + 1;  // pitch of the staged multipliers
             extern __shared__ __align__(16) unsigned char panel_shared[];
             T *stage = reinterpret_cast<T *>(panel_shared);  // stage[k * P + local row]
@@ -229,6 +241,8 @@ namespace sci_cuda {
             __shared__ unsigned long long pivot_at, pivot_origin, displaced_origin;
             __shared__ long long exchanges[W];  // CTA 0: piv[j0 + j]
 
+            chain_wait();
+            chain_release();
             const unsigned c = cluster_rank(), t = threadIdx.x, lane = t % 32, warp = t / 32;
             const unsigned long long first = j0 + 1ull * c * kCtaRows;  // this CTA's first row
             unsigned long long r[R], origin[R];
@@ -502,23 +516,73 @@ namespace sci_cuda {
             }
         }
 
-        // Launches panel_factor<T, CL> as one cluster of CL CTAs.
-        template <typename T, int CL>
+        // Launches panel_factor<T, CL, ROWS> as one cluster of CL CTAs (chained: see chain_wait).
+        template <typename T, int CL, int ROWS = static_cast<int>(kPanelRows)>
         cudaError_t launch_panel(cudaStream_t stream, T *a, unsigned long long n, unsigned long long j0, int w, long long *piv,
-                                 Movement *moved, int *status) {
+                                 Movement *moved, int *status, bool chained = false) {
             cudaLaunchConfig_t config{};
             config.gridDim = dim3(CL);
             config.blockDim = dim3(kPanelBlock);
-            config.dynamicSmemBytes = panel_shared_bytes<T, CL>();
+            config.dynamicSmemBytes = panel_shared_bytes<T, CL, ROWS>();
             config.stream = stream;
-            cudaLaunchAttribute attribute[1];
+            cudaLaunchAttribute attribute[2];
             attribute[0].id = cudaLaunchAttributeClusterDimension;
             attribute[0].val.clusterDim.x = CL;
             attribute[0].val.clusterDim.y = 1;
             attribute[0].val.clusterDim.z = 1;
+            attribute[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attribute[1].val.programmaticStreamSerializationAllowed = 1;
+            config.attrs = attribute;
+            config.numAttrs = chained ? 2 : 1;
+            return cudaLaunchKernelEx(&config, panel_factor<T, CL, ROWS>, a, n, j0, w, piv, moved, status);
+        }
+
+        // Raises the dynamic shared-memory limit of the short panels (one row per thread) once.
+        template <typename T> void prepare_short_panels() {
+            static const bool done = [] {
+                cudaFuncSetAttribute(reinterpret_cast<const void *>(&panel_factor<T, 1, 512>),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(panel_shared_bytes<T, 1, 512>()));
+                cudaFuncSetAttribute(reinterpret_cast<const void *>(&panel_factor<T, 2, 1024>),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(panel_shared_bytes<T, 2, 1024>()));
+                cudaFuncSetAttribute(reinterpret_cast<const void *>(&panel_factor<T, 4, 2048>),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(panel_shared_bytes<T, 4, 2048>()));
+                cudaFuncSetAttribute(reinterpret_cast<const void *>(&panel_factor<T, 8, 4096>),
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, int(panel_shared_bytes<T, 8, 4096>()));
+                return true;
+            }();
+            (void)done;
+        }
+
+        // The panel at columns [j0, j0 + w): the smallest cluster that holds its n - j0 rows at one
+        // row per thread, or the full panel's cluster (`cluster` CTAs, 8192 rows).
+        template <typename T>
+        cudaError_t launch_panel_for(int cluster, cudaStream_t stream, T *a, unsigned long long n, unsigned long long j0, int w,
+                                     long long *piv, Movement *moved, int *status, bool chained) {
+            const unsigned long long rows = n - j0;
+            prepare_short_panels<T>();
+            if (rows <= 512) return launch_panel<T, 1, 512>(stream, a, n, j0, w, piv, moved, status, chained);
+            if (rows <= 1024) return launch_panel<T, 2, 1024>(stream, a, n, j0, w, piv, moved, status, chained);
+            if (rows <= 2048) return launch_panel<T, 4, 2048>(stream, a, n, j0, w, piv, moved, status, chained);
+            if (rows <= 4096 && cluster == 16) return launch_panel<T, 8, 4096>(stream, a, n, j0, w, piv, moved, status, chained);
+            return cluster == 16 ? launch_panel<T, 16>(stream, a, n, j0, w, piv, moved, status, chained)
+                                 : launch_panel<T, 8>(stream, a, n, j0, w, piv, moved, status, chained);
+        }
+
+        // Launches `kernel` on `stream` with programmatic stream serialization, for kernels that
+        // call chain_wait() before reading what the kernel before them wrote.
+        template <typename... Params, typename... Args>
+        cudaError_t launch_chained(void (*kernel)(Params...), dim3 grid, dim3 block, cudaStream_t stream, Args... args) {
+            cudaLaunchConfig_t config{};
+            config.gridDim = grid;
+            config.blockDim = block;
+            config.dynamicSmemBytes = 0;
+            config.stream = stream;
+            cudaLaunchAttribute attribute[1];
+            attribute[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attribute[0].val.programmaticStreamSerializationAllowed = 1;
             config.attrs = attribute;
             config.numAttrs = 1;
-            return cudaLaunchKernelEx(&config, panel_factor<T, CL>, a, n, j0, w, piv, moved, status);
+            return cudaLaunchKernelEx(&config, kernel, static_cast<Params>(args)...);
         }
 
         // The panel's cluster size for this process: 16 CTAs (half the rows per SM, a non-portable
@@ -527,12 +591,11 @@ namespace sci_cuda {
         template <typename T> int panel_cluster() {
             static const int chosen = [] {
                 const int smem8 = static_cast<int>(panel_shared_bytes<T, 8>()), smem16 = static_cast<int>(panel_shared_bytes<T, 16>());
-                cudaFuncSetAttribute(reinterpret_cast<const void *>(&panel_factor<T, 8>),
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem8);
-                cudaFuncSetAttribute(reinterpret_cast<const void *>(&panel_factor<T, 16>),
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem16);
-                cudaFuncSetAttribute(reinterpret_cast<const void *>(&panel_factor<T, 16>),
-                                     cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+                const void *full8 = reinterpret_cast<const void *>(&panel_factor<T, 8, static_cast<int>(kPanelRows)>);
+                const void *full16 = reinterpret_cast<const void *>(&panel_factor<T, 16, static_cast<int>(kPanelRows)>);
+                cudaFuncSetAttribute(full8, cudaFuncAttributeMaxDynamicSharedMemorySize, smem8);
+                cudaFuncSetAttribute(full16, cudaFuncAttributeMaxDynamicSharedMemorySize, smem16);
+                cudaFuncSetAttribute(full16, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
                 auto schedulable = [](const void *kernel, int cl, int smem) {
                     cudaLaunchConfig_t config{};
                     config.gridDim = dim3(cl);
@@ -552,8 +615,8 @@ namespace sci_cuda {
                     }
                     return clusters >= 1;
                 };
-                const bool can16 = schedulable(reinterpret_cast<const void *>(&panel_factor<T, 16>), 16, smem16);
-                const bool can8 = schedulable(reinterpret_cast<const void *>(&panel_factor<T, 8>), 8, smem8);
+                const bool can16 = schedulable(full16, 16, smem16);
+                const bool can8 = schedulable(full8, 8, smem8);
                 const char *asked = std::getenv("SCI_CUDA_PANEL_CLUSTER");
                 if (asked && std::atoi(asked) == 8 && can8) return 8;
                 if (can16) return 16;
@@ -567,6 +630,8 @@ namespace sci_cuda {
         template <typename T>
         __global__ void move_rows(T *a, unsigned long long n, const Movement *moved, unsigned long long c0,
                                   unsigned long long c1, unsigned long long skip0, unsigned long long skip1) {
+            chain_wait();
+            chain_release();
             const unsigned long long col = c0 + blockIdx.x * 256ull + threadIdx.x;
             if (col >= c1 || (col >= skip0 && col < skip1)) return;
             const int count = static_cast<int>(moved->count);
@@ -636,6 +701,8 @@ namespace sci_cuda {
             constexpr int BM = 64, BK = 32, TN = BN / 16, LA = BM * BK / 256, LB = BK * BN / 256;
             __shared__ T as[BK][BM + 1];
             __shared__ T bs[BK][BN + 1];
+            chain_wait();
+            chain_release();
             const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
             const unsigned long long m0 = blockIdx.y * 1ull * BM, n0 = blockIdx.x * 1ull * BN;
             T acc[4][TN];
@@ -702,15 +769,23 @@ namespace sci_cuda {
 
         template <typename T>
         int update(Context &ctx, const T *a, unsigned long long lda, const T *b, unsigned long long ldb, T *c,
-                   unsigned long long ldc, unsigned long long m, unsigned long long n, unsigned long long k) {
+                   unsigned long long ldc, unsigned long long m, unsigned long long n, unsigned long long k,
+                   bool chained = false) {
             if (m == 0 || n == 0 || k == 0) return SCI_CUDA_OK;
             if ((m + 63) / 64 > 65535) return ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "update: too many rows");
-            if (n <= 16) {
-                rank_update<T, 16><<<dim3(static_cast<unsigned>((n + 15) / 16), static_cast<unsigned>((m + 63) / 64)), 256, 0,
-                                     ctx.stream>>>(a, lda, b, ldb, c, ldc, m, n, k);
+            const bool narrow = n <= 16;
+            const dim3 grid(static_cast<unsigned>(narrow ? (n + 15) / 16 : (n + 63) / 64), static_cast<unsigned>((m + 63) / 64));
+            if (chained) {
+                const cudaError_t launched = narrow ? launch_chained(rank_update<T, 16>, grid, dim3(256), ctx.stream, a, lda, b,
+                                                                     ldb, c, ldc, m, n, k)
+                                                    : launch_chained(rank_update<T, 64>, grid, dim3(256), ctx.stream, a, lda, b,
+                                                                     ldb, c, ldc, m, n, k);
+                return ctx.check(launched, "launching a rank update");
+            }
+            if (narrow) {
+                rank_update<T, 16><<<grid, 256, 0, ctx.stream>>>(a, lda, b, ldb, c, ldc, m, n, k);
             } else {
-                rank_update<T, 64><<<dim3(static_cast<unsigned>((n + 63) / 64), static_cast<unsigned>((m + 63) / 64)), 256, 0,
-                                     ctx.stream>>>(a, lda, b, ldb, c, ldc, m, n, k);
+                rank_update<T, 64><<<grid, 256, 0, ctx.stream>>>(a, lda, b, ldb, c, ldc, m, n, k);
             }
             return ctx.check(cudaGetLastError(), "launching a rank update");
         }
@@ -723,6 +798,8 @@ namespace sci_cuda {
             constexpr int W = PanelWidth<T>::value;
             constexpr int threads = 128, L = W * W / threads;
             __shared__ T lower[W][W];
+            chain_wait();
+            chain_release();
             const unsigned long long col = c0 + blockIdx.x * 1ull * threads + threadIdx.x;
             // every global load of the thread is issued before the first shared store
             T staged[L], x[W];
@@ -1202,22 +1279,32 @@ namespace sci_cuda {
                 for (unsigned long long j0 = J0; j0 < block_end; j0 += W, ++panels) {
                     const int w = static_cast<int>(std::min<unsigned long long>(W, block_end - j0));
                     Movement *mine = moved + panels;
-                    const cudaError_t launched = cluster == 16 ? launch_panel<T, 16>(ctx.stream, a, n, j0, w, piv, mine, ctx.status)
-                                                               : launch_panel<T, 8>(ctx.stream, a, n, j0, w, piv, mine, ctx.status);
+                    // Within a block, each kernel of the chain panel -> row moves -> U rows -> rank
+                    // update -> next panel follows the one before it directly on the stream, so it is
+                    // launched chained (programmatic dependent launch): its launch overlaps the end of
+                    // its predecessor. The block's first panel follows other work and waits plainly.
+                    const bool chained = j0 != J0;
+                    const cudaError_t launched =
+                            launch_panel_for<T>(cluster, ctx.stream, a, n, j0, w, piv, mine, ctx.status, chained);
                     if (int code = ctx.check(launched, "launching the panel factorisation")) return code;
                     // the panel's row movement: now inside the block (everywhere without look-ahead)
                     const unsigned long long m0 = ahead ? J0 : 0, m1 = ahead ? block_end : n;
-                    move_rows<T><<<static_cast<unsigned>((m1 - m0 + 255) / 256), 256, 0, ctx.stream>>>(a, n, mine, m0, m1, j0,
-                                                                                                      j0 + w);
+                    if (int code = ctx.check(launch_chained(move_rows<T>, dim3(static_cast<unsigned>((m1 - m0 + 255) / 256)),
+                                                            dim3(256), ctx.stream, a, n, mine, m0, m1, j0, j0 + w),
+                                             "launching the panel's row moves"))
+                        return code;
                     // Inside the outer block only: U rows of the panel, then the rows below it. Columns
                     // beyond the block wait until the block's pivots are all known (a later pivot of
                     // this block may still bring a row up from below).
                     const unsigned long long right = j0 + w;
                     if (right < block_end) {
-                        trsm_rows<T><<<static_cast<unsigned>((block_end - right + 127) / 128), 128, 0, ctx.stream>>>(
-                                a, n, j0, w, right, block_end);
+                        if (int code = ctx.check(launch_chained(trsm_rows<T>,
+                                                                dim3(static_cast<unsigned>((block_end - right + 127) / 128)),
+                                                                dim3(128), ctx.stream, a, n, j0, w, right, block_end),
+                                                 "launching the panel's U rows"))
+                            return code;
                         if (int code = update<T>(ctx, a + right * n + j0, n, a + j0 * n + right, n, a + right * n + right, n,
-                                                 n - right, block_end - right, w))
+                                                 n - right, block_end - right, w, true))
                             return code;
                     }
                     if (int code = ctx.check(cudaGetLastError(), "launching the panel updates")) return code;

@@ -28,7 +28,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 namespace sci_cuda {
 
@@ -303,6 +306,263 @@ namespace sci_cuda {
             }
         }
 
+        // ---- the persistent CTA-pair kernel -----------------------------------------------------------
+        // Two CTAs of a cluster compute 256 x 256 tiles of C together with tcgen05.mma.cta_group::2
+        // (M = 256): each CTA stages 128 rows of A and 128 rows of B^T per term and holds 128 rows of
+        // the FP32 accumulator in its own tensor memory, so each byte of B a CTA stages feeds twice
+        // the tensor work of the one-CTA kernel's 128 x 256 tile. The grid is persistent: pair p takes
+        // tiles p, p + pairs, ... in a grouped order (kGroup tile rows at a time, so the rows of A and
+        // the columns of B in use stay in L2). Tensor memory holds two accumulators of 256 columns:
+        // the epilogue drains tile i from one while the MMA issuer fills tile i + 1 into the other.
+        //
+        // 192 threads per CTA: warps 0-3 epilogue (tensor-memory lanes 32 w .. 32 w + 31), warp 4
+        // producer (both CTAs load their halves of each stage, and the bytes are counted on the
+        // leader's `full` barrier), warp 5 MMA issuer (leader CTA, rank 0, only). Barriers: full[s]
+        // (leader: both CTAs' bytes), empty[s] and acc_full[b] (both CTAs, arrived by the leader's
+        // commit, multicast to the pair), acc_empty[b] (leader: one arrival per epilogue warp of both
+        // CTAs). Every wait is bounded: a role whose wait runs out records the timeout in the status
+        // word and stops; the others' waits then run out too, and the pair meets at a cluster barrier
+        // before freeing its tensor memory.
+        constexpr unsigned kGroup = 8;
+        template <int TERMS> struct PairShape {
+            static constexpr int BN = 256;                                  // N of the tile and of the MMA
+            static constexpr int stages = TERMS == 1 ? 6 : (TERMS == 2 ? 3 : 2);
+            static constexpr unsigned a_bytes = 128 * kBK * 2;              // this CTA's rows of A, one term
+            static constexpr unsigned b_bytes = (BN / 2) * kBK * 2;         // this CTA's rows of B^T, one term
+            static constexpr unsigned stage = TERMS * (a_bytes + b_bytes);  // one CTA's share of a stage
+            static constexpr unsigned instr =
+                    (1u << 4) | (1u << 7) | (1u << 10) | (unsigned(BN >> 3) << 17) | (unsigned(256 >> 4) << 24);
+        };
+
+        __device__ __forceinline__ unsigned pair_rank() {
+            unsigned r;
+            asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+            return r;
+        }
+        __device__ __forceinline__ unsigned pair_address(const void *local, unsigned rank) {
+            unsigned mapped;
+            asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(mapped) : "r"(saddr(local)), "r"(rank));
+            return mapped;
+        }
+        __device__ __forceinline__ void pair_sync() {
+            asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+        }
+        __device__ __forceinline__ void pair_tma_load(void *dst, const CUtensorMap *map, int x, int y, unsigned leader_bar) {
+            asm volatile(
+                    "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+                            saddr(dst)),
+                    "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(leader_bar)
+                    : "memory");
+        }
+        __device__ __forceinline__ void pair_mma(unsigned tmem, unsigned long long a, unsigned long long b, unsigned instr,
+                                                 unsigned accumulate) {
+            asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                    "l"(a), "l"(b), "r"(instr), "r"(accumulate)
+                    : "memory");
+        }
+        // Arrives on the barrier at this offset in both CTAs of the pair once the MMAs issued so far are done.
+        __device__ __forceinline__ void pair_commit(unsigned long long *bar) {
+            asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(
+                                 saddr(bar)),
+                         "h"(static_cast<unsigned short>(0x3))
+                         : "memory");
+        }
+        __device__ __forceinline__ void pair_arrive(unsigned address) {
+            asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(address) : "memory");
+        }
+        // Tile t of the grouped order: kGroup tile rows at a time, down the rows of the group first.
+        __device__ __forceinline__ void pair_tile(unsigned t, unsigned tiles_m, unsigned tiles_n, unsigned &tm, unsigned &tn) {
+            const unsigned per_group = kGroup * tiles_n;
+            const unsigned group = t / per_group, first = group * kGroup;
+            const unsigned rows = tiles_m - first < kGroup ? tiles_m - first : kGroup;
+            const unsigned local = t - group * per_group;
+            tm = first + local % rows;
+            tn = local / rows;
+        }
+
+        template <int TERMS>
+        __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
+                tensor_product_pair(const __grid_constant__ Maps maps, const ProductArgs args, unsigned tiles_m,
+                                    unsigned tiles_n) {
+            using Sh = PairShape<TERMS>;
+            using Pr = Products<TERMS>;
+            constexpr int S = Sh::stages, BN = Sh::BN;
+            extern __shared__ unsigned char raw[];
+            __shared__ unsigned long long full[S], empty[S], acc_full[2], acc_empty[2];
+            __shared__ unsigned tmem_slot;
+            unsigned char *ring = reinterpret_cast<unsigned char *>((reinterpret_cast<unsigned long long>(raw) + 1023) & ~1023ull);
+
+            const unsigned warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+            const unsigned rank = pair_rank();
+            const unsigned pair = blockIdx.x / 2, pairs = gridDim.x / 2;
+            const unsigned tiles = tiles_m * tiles_n;
+            const int kblocks = static_cast<int>(args.kp / kBK);
+
+            if (threadIdx.x == 0) {
+                for (int s = 0; s < S; ++s) {
+                    mbar_init(&full[s], 1);
+                    mbar_init(&empty[s], 1);
+                }
+                for (int b = 0; b < 2; ++b) {
+                    mbar_init(&acc_full[b], 1);
+                    mbar_init(&acc_empty[b], 8);
+                }
+                asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            }
+            if (warp == 0) {
+                asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&tmem_slot)),
+                             "r"(2 * BN)
+                             : "memory");
+                asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            pair_sync();  // both CTAs' barriers exist before either sees a remote arrival or a transfer
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const unsigned tmem = tmem_slot;
+
+            if (warp == 4) {
+                if (lane == 0) {
+                    // producer: this CTA's 128 rows of A and 128 rows of B^T per term, per stage
+                    unsigned s = 0, phase = 0;
+                    bool ok = true;
+                    for (unsigned t = pair; t < tiles && ok; t += pairs) {
+                        unsigned tm, tn;
+                        pair_tile(t, tiles_m, tiles_n, tm, tn);
+                        const int ya = static_cast<int>(tm * 256 + rank * 128), yb = static_cast<int>(tn * BN + rank * (BN / 2));
+                        for (int kb = 0; kb < kblocks; ++kb) {
+                            if (!mbar_wait(&empty[s], phase ^ 1u)) {
+                                ok = false;
+                                break;
+                            }
+                            if (rank == 0) mbar_expect(&full[s], 2 * Sh::stage);
+                            const unsigned bar = pair_address(&full[s], 0);
+                            unsigned char *stage = ring + s * Sh::stage;
+                            const int x = kb * kBK;
+#pragma unroll
+                            for (int q = 0; q < TERMS; ++q) {
+                                pair_tma_load(stage + q * Sh::a_bytes, &maps.a[q], x, ya, bar);
+                                pair_tma_load(stage + TERMS * Sh::a_bytes + q * Sh::b_bytes, &maps.b[q], x, yb, bar);
+                            }
+                            if (++s == S) {
+                                s = 0;
+                                phase ^= 1u;
+                            }
+                        }
+                    }
+                    if (!ok) atomicOr(args.status, kStatusTimeout);
+                }
+            } else if (warp == 5) {
+                if (rank == 0 && lane == 0) {
+                    // MMA issuer: 256 x 256 x 16 steps into accumulator b of tile i
+                    unsigned s = 0, phase = 0, i = 0;
+                    bool ok = true;
+                    for (unsigned t = pair; t < tiles && ok; t += pairs, ++i) {
+                        const unsigned b = i & 1u;
+                        if (!mbar_wait(&acc_empty[b], ((i >> 1) & 1u) ^ 1u)) {
+                            ok = false;
+                            break;
+                        }
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                        const unsigned d = tmem + b * BN;
+                        for (int kb = 0; kb < kblocks; ++kb) {
+                            if (!mbar_wait(&full[s], phase)) {
+                                ok = false;
+                                break;
+                            }
+                            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                            unsigned char *stage = ring + s * Sh::stage;
+#pragma unroll
+                            for (int kk = 0; kk < kBK / kUmmaK; ++kk) {
+                                const unsigned long long step = (kk * kUmmaK * 2) >> 4;  // 32 bytes along K
+#pragma unroll
+                                for (int p = 0; p < Pr::count; ++p) {
+                                    const unsigned long long da = smem_desc(stage + product_a(p) * Sh::a_bytes) + step;
+                                    const unsigned long long db =
+                                            smem_desc(stage + TERMS * Sh::a_bytes + product_b(p) * Sh::b_bytes) + step;
+                                    pair_mma(d, da, db, Sh::instr, (kb | kk | p) != 0);
+                                }
+                            }
+                            pair_commit(&empty[s]);  // both CTAs' stage s is free once these MMAs have read it
+                            if (++s == S) {
+                                s = 0;
+                                phase ^= 1u;
+                            }
+                        }
+                        if (!ok) break;
+                        pair_commit(&acc_full[b]);  // the tile's accumulator is complete in both CTAs
+                    }
+                    if (!ok) atomicOr(args.status, kStatusTimeout);
+                }
+            } else {
+                // epilogue: tensor-memory lanes 32 warp .. 32 warp + 31 hold this CTA's rows
+                // tm * 256 + 128 rank + 32 warp + lane; tcgen05.ld is warp-collective
+                const unsigned empty0 = pair_address(&acc_empty[0], 0), empty1 = pair_address(&acc_empty[1], 0);
+                unsigned i = 0;
+                for (unsigned t = pair; t < tiles; t += pairs, ++i) {
+                    const unsigned b = i & 1u;
+                    const bool waited = mbar_wait(&acc_full[b], (i >> 1) & 1u);
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    if (!__all_sync(0xffffffffu, waited)) {
+                        if (lane == 0) atomicOr(args.status, kStatusTimeout);
+                        break;
+                    }
+                    unsigned tm, tn;
+                    pair_tile(t, tiles_m, tiles_n, tm, tn);
+                    const unsigned long long row = 256ull * tm + 128 * rank + warp * 32 + lane;
+                    const unsigned long long n0 = 1ull * tn * BN;
+#pragma unroll 1
+                    for (int chunk = 0; chunk < BN / 32; ++chunk) {
+                        unsigned v[32];
+                        const unsigned address = tmem + ((warp * 32u) << 16) + b * BN + chunk * 32u;
+                        asm volatile(
+                                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                                  "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                                  "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
+                                  "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
+                                  "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                                : "r"(address));
+                        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                        const unsigned long long col = n0 + chunk * 32;
+                        if (row < args.m && col < args.n) {
+                            float *dst = args.c + row * args.ldc + col;
+                            if (col + 32 <= args.n && (args.ldc % 4) == 0 &&
+                                (reinterpret_cast<unsigned long long>(args.c) % 16) == 0) {
+#pragma unroll
+                                for (int j = 0; j < 32; j += 4) {
+                                    float4 out = make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]),
+                                                             __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
+                                    if (args.subtract) {
+                                        const float4 old = *reinterpret_cast<const float4 *>(dst + j);
+                                        out = make_float4(old.x - out.x, old.y - out.y, old.z - out.z, old.w - out.w);
+                                    }
+                                    *reinterpret_cast<float4 *>(dst + j) = out;
+                                }
+                            } else {
+                                for (int j = 0; j < 32; ++j)
+                                    if (col + j < args.n)
+                                        dst[j] = args.subtract ? dst[j] - __uint_as_float(v[j]) : __uint_as_float(v[j]);
+                            }
+                        }
+                    }
+                    // accumulator b may be refilled once all eight epilogue warps have read it
+                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) pair_arrive(b ? empty1 : empty0);
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads();
+            pair_sync();  // neither CTA leaves while the pair's MMAs may still read its shared memory
+            if (warp == 0) {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN) : "memory");
+            }
+        }
+
         // ---- plain SIMT products (the comparison forms) ---------------------------------------------
         // 128 x 128 output tile per 256-thread block, 8 x 8 per thread, K slices of 8 through shared
         // memory. T = float accumulates in float, T = double in double (the reference's
@@ -402,6 +662,45 @@ namespace sci_cuda {
             return fn;
         }
 
+        // Whether products of 256 rows or more run on the CTA-pair kernel (the default); the
+        // environment variable SCI_CUDA_PRODUCT_PAIR=0 keeps them on the one-CTA kernel.
+        bool pair_kernel_enabled() {
+            static const bool enabled = [] {
+                const char *setting = std::getenv("SCI_CUDA_PRODUCT_PAIR");
+                return !(setting && std::strcmp(setting, "0") == 0);
+            }();
+            return enabled;
+        }
+
+        // CTA pairs of the pair kernel that can be resident at once (persistent grid), at most one
+        // per two SMs; cached per kernel.
+        unsigned long long pair_slots(const void *kernel, size_t smem, int sms) {
+            static std::mutex guard;
+            static std::map<const void *, unsigned long long> known;
+            std::lock_guard<std::mutex> lock(guard);
+            auto found = known.find(kernel);
+            if (found != known.end()) return found->second;
+            cudaLaunchConfig_t config{};
+            config.gridDim = dim3(static_cast<unsigned>(sms / 2 * 2));
+            config.blockDim = dim3(192);
+            config.dynamicSmemBytes = smem;
+            cudaLaunchAttribute attribute[1];
+            attribute[0].id = cudaLaunchAttributeClusterDimension;
+            attribute[0].val.clusterDim.x = 2;
+            attribute[0].val.clusterDim.y = 1;
+            attribute[0].val.clusterDim.z = 1;
+            config.attrs = attribute;
+            config.numAttrs = 1;
+            int clusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&clusters, kernel, &config) != cudaSuccess || clusters < 1) {
+                cudaGetLastError();
+                clusters = sms / 2;
+            }
+            const unsigned long long slots = static_cast<unsigned long long>(std::min(clusters, sms / 2));
+            known[kernel] = slots;
+            return slots;
+        }
+
         // A 2-D bf16 tensor map over a rows x kp K-major matrix, box rows_box x 64, 128-byte swizzle.
         bool make_map(CUtensorMap *map, const void *base, unsigned long long rows, unsigned long long kp, unsigned box_rows) {
             EncodeTiled encode = encoder();
@@ -423,13 +722,13 @@ namespace sci_cuda {
     // transposition, so the tensor-core kernel is the same either way.
     int tensor_gemm(Context &ctx, int terms, const float *a, unsigned long long lda, const float *b,
                     unsigned long long ldb, float *c, unsigned long long ldc, unsigned long long m, unsigned long long n,
-                    unsigned long long k, bool subtract) {
-        return tensor_gemm_t(ctx, terms, a, lda, false, b, ldb, false, c, ldc, m, n, k, subtract);
+                    unsigned long long k, bool subtract, bool whole_gpu) {
+        return tensor_gemm_t(ctx, terms, a, lda, false, b, ldb, false, c, ldc, m, n, k, subtract, whole_gpu);
     }
 
     int tensor_gemm_t(Context &ctx, int terms, const float *a, unsigned long long lda, bool a_t, const float *b,
                       unsigned long long ldb, bool b_t, float *c, unsigned long long ldc, unsigned long long m,
-                      unsigned long long n, unsigned long long k, bool subtract) {
+                      unsigned long long n, unsigned long long k, bool subtract, bool whole_gpu) {
         if (terms < 1 || terms > 3) return ctx.fail(SCI_CUDA_ERROR_INVALID, "bf16 terms %d", terms);
         const unsigned long long kp = (k + kBK - 1) / kBK * kBK;
         if (kp > (1ull << 31) || m > (1ull << 31) || n > (1ull << 31))
@@ -457,6 +756,32 @@ namespace sci_cuda {
         else columns_of(b, ldb, bt, n);
         if (int code = ctx.check(cudaGetLastError(), "launching the bf16 conversion")) return code;
 
+        ProductArgs args{c, m, n, kp, ldc, subtract ? 1 : 0, ctx.status};
+        if (whole_gpu && m >= 256 && pair_kernel_enabled()) {
+            // 256 x 256 tiles on CTA pairs, persistent: each CTA stages 128 rows of A and of B^T
+            Maps maps;
+            std::memset(&maps, 0, sizeof(maps));
+            for (int q = 0; q < terms; ++q) {
+                if (!make_map(&maps.a[q], at.t[q], m, kp, 128) || !make_map(&maps.b[q], bt.t[q], n, kp, 128))
+                    return ctx.fail(SCI_CUDA_ERROR_LAUNCH, "cuTensorMapEncodeTiled failed");
+            }
+            const void *kernel = terms == 1 ? reinterpret_cast<const void *>(&tensor_product_pair<1>)
+                               : terms == 2 ? reinterpret_cast<const void *>(&tensor_product_pair<2>)
+                                            : reinterpret_cast<const void *>(&tensor_product_pair<3>);
+            const size_t smem = terms == 1 ? PairShape<1>::stages * PairShape<1>::stage + 1024
+                              : terms == 2 ? PairShape<2>::stages * PairShape<2>::stage + 1024
+                                           : PairShape<3>::stages * PairShape<3>::stage + 1024;
+            if (int code = ctx.check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
+                                     "raising the pair kernel's shared memory"))
+                return code;
+            unsigned tiles_m = static_cast<unsigned>((m + 255) / 256), tiles_n = static_cast<unsigned>((n + 255) / 256);
+            const unsigned long long tiles = 1ull * tiles_m * tiles_n;
+            const unsigned long long pairs = std::min<unsigned long long>(tiles, pair_slots(kernel, smem, ctx.sms));
+            void *params[] = {&maps, &args, &tiles_m, &tiles_n};
+            return ctx.check(cudaLaunchKernel(kernel, dim3(static_cast<unsigned>(2 * pairs)), dim3(192), params, smem, ctx.stream),
+                             "launching the pair tensor product");
+        }
+
         const unsigned bn = terms == 3 ? 128u : 256u;
         Maps maps;
         std::memset(&maps, 0, sizeof(maps));
@@ -473,7 +798,6 @@ namespace sci_cuda {
         if (int code = ctx.check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
                                  "raising the product kernel's shared memory"))
             return code;
-        ProductArgs args{c, m, n, kp, ldc, subtract ? 1 : 0, ctx.status};
         void *params[] = {&maps, &args};
         const dim3 pgrid(static_cast<unsigned>((n + bn - 1) / bn), static_cast<unsigned>((m + kBM - 1) / kBM));
         return ctx.check(cudaLaunchKernel(kernel, pgrid, dim3(192), params, smem, ctx.stream), "launching the tensor product");
@@ -537,7 +861,7 @@ extern "C" int sci_cuda_product(sci_cuda_context *context, uint32_t precision, u
     return tensor_gemm(*context, mode == SCI_PRODUCT_SPLIT3_BF16 ? 3 : (mode == SCI_PRODUCT_SPLIT_BF16 ? 2 : 1),
                        static_cast<const float *>(left), depth,
                        static_cast<const float *>(right), columns, static_cast<float *>(output), columns, rows, columns,
-                       depth, false);
+                       depth, false, true);
 }
 
 extern "C" int sci_cuda_product_gradient(sci_cuda_context *context, uint32_t precision, uint32_t mode, const void *left,
@@ -565,7 +889,7 @@ extern "C" int sci_cuda_product_gradient(sci_cuda_context *context, uint32_t pre
                                       b_t, static_cast<float *>(out), n, m, n, k, false);
         return tensor_gemm_t(*context, mode == SCI_PRODUCT_SPLIT3_BF16 ? 3 : (mode == SCI_PRODUCT_SPLIT_BF16 ? 2 : 1),
                              static_cast<const float *>(a), lda, a_t, static_cast<const float *>(b), ldb, b_t,
-                             static_cast<float *>(out), n, m, n, k, false);
+                             static_cast<float *>(out), n, m, n, k, false, true);
     };
     if (int code = one(left_gradient, upstream, columns, false, right, columns, true, rows, depth, columns)) return code;
     return one(right_gradient, left, depth, true, upstream, columns, false, depth, columns, rows);

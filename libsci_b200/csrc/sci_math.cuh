@@ -442,6 +442,37 @@ namespace sci_cuda {
         return a == a ? result : __fadd_rn(x, x);
     }
 
+    // tanh of a float with |x| <= 1, in double: tanh x = x + x^3 g(x^2), where g is the degree-11
+    // polynomial interpolating g(u) = (tanh(sqrt u) / sqrt u - 1) / u at the 12 Chebyshev nodes of
+    // [0, 1] (coefficients computed in 60-digit arithmetic by libsci_b200/coefficients.py and
+    // rounded to double; their relative error against g is below 2^-41.7 on [0, 1]). u = x^2 is
+    // exact in double, and the result t is within 2^-43 relative of tanh x. Its float rounding is
+    // therefore the correctly rounded value -- the one tanh_float returns, whose own error is about
+    // 2^-50 -- unless tanh x lies within 2^-41 relative of a float rounding midpoint: the 29 bits of
+    // t below the float's last place then lie within 2^12 of 100...0, and `rare` is set so that the
+    // caller recomputes with tanh_float. No infinity or NaN reaches it (|x| <= 1); a zero keeps its
+    // sign.
+    __device__ __forceinline__ float tanh_float_near(float x, bool &rare) {
+        const double a = static_cast<double>(x);
+        const double u = __dmul_rn(a, a);
+        double g = 0x1.fcc078193c27dp-20;
+        g = __fma_rn(g, u, -0x1.0d3ce4aaa45fcp-16);
+        g = __fma_rn(g, u, 0x1.2347b46ddb8b5p-14);
+        g = __fma_rn(g, u, -0x1.c5bfee363a8b2p-13);
+        g = __fma_rn(g, u, 0x1.2e76669b584c5p-11);
+        g = __fma_rn(g, u, -0x1.7c4648492ca7bp-10);
+        g = __fma_rn(g, u, 0x1.d6a56a6f2f6f3p-9);
+        g = __fma_rn(g, u, -0x1.226c3a99b757dp-7);
+        g = __fma_rn(g, u, 0x1.664f2ec3a9f0dp-6);
+        g = __fma_rn(g, u, -0x1.ba1ba10bdf714p-5);
+        g = __fma_rn(g, u, 0x1.1111111028c6fp-3);
+        g = __fma_rn(g, u, -0x1.5555555554ee4p-2);
+        const double t = __fma_rn(__dmul_rn(a, u), g, a);
+        const unsigned below = static_cast<unsigned>(__double2loint(t)) & 0x1fffffffu;
+        rare = rare || below - 0x0ffff000u <= 0x2000u;
+        return static_cast<float>(t);
+    }
+
     // ---- two floats per instruction ----------------------------------------------------------------
     // sm_100 adds packed two-lane FP32 arithmetic (add / sub / mul / fma .rn .f32x2): each lane is
     // rounded exactly as the one-lane instruction rounds it, and one instruction issues for both. The

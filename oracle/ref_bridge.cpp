@@ -221,6 +221,40 @@ const float *sci_ref_workload_output(void *handle, const int which) {
 
 void sci_ref_workload_destroy(void *handle) { delete static_cast<sci_ref_workload *>(handle); }
 
+// The plain fused expression, run through the reference's public API: a = linspace(0, 1, n),
+// b, c given; each step stores t = a*b + c*2.0f and e = exponential(t)*0.5f and reduces
+// s = sum(sin(t)), the way a libsci user writes them.
+struct sci_ref_plain {
+    sci::Array<float, 1> a, b, c, t, e;
+};
+
+void *sci_ref_plain_create(const float *b, const float *c, const uint64_t count) {
+    auto *work = new sci_ref_plain{
+            sci::linspace(0.0f, 1.0f, count),
+            sci::Array<float, 1>(sci::Shape<1>{count}, sci::array::Uninitialized{}),
+            sci::Array<float, 1>(sci::Shape<1>{count}, sci::array::Uninitialized{}),
+            sci::Array<float, 1>(sci::Shape<1>{count}, sci::array::Uninitialized{}),
+            sci::Array<float, 1>(sci::Shape<1>{count}, sci::array::Uninitialized{}),
+    };
+    std::memcpy(work->b.data(), b, count * sizeof(float));
+    std::memcpy(work->c.data(), c, count * sizeof(float));
+    return work;
+}
+
+double sci_ref_plain_step(void *handle) {
+    auto &work = *static_cast<sci_ref_plain *>(handle);
+    work.t = work.a * work.b + work.c * 2.0f;
+    work.e = sci::exponential(work.t) * 0.5f;
+    return sci::sum(sci::sin(work.t));
+}
+
+const float *sci_ref_plain_output(void *handle, const int which) {
+    auto &work = *static_cast<sci_ref_plain *>(handle);
+    return which == 0 ? work.t.data() : which == 1 ? work.e.data() : work.a.data();
+}
+
+void sci_ref_plain_destroy(void *handle) { delete static_cast<sci_ref_plain *>(handle); }
+
 // ---- creation: the reference's own functions (include/operations/creation.hpp) -----------------
 void sci_ref_full(uint32_t precision, void *out, uint64_t count, double value) {  // creation.hpp:52-58
     if (precision == SCI_PRECISION_WIDE) {

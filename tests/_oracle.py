@@ -70,6 +70,13 @@ def reference() -> ctypes.CDLL | None:
     lib.sci_ref_workload_output.restype = ctypes.c_void_p
     lib.sci_ref_workload_output.argtypes = [ctypes.c_void_p, ctypes.c_int]
     lib.sci_ref_workload_destroy.argtypes = [ctypes.c_void_p]
+    lib.sci_ref_plain_create.restype = ctypes.c_void_p
+    lib.sci_ref_plain_create.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64]
+    lib.sci_ref_plain_step.restype = ctypes.c_double
+    lib.sci_ref_plain_step.argtypes = [ctypes.c_void_p]
+    lib.sci_ref_plain_output.restype = ctypes.c_void_p
+    lib.sci_ref_plain_output.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.sci_ref_plain_destroy.argtypes = [ctypes.c_void_p]
     lib.sci_ref_elements.argtypes = [ctypes.c_int, ctypes.c_uint32] + [ctypes.c_void_p] * 3 + [ctypes.c_uint64,
                                                                                             ctypes.c_void_p]
     _cache["ref"] = lib
