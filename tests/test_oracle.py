@@ -236,3 +236,29 @@ def test_creation_oracle_matches_the_reference(oracle, reference, dtype):
     mine["grid"](precision, x.ctypes.data, 7, y.ctypes.data, 5, xx.ctypes.data, yy.ctypes.data)
     gx, gy = np.meshgrid(x, y)  # numpy.meshgrid, which grid is named after
     assert np.array_equal(xx.reshape(5, 7), gx) and np.array_equal(yy.reshape(5, 7), gy)
+
+
+def test_plain_workload_through_the_reference_api(oracle, reference):
+    """The plain fused workload as bench.py's CPU arm runs it through libsci's public API
+    (sci_ref_plain_*: a = linspace(0, 1, n), t = a*b + c*2, e = exp(t)*0.5, s = sum(sin t)) equals the
+    oracle's chunks bit for bit, with s within the reference's float-block fold."""
+    n = (1 << 16) + 5
+    b = np.random.default_rng(0).uniform(-1, 1, n).astype(np.float32)
+    c = np.ones(n, np.float32)
+    handle = reference.sci_ref_plain_create(b.ctypes.data, c.ctypes.data, n)
+    s = reference.sci_ref_plain_step(handle)
+
+    def output(which):
+        pointer = ctypes.cast(reference.sci_ref_plain_output(handle, which), ctypes.POINTER(ctypes.c_float))
+        return np.ctypeslib.as_array(pointer, shape=(n,)).copy()
+
+    t, e, a = output(0), output(1), output(2)
+    reference.sci_ref_plain_destroy(handle)
+    refs = [C.Reference(v.ctypes.data, n, np.float32) for v in (a, b, c)]
+    t_want = _oracle.execute(oracle, C.record_output(refs[0] * refs[1] + refs[2] * 2.0), n, np.float32)
+    assert _oracle.mismatches(t, t_want).size == 0
+    tr = C.Reference(t_want.ctypes.data, n, np.float32)
+    e_want = _oracle.execute(oracle, C.record_output(C.unary("exponential", tr) * 0.5), n, np.float32)
+    assert _oracle.mismatches(e, e_want).size == 0
+    s_want = _oracle.reduce(oracle, C.record_reduce(C.unary("sin", tr)), C.SUM, n)
+    assert abs(s - s_want) <= 1e-6 * abs(s_want)
