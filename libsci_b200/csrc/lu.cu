@@ -1244,13 +1244,21 @@ namespace sci_cuda {
             auto block_rows = [&](unsigned long long J0, unsigned long long block_end, unsigned long long c0,
                                   unsigned long long c1) -> int {
                 if (c1 <= c0) return SCI_CUDA_OK;
+                // a chain of kernels, each following the one before directly on the stream: chained
+                // launches after the first (which follows an event wait or other work)
                 for (unsigned long long j0 = J0; j0 < block_end; j0 += W) {
                     const int w = static_cast<int>(std::min<unsigned long long>(W, block_end - j0));
-                    trsm_rows<T><<<static_cast<unsigned>((c1 - c0 + 127) / 128), 128, 0, ctx.stream>>>(a, n, j0, w, c0, c1);
+                    const dim3 grid(static_cast<unsigned>((c1 - c0 + 127) / 128));
+                    if (j0 == J0) {
+                        trsm_rows<T><<<grid, 128, 0, ctx.stream>>>(a, n, j0, w, c0, c1);
+                    } else if (int code = ctx.check(launch_chained(trsm_rows<T>, grid, dim3(128), ctx.stream, a, n, j0, w, c0, c1),
+                                                    "launching the block's U rows")) {
+                        return code;
+                    }
                     const unsigned long long below = j0 + w;
                     if (below < block_end) {
                         if (int code = update<T>(ctx, a + below * n + j0, n, a + j0 * n + c0, n, a + below * n + c0, n,
-                                                 block_end - below, c1 - c0, w))
+                                                 block_end - below, c1 - c0, w, true))
                             return code;
                     }
                 }
@@ -1263,7 +1271,9 @@ namespace sci_cuda {
                                 unsigned long long c1, bool narrow) -> int {
                 if (t0 >= n || c1 <= c0) return SCI_CUDA_OK;
                 const unsigned long long ob = t0 - J0;
-                if (narrow) return update<T>(ctx, a + t0 * n + J0, n, a + J0 * n + c0, n, a + t0 * n + c0, n, n - t0, c1 - c0, ob);
+                // narrow follows the block's U rows (a kernel) directly on the main stream: chained
+                if (narrow)
+                    return update<T>(ctx, a + t0 * n + J0, n, a + J0 * n + c0, n, a + t0 * n + c0, n, n - t0, c1 - c0, ob, true);
                 if constexpr (sizeof(T) == 4) {
                     if (tensor)
                         return tensor_gemm(ctx, split ? 3 : 1, a + t0 * n + J0, n, a + J0 * n + c0, n, a + t0 * n + c0, n,

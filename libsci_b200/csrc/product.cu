@@ -307,29 +307,43 @@ namespace sci_cuda {
         }
 
         // ---- the persistent CTA-pair kernel -----------------------------------------------------------
-        // Two CTAs of a cluster compute 256 x 256 tiles of C together with tcgen05.mma.cta_group::2
-        // (M = 256): each CTA stages 128 rows of A and 128 rows of B^T per term and holds 128 rows of
-        // the FP32 accumulator in its own tensor memory, so each byte of B a CTA stages feeds twice
-        // the tensor work of the one-CTA kernel's 128 x 256 tile. The grid is persistent: pair p takes
-        // tiles p, p + pairs, ... in a grouped order (kGroup tile rows at a time, so the rows of A and
-        // the columns of B in use stay in L2). Tensor memory holds two accumulators of 256 columns:
-        // the epilogue drains tile i from one while the MMA issuer fills tile i + 1 into the other.
+        // Two CTAs of a cluster compute 256 x BN tiles of C together with tcgen05.mma.cta_group::2
+        // (M = 256): each CTA stages 128 rows of A and BN / 2 rows of B^T per term and holds 128 rows of
+        // the FP32 accumulators in its own tensor memory, so each byte of B a CTA stages feeds twice
+        // the tensor work of the one-CTA kernel. The grid is persistent: pair p takes tiles p,
+        // p + pairs, ... in a grouped order (kGroup tile rows at a time, so the rows of A and the
+        // columns of B in use stay in L2). Tensor memory holds two accumulator buffers of 256 columns:
+        // the epilogue drains one while the MMA issuer fills the other.
+        //
+        // Accuracy of the split modes. The tensor cores' FP32 accumulation loses accuracy in
+        // proportion to the number of products accumulated into one accumulator (measured at
+        // 8192^3: split3 with one accumulator over all of K was 5.4e-5 relative, twice the split
+        // mode's error, where FP32 arithmetic gives 1.6e-6). So with two or three terms each
+        // 256 x 128 tile is computed in K segments of kSegment k-blocks, and each buffer holds two
+        // accumulators: the leading product t0 * t0 and, separately, the sum of the small products
+        // (2^-8 of it and below). The epilogue adds the two in FP32 and adds the segment into C
+        // (the first segment stores), so no accumulator takes more than kSegment * 4 leading
+        // products.
         //
         // 192 threads per CTA: warps 0-3 epilogue (tensor-memory lanes 32 w .. 32 w + 31), warp 4
         // producer (both CTAs load their halves of each stage, and the bytes are counted on the
         // leader's `full` barrier), warp 5 MMA issuer (leader CTA, rank 0, only). Barriers: full[s]
         // (leader: both CTAs' bytes), empty[s] and acc_full[b] (both CTAs, arrived by the leader's
         // commit, multicast to the pair), acc_empty[b] (leader: one arrival per epilogue warp of both
-        // CTAs). Every wait is bounded: a role whose wait runs out records the timeout in the status
-        // word and stops; the others' waits then run out too, and the pair meets at a cluster barrier
-        // before freeing its tensor memory.
+        // CTAs). Work items are (tile, segment) pairs in the same order for every role. Every wait is
+        // bounded: a role whose wait runs out records the timeout in the status word and stops; the
+        // others' waits then run out too, and the pair meets at a cluster barrier before freeing its
+        // tensor memory.
         constexpr unsigned kGroup = 8;
+        constexpr int kSegment = 32;  // k-blocks (64 deep) per segment of the split modes
         template <int TERMS> struct PairShape {
-            static constexpr int BN = 256;                                  // N of the tile and of the MMA
-            static constexpr int stages = TERMS == 1 ? 6 : (TERMS == 2 ? 3 : 2);
+            static constexpr int BN = TERMS == 1 ? 256 : 128;               // N of the tile and of the MMA
+            static constexpr bool split = TERMS > 1;                        // two accumulators per buffer
+            static constexpr int stages = TERMS == 1 ? 6 : (TERMS == 2 ? 4 : 3);
             static constexpr unsigned a_bytes = 128 * kBK * 2;              // this CTA's rows of A, one term
             static constexpr unsigned b_bytes = (BN / 2) * kBK * 2;         // this CTA's rows of B^T, one term
             static constexpr unsigned stage = TERMS * (a_bytes + b_bytes);  // one CTA's share of a stage
+            static constexpr unsigned buffer = 256;                         // tensor-memory columns per buffer
             static constexpr unsigned instr =
                     (1u << 4) | (1u << 7) | (1u << 10) | (unsigned(BN >> 3) << 17) | (unsigned(256 >> 4) << 24);
         };
@@ -381,6 +395,17 @@ namespace sci_cuda {
             tm = first + local % rows;
             tn = local / rows;
         }
+        __device__ __forceinline__ void tmem_load32(unsigned address, unsigned (&v)[32]) {
+            asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                    "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                      "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                      "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                      "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(address));
+        }
 
         template <int TERMS>
         __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
@@ -399,6 +424,8 @@ namespace sci_cuda {
             const unsigned pair = blockIdx.x / 2, pairs = gridDim.x / 2;
             const unsigned tiles = tiles_m * tiles_n;
             const int kblocks = static_cast<int>(args.kp / kBK);
+            const int per_segment = Sh::split ? kSegment : kblocks;
+            const int segments = (kblocks + per_segment - 1) / per_segment;
 
             if (threadIdx.x == 0) {
                 for (int s = 0; s < S; ++s) {
@@ -413,7 +440,7 @@ namespace sci_cuda {
             }
             if (warp == 0) {
                 asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&tmem_slot)),
-                             "r"(2 * BN)
+                             "r"(2 * Sh::buffer)
                              : "memory");
                 asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
             }
@@ -424,14 +451,14 @@ namespace sci_cuda {
 
             if (warp == 4) {
                 if (lane == 0) {
-                    // producer: this CTA's 128 rows of A and 128 rows of B^T per term, per stage
+                    // producer: this CTA's 128 rows of A and BN / 2 rows of B^T per term, per stage
                     unsigned s = 0, phase = 0;
                     bool ok = true;
                     for (unsigned t = pair; t < tiles && ok; t += pairs) {
                         unsigned tm, tn;
                         pair_tile(t, tiles_m, tiles_n, tm, tn);
                         const int ya = static_cast<int>(tm * 256 + rank * 128), yb = static_cast<int>(tn * BN + rank * (BN / 2));
-                        for (int kb = 0; kb < kblocks; ++kb) {
+                        for (int kb = 0; kb < kblocks && ok; ++kb) {
                             if (!mbar_wait(&empty[s], phase ^ 1u)) {
                                 ok = false;
                                 break;
@@ -455,43 +482,51 @@ namespace sci_cuda {
                 }
             } else if (warp == 5) {
                 if (rank == 0 && lane == 0) {
-                    // MMA issuer: 256 x 256 x 16 steps into accumulator b of tile i
+                    // MMA issuer: 256 x BN x 16 steps into the accumulators of buffer b for work item i
                     unsigned s = 0, phase = 0, i = 0;
                     bool ok = true;
-                    for (unsigned t = pair; t < tiles && ok; t += pairs, ++i) {
-                        const unsigned b = i & 1u;
-                        if (!mbar_wait(&acc_empty[b], ((i >> 1) & 1u) ^ 1u)) {
-                            ok = false;
-                            break;
-                        }
-                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                        const unsigned d = tmem + b * BN;
-                        for (int kb = 0; kb < kblocks; ++kb) {
-                            if (!mbar_wait(&full[s], phase)) {
+                    for (unsigned t = pair; t < tiles && ok; t += pairs) {
+                        for (int segment = 0; segment < segments && ok; ++segment, ++i) {
+                            const unsigned b = i & 1u;
+                            if (!mbar_wait(&acc_empty[b], ((i >> 1) & 1u) ^ 1u)) {
                                 ok = false;
                                 break;
                             }
                             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                            unsigned char *stage = ring + s * Sh::stage;
+                            const unsigned lead = tmem + b * Sh::buffer, rest = Sh::split ? lead + BN : lead;
+                            const int k0 = segment * per_segment;
+                            const int k1 = k0 + per_segment < kblocks ? k0 + per_segment : kblocks;
+                            for (int kb = k0; kb < k1; ++kb) {
+                                if (!mbar_wait(&full[s], phase)) {
+                                    ok = false;
+                                    break;
+                                }
+                                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                                unsigned char *stage = ring + s * Sh::stage;
 #pragma unroll
-                            for (int kk = 0; kk < kBK / kUmmaK; ++kk) {
-                                const unsigned long long step = (kk * kUmmaK * 2) >> 4;  // 32 bytes along K
+                                for (int kk = 0; kk < kBK / kUmmaK; ++kk) {
+                                    const unsigned long long step = (kk * kUmmaK * 2) >> 4;  // 32 bytes along K
+                                    const bool first = kb == k0 && kk == 0;
 #pragma unroll
-                                for (int p = 0; p < Pr::count; ++p) {
-                                    const unsigned long long da = smem_desc(stage + product_a(p) * Sh::a_bytes) + step;
-                                    const unsigned long long db =
-                                            smem_desc(stage + TERMS * Sh::a_bytes + product_b(p) * Sh::b_bytes) + step;
-                                    pair_mma(d, da, db, Sh::instr, (kb | kk | p) != 0);
+                                    for (int p = 0; p < Pr::count; ++p) {
+                                        const unsigned long long da = smem_desc(stage + product_a(p) * Sh::a_bytes) + step;
+                                        const unsigned long long db =
+                                                smem_desc(stage + TERMS * Sh::a_bytes + product_b(p) * Sh::b_bytes) + step;
+                                        // the leading product into its own accumulator; the small ones together
+                                        const bool into_rest = Sh::split && p > 0;
+                                        const bool starts = first && (p == 0 || (into_rest && p == 1));
+                                        pair_mma(into_rest ? rest : lead, da, db, Sh::instr, starts ? 0u : 1u);
+                                    }
+                                }
+                                pair_commit(&empty[s]);  // both CTAs' stage s is free once these MMAs have read it
+                                if (++s == S) {
+                                    s = 0;
+                                    phase ^= 1u;
                                 }
                             }
-                            pair_commit(&empty[s]);  // both CTAs' stage s is free once these MMAs have read it
-                            if (++s == S) {
-                                s = 0;
-                                phase ^= 1u;
-                            }
+                            if (!ok) break;
+                            pair_commit(&acc_full[b]);  // the item's accumulators are complete in both CTAs
                         }
-                        if (!ok) break;
-                        pair_commit(&acc_full[b]);  // the tile's accumulator is complete in both CTAs
                     }
                     if (!ok) atomicOr(args.status, kStatusTimeout);
                 }
@@ -499,59 +534,70 @@ namespace sci_cuda {
                 // epilogue: tensor-memory lanes 32 warp .. 32 warp + 31 hold this CTA's rows
                 // tm * 256 + 128 rank + 32 warp + lane; tcgen05.ld is warp-collective
                 const unsigned empty0 = pair_address(&acc_empty[0], 0), empty1 = pair_address(&acc_empty[1], 0);
+                const bool vector = (args.ldc % 4) == 0 && (reinterpret_cast<unsigned long long>(args.c) % 16) == 0;
                 unsigned i = 0;
-                for (unsigned t = pair; t < tiles; t += pairs, ++i) {
-                    const unsigned b = i & 1u;
-                    const bool waited = mbar_wait(&acc_full[b], (i >> 1) & 1u);
-                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                    if (!__all_sync(0xffffffffu, waited)) {
-                        if (lane == 0) atomicOr(args.status, kStatusTimeout);
-                        break;
-                    }
+                bool ok = true;
+                for (unsigned t = pair; t < tiles && ok; t += pairs) {
                     unsigned tm, tn;
                     pair_tile(t, tiles_m, tiles_n, tm, tn);
                     const unsigned long long row = 256ull * tm + 128 * rank + warp * 32 + lane;
                     const unsigned long long n0 = 1ull * tn * BN;
+                    for (int segment = 0; segment < segments; ++segment, ++i) {
+                        const unsigned b = i & 1u;
+                        const bool waited = mbar_wait(&acc_full[b], (i >> 1) & 1u);
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                        if (!__all_sync(0xffffffffu, waited)) {
+                            if (lane == 0) atomicOr(args.status, kStatusTimeout);
+                            ok = false;
+                            break;
+                        }
+                        // the first segment of a product stores; later ones (and every segment of a
+                        // subtracting update) combine with what C holds
+                        const int how = args.subtract ? -1 : (segment == 0 ? 0 : 1);
 #pragma unroll 1
-                    for (int chunk = 0; chunk < BN / 32; ++chunk) {
-                        unsigned v[32];
-                        const unsigned address = tmem + ((warp * 32u) << 16) + b * BN + chunk * 32u;
-                        asm volatile(
-                                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
-                                  "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-                                  "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]),
-                                  "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]),
-                                  "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-                                : "r"(address));
-                        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                        const unsigned long long col = n0 + chunk * 32;
-                        if (row < args.m && col < args.n) {
-                            float *dst = args.c + row * args.ldc + col;
-                            if (col + 32 <= args.n && (args.ldc % 4) == 0 &&
-                                (reinterpret_cast<unsigned long long>(args.c) % 16) == 0) {
+                        for (int chunk = 0; chunk < BN / 32; ++chunk) {
+                            unsigned v[32];
+                            const unsigned address = tmem + ((warp * 32u) << 16) + b * Sh::buffer + chunk * 32u;
+                            tmem_load32(address, v);
+                            if constexpr (Sh::split) {
+                                unsigned w[32];
+                                tmem_load32(address + BN, w);
+                                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-                                for (int j = 0; j < 32; j += 4) {
-                                    float4 out = make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]),
-                                                             __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
-                                    if (args.subtract) {
-                                        const float4 old = *reinterpret_cast<const float4 *>(dst + j);
-                                        out = make_float4(old.x - out.x, old.y - out.y, old.z - out.z, old.w - out.w);
-                                    }
-                                    *reinterpret_cast<float4 *>(dst + j) = out;
-                                }
-                            } else {
                                 for (int j = 0; j < 32; ++j)
-                                    if (col + j < args.n)
-                                        dst[j] = args.subtract ? dst[j] - __uint_as_float(v[j]) : __uint_as_float(v[j]);
+                                    v[j] = __float_as_uint(__fadd_rn(__uint_as_float(v[j]), __uint_as_float(w[j])));
+                            } else {
+                                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                            }
+                            const unsigned long long col = n0 + chunk * 32;
+                            if (row < args.m && col < args.n) {
+                                float *dst = args.c + row * args.ldc + col;
+                                if (col + 32 <= args.n && vector) {
+#pragma unroll
+                                    for (int j = 0; j < 32; j += 4) {
+                                        float4 out = make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]),
+                                                                 __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
+                                        if (how != 0) {
+                                            const float4 old = *reinterpret_cast<const float4 *>(dst + j);
+                                            out = how < 0 ? make_float4(old.x - out.x, old.y - out.y, old.z - out.z, old.w - out.w)
+                                                          : make_float4(old.x + out.x, old.y + out.y, old.z + out.z, old.w + out.w);
+                                        }
+                                        *reinterpret_cast<float4 *>(dst + j) = out;
+                                    }
+                                } else {
+                                    for (int j = 0; j < 32; ++j) {
+                                        if (col + j >= args.n) break;
+                                        const float x = __uint_as_float(v[j]);
+                                        dst[j] = how == 0 ? x : (how < 0 ? dst[j] - x : dst[j] + x);
+                                    }
+                                }
                             }
                         }
+                        // buffer b may be refilled once all eight epilogue warps have read it
+                        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                        __syncwarp();
+                        if (lane == 0) pair_arrive(b ? empty1 : empty0);
                     }
-                    // accumulator b may be refilled once all eight epilogue warps have read it
-                    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                    __syncwarp();
-                    if (lane == 0) pair_arrive(b ? empty1 : empty0);
                 }
             }
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -559,7 +605,8 @@ namespace sci_cuda {
             pair_sync();  // neither CTA leaves while the pair's MMAs may still read its shared memory
             if (warp == 0) {
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN) : "memory");
+                asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * Sh::buffer)
+                             : "memory");
             }
         }
 
@@ -758,11 +805,12 @@ namespace sci_cuda {
 
         ProductArgs args{c, m, n, kp, ldc, subtract ? 1 : 0, ctx.status};
         if (whole_gpu && m >= 256 && pair_kernel_enabled()) {
-            // 256 x 256 tiles on CTA pairs, persistent: each CTA stages 128 rows of A and of B^T
+            // 256 x 256 (one term) or 256 x 128 tiles on CTA pairs, persistent
             Maps maps;
             std::memset(&maps, 0, sizeof(maps));
             for (int q = 0; q < terms; ++q) {
-                if (!make_map(&maps.a[q], at.t[q], m, kp, 128) || !make_map(&maps.b[q], bt.t[q], n, kp, 128))
+                const unsigned b_box = terms == 1 ? PairShape<1>::BN / 2 : PairShape<3>::BN / 2;
+                if (!make_map(&maps.a[q], at.t[q], m, kp, 128) || !make_map(&maps.b[q], bt.t[q], n, kp, b_box))
                     return ctx.fail(SCI_CUDA_ERROR_LAUNCH, "cuTensorMapEncodeTiled failed");
             }
             const void *kernel = terms == 1 ? reinterpret_cast<const void *>(&tensor_product_pair<1>)
@@ -774,7 +822,8 @@ namespace sci_cuda {
             if (int code = ctx.check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)),
                                      "raising the pair kernel's shared memory"))
                 return code;
-            unsigned tiles_m = static_cast<unsigned>((m + 255) / 256), tiles_n = static_cast<unsigned>((n + 255) / 256);
+            const unsigned bn = terms == 1 ? PairShape<1>::BN : PairShape<3>::BN;
+            unsigned tiles_m = static_cast<unsigned>((m + 255) / 256), tiles_n = static_cast<unsigned>((n + bn - 1) / bn);
             const unsigned long long tiles = 1ull * tiles_m * tiles_n;
             const unsigned long long pairs = std::min<unsigned long long>(tiles, pair_slots(kernel, smem, ctx.sms));
             void *params[] = {&maps, &args, &tiles_m, &tiles_n};

@@ -450,8 +450,7 @@ namespace sci_cuda {
     // therefore the correctly rounded value -- the one tanh_float returns, whose own error is about
     // 2^-50 -- unless tanh x lies within 2^-41 relative of a float rounding midpoint: the 29 bits of
     // t below the float's last place then lie within 2^12 of 100...0, and `rare` is set so that the
-    // caller recomputes with tanh_float. No infinity or NaN reaches it (|x| <= 1); a zero keeps its
-    // sign.
+    // caller recomputes with tanh_float. No infinity or NaN reaches it (|x| <= 1).
     __device__ __forceinline__ float tanh_float_near(float x, bool &rare) {
         const double a = static_cast<double>(x);
         const double u = __dmul_rn(a, a);
@@ -470,7 +469,8 @@ namespace sci_cuda {
         const double t = __fma_rn(__dmul_rn(a, u), g, a);
         const unsigned below = static_cast<unsigned>(__double2loint(t)) & 0x1fffffffu;
         rare = rare || below - 0x0ffff000u <= 0x2000u;
-        return static_cast<float>(t);
+        // t has x's sign except at x = -0, where the sum gives +0: the sign is taken from x
+        return copysignf(static_cast<float>(t), x);
     }
 
     // ---- two floats per instruction ----------------------------------------------------------------
