@@ -164,9 +164,10 @@ def test_product_at_full_size(device, oracle):
         got = dc.numpy().reshape(size, size)[rows]
         assert np.all(np.abs(got - want) <= product_bound(mode, size, s)), mode
         errors[mode] = np.linalg.norm(got - want) / np.linalg.norm(want)
-    # every tensor-core mode far more accurate than plain bf16; plain FP32 at FP32's level
-    assert errors[SPLIT3] < errors[BF16] / 10 and errors[SPLIT] < errors[BF16] / 10
-    assert errors[FP32] <= 1e-5
+    # split3 at FP32's accuracy (measured 1.9e-6 against plain FP32's 1.6e-6), split about 16 bits,
+    # bf16 about 8
+    assert errors[FP32] <= 4e-6 and errors[SPLIT3] <= 4e-6
+    assert errors[SPLIT] <= 2e-5 and errors[BF16] <= 4e-3
     for arr in (da, db, dc):
         arr.free()
 
