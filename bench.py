@@ -1345,7 +1345,10 @@ def main() -> int:
         if entry:
             traffic = entry["bytes_per_element"] * n
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak_gbs, "unit": "GB/s", "frac": achieved / peak_gbs,
-                "traffic": traffic, "kernel": f"chunk_stream ({dominant})", "peak_source": f"{peak_kind} hbm_gbs"}
+                "traffic": traffic, "kernel": f"chunk_stream ({dominant})", "peak_source": f"{peak_kind} hbm_gbs",
+                "traffic_source": "profiles/traffic.json: ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                                  "at 2^28 elements (this size), scaled to the element count; the output's last ~20 MB "
+                                  "are still in L2 when the kernel ends, so writes read slightly under 4 B/element"}
     kernels = {name: {"ms": mean_ms[name], "GB/s": BYTES_PER_ELEMENT[name] * n / (mean_ms[name] * 1e-3) / 1e9,
                       "frac": BYTES_PER_ELEMENT[name] * n / (mean_ms[name] * 1e-3) / 1e9 / peak_gbs}
                for name in names}
