@@ -48,38 +48,81 @@ namespace sci_cuda {
         struct Terms {
             __nv_bfloat16 *t[3];
         };
-        __device__ __forceinline__ void split_value(float v, int terms, const Terms &out, unsigned long long at) {
-            float rest = v;
+        // Eight K-consecutive values of one row split into the terms, one 16-byte store per term (`at`
+        // is a multiple of 8: Kp is a multiple of 64 and every term buffer 1024-byte aligned).
+        __device__ __forceinline__ void split_eight(const float (&v)[8], int terms, const Terms &out, unsigned long long at) {
+            float rest[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) rest[e] = v[e];
             for (int q = 0; q < terms; ++q) {
-                const __nv_bfloat16 h = __float2bfloat16_rn(rest);
-                out.t[q][at] = h;
-                rest = rest - __bfloat162float(h);
+                __align__(16) __nv_bfloat16 h[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    h[e] = __float2bfloat16_rn(rest[e]);
+                    rest[e] = rest[e] - __bfloat162float(h[e]);
+                }
+                *reinterpret_cast<uint4 *>(out.t[q] + at) = *reinterpret_cast<const uint4 *>(h);
             }
         }
+
+        // A (rows x k, pitch lda) into K-major terms, rows x kp: eight values per thread step, read as
+        // two 16-byte vectors where the row allows it.
         __global__ void split_rows(const float *__restrict__ a, unsigned long long lda, Terms out, int terms,
                                    unsigned long long rows, unsigned long long k, unsigned long long kp) {
-            const unsigned long long total = rows * kp;
+            const unsigned long long per_row = kp / 8, total = rows * per_row;
+            const bool vector = lda % 4 == 0 && reinterpret_cast<unsigned long long>(a) % 16 == 0;
             for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < total; i += 256ull * gridDim.x) {
-                const unsigned long long r = i / kp, c = i % kp;
-                split_value(c < k ? a[r * lda + c] : 0.0f, terms, out, i);
+                const unsigned long long r = i / per_row, c = (i - r * per_row) * 8;
+                const float *src = a + r * lda + c;
+                float v[8];
+                if (vector && c + 8 <= k) {
+                    const float4 lo = *reinterpret_cast<const float4 *>(src), hi = *reinterpret_cast<const float4 *>(src + 4);
+                    v[0] = lo.x, v[1] = lo.y, v[2] = lo.z, v[3] = lo.w, v[4] = hi.x, v[5] = hi.y, v[6] = hi.z, v[7] = hi.w;
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) v[e] = c + e < k ? src[e] : 0.0f;
+                }
+                split_eight(v, terms, out, r * kp + c);
             }
         }
 
         // B is K x N row-major (pitch ldb); its terms are the transpose, N x Kp, so both operands are
-        // K-major. 32 x 32 tiles through shared memory keep both sides coalesced.
-        __global__ void split_transpose(const float *__restrict__ b, unsigned long long ldb, Terms out, int terms,
-                                        unsigned long long k, unsigned long long n, unsigned long long kp) {
-            __shared__ float tile[32][33];
-            const unsigned long long k0 = blockIdx.y * 32ull, n0 = blockIdx.x * 32ull;
-            const unsigned tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
-            for (unsigned j = ty; j < 32; j += 8) {
-                const unsigned long long kk = k0 + j, nn = n0 + tx;
-                tile[j][tx] = (kk < k && nn < n) ? b[kk * ldb + nn] : 0.0f;
+        // K-major. 64 x 64 tiles through shared memory: read as 16-byte vectors along N, written as
+        // 16-byte vectors (eight K values) along K; the padded pitch keeps both passes free of bank
+        // conflicts but for the 2-way ones of the reads.
+        __global__ void __launch_bounds__(256) split_transpose(const float *__restrict__ b, unsigned long long ldb, Terms out,
+                                                               int terms, unsigned long long k, unsigned long long n,
+                                                               unsigned long long kp) {
+            __shared__ float tile[64][65];
+            const unsigned long long k0 = blockIdx.y * 64ull, n0 = blockIdx.x * 64ull;
+            const bool vector = ldb % 4 == 0 && reinterpret_cast<unsigned long long>(b) % 16 == 0;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const unsigned idx = threadIdx.x + 256u * u, kr = idx / 16, nv = idx % 16;
+                const unsigned long long kk = k0 + kr, nn = n0 + 4 * nv;
+                float v[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                if (kk < k) {
+                    const float *src = b + kk * ldb + nn;
+                    if (vector && nn + 4 <= n) {
+                        const float4 q = *reinterpret_cast<const float4 *>(src);
+                        v[0] = q.x, v[1] = q.y, v[2] = q.z, v[3] = q.w;
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) v[e] = nn + e < n ? src[e] : 0.0f;
+                    }
+                }
+#pragma unroll
+                for (int e = 0; e < 4; ++e) tile[kr][4 * nv + e] = v[e];
             }
             __syncthreads();
-            for (unsigned j = ty; j < 32; j += 8) {
-                const unsigned long long nn = n0 + j, kk = k0 + tx;
-                if (nn < n && kk < kp) split_value(tile[tx][j], terms, out, nn * kp + kk);
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const unsigned idx = threadIdx.x + 256u * u, nr = idx % 64, kv = idx / 64;
+                if (n0 + nr >= n) continue;
+                float v[8];
+#pragma unroll
+                for (int e = 0; e < 8; ++e) v[e] = tile[8 * kv + e][nr];
+                split_eight(v, terms, out, (n0 + nr) * kp + k0 + 8 * kv);
             }
         }
 
@@ -790,12 +833,13 @@ namespace sci_cuda {
             bt.t[q] = reinterpret_cast<__nv_bfloat16 *>(base + terms * a_bytes + q * b_bytes);
         }
         auto rows_of = [&](const float *x, unsigned long long ld, Terms out, unsigned long long rows) {
-            const unsigned grid = static_cast<unsigned>(std::min<unsigned long long>((rows * kp + 255) / 256, ctx.sms * 16ull));
+            const unsigned grid =
+                    static_cast<unsigned>(std::min<unsigned long long>((rows * (kp / 8) + 255) / 256, ctx.sms * 16ull));
             split_rows<<<grid, 256, 0, ctx.stream>>>(x, ld, out, terms, rows, k, kp);
         };
         auto columns_of = [&](const float *x, unsigned long long ld, Terms out, unsigned long long columns) {
-            const dim3 tgrid(static_cast<unsigned>((columns + 31) / 32), static_cast<unsigned>((kp + 31) / 32));
-            split_transpose<<<tgrid, dim3(32, 8), 0, ctx.stream>>>(x, ld, out, terms, k, columns, kp);
+            const dim3 tgrid(static_cast<unsigned>((columns + 63) / 64), static_cast<unsigned>(kp / 64));
+            split_transpose<<<tgrid, 256, 0, ctx.stream>>>(x, ld, out, terms, k, columns, kp);
         };
         if (a_t) columns_of(a, lda, at, m);
         else rows_of(a, lda, at, m);
