@@ -236,10 +236,9 @@ namespace sci_cuda {
             __shared__ bool stalled;
             __shared__ __align__(16) T jbuf[2][W];  // CTA 0: the row at the pivot position
             __shared__ unsigned long long jbuf_origin[2];
-            // the pivot of column j, by parity: the next column's is decided while rows finish this one
-            __shared__ __align__(16) T pivot_row[2][W];
-            __shared__ __align__(16) T displaced[2][W];
-            __shared__ unsigned long long pivot_at[2], pivot_origin[2], displaced_origin[2];
+            __shared__ __align__(16) T pivot_row[W];
+            __shared__ __align__(16) T displaced[W];
+            __shared__ unsigned long long pivot_at, pivot_origin, displaced_origin;
             __shared__ long long exchanges[W];  // CTA 0: piv[j0 + j]
 
             chain_wait();
@@ -265,22 +264,21 @@ namespace sci_cuda {
                 }
             }
 
-            // Column jn's candidates: each warp's best row at or below the diagonal (value_of(i) is
-            // row i's value in column jn), its row values and those of the row at the pivot position
-            // (CTA 0) staged for warp 0. complete(i) brings row i's registers to the start of column
-            // jn first (a row is only completed once).
-            auto propose = [&](auto span, const int jn, auto value_of, auto complete) {
+            // One column step, specialised on Q >= width - j: after j shifts only v[i][0, width - j)
+            // is live (the rest is zero), so publication, elimination and the shift stop at Q.
+            auto column = [&](auto span, const int j) {
                 constexpr int Q = decltype(span)::value;
-                const unsigned long long row_n = j0 + jn;
-                // candidacy; a NaN only stands at the pivot position itself, where the reference's
-                // comparisons against it all fail (decompose.hpp:35-38).
+                const int par = j & 1;
+                const unsigned long long row_j = j0 + j;
+                // 1. candidacy; a NaN only stands at the pivot position itself, where the reference's
+                //    comparisons against it all fail (decompose.hpp:35-38).
                 Key key = 0;
                 unsigned rel = kNoRow;
 #pragma unroll
                 for (int i = 0; i < R; ++i) {
-                    if (valid[i] && r[i] >= row_n) {
-                        const T m = fabs(value_of(i));
-                        const bool candidate = m == m || r[i] == row_n;
+                    if (valid[i] && r[i] >= row_j) {
+                        const T m = fabs(v[i][0]);
+                        const bool candidate = m == m || r[i] == row_j;
                         const Key k = candidate ? magnitude_key(m == m ? m : T(INFINITY)) : Key(0);
                         const unsigned at = static_cast<unsigned>(r[i] - j0);
                         if (k > key || (k == key && k != 0 && at < rel)) {
@@ -297,149 +295,118 @@ namespace sci_cuda {
 #pragma unroll
                 for (int i = 0; i < R; ++i) {
                     if (rel != kNoRow && r[i] - j0 == rel) {
-                        complete(i);
 #pragma unroll
                         for (int k = 0; k < Q; ++k) warp_values[warp][k] = v[i][k];
                         warp_origin[warp] = origin[i];
                     }
                 }
+                if (c == 0 && t == static_cast<unsigned>(j)) {  // row_j is row 0 of thread j in CTA 0
 #pragma unroll
-                for (int i = 0; i < R; ++i) {
-                    if (c == 0 && r[i] == row_n) {  // CTA 0 holds the pivot position's row
-                        complete(i);
+                    for (int k = 0; k < Q; ++k) jbuf[par][k] = v[0][k];
+                    jbuf_origin[par] = origin[0];
+                }
+                if (warp == 0) {
+                    named_sync(1, TH);
+                    Key k2 = lane < WARPS ? warp_key[lane] : Key(0);
+                    unsigned r2 = lane < WARPS ? warp_rel[lane] : kNoRow;
+                    best_of_warp(k2, r2);
+                    const unsigned source = r2 == kNoRow ? 0u : ((r2 - c * kCtaRows) % TH) / 32;
+                    // 2. lane q sends this CTA's candidate (and CTA 0 the pivot-position row) to CTA q,
+                    //    16 bytes per store; every CTA then waits for its own inbox to fill. A slot of
+                    //    parity par is rewritten two columns later, after every reader has taken its
+                    //    pivot from it (each CTA's next message follows its own pivot decision).
+                    constexpr unsigned kValueBytes = Q * sizeof(T), kMessage = kValueBytes + 32;
+                    static_assert(kValueBytes % 16 == 0, "16-byte stores");
+                    if (lane < static_cast<unsigned>(kClusterCtas)) {
+                        const unsigned bar = remote(&inbox_bar[par], lane);
+                        auto send = [&](const T *values, unsigned slot, unsigned long long k, unsigned long long o, unsigned rw) {
+                            const unsigned *words = reinterpret_cast<const unsigned *>(values);
+                            const unsigned base = remote(&inbox[par][slot][0], lane);
 #pragma unroll
-                        for (int k = 0; k < Q; ++k) jbuf[jn & 1][k] = v[i][k];
-                        jbuf_origin[jn & 1] = origin[i];
+                            for (unsigned m = 0; m < kValueBytes / 16; ++m)
+                                send16(base + 16 * m, words[4 * m], words[4 * m + 1], words[4 * m + 2], words[4 * m + 3], bar);
+                            const unsigned head = remote(&inbox_head[par][slot][0], lane);
+                            send16(head, static_cast<unsigned>(k), static_cast<unsigned>(k >> 32), static_cast<unsigned>(o),
+                                   static_cast<unsigned>(o >> 32), bar);
+                            send16(head + 16, rw, 0u, 0u, 0u, bar);
+                        };
+                        send(warp_values[source], c, static_cast<unsigned long long>(k2), warp_origin[source], r2);
+                        if (c == 0) send(jbuf[par], kClusterCtas, 0ull, jbuf_origin[par], 0u);
                     }
-                }
-            };
-
-            // Warp 0: column jn's pivot across the cluster, into the pivot buffers of parity jn & 1.
-            auto decide = [&](auto span, const int jn) {
-                constexpr int Q = decltype(span)::value;
-                const int par = jn & 1;
-                const unsigned long long row_n = j0 + jn;
-                named_sync(1, TH);
-                Key k2 = lane < WARPS ? warp_key[lane] : Key(0);
-                unsigned r2 = lane < WARPS ? warp_rel[lane] : kNoRow;
-                best_of_warp(k2, r2);
-                const unsigned source = r2 == kNoRow ? 0u : ((r2 - c * kCtaRows) % TH) / 32;
-                // lane q sends this CTA's candidate (and CTA 0 the pivot-position row) to CTA q, 16
-                // bytes per store; every CTA then waits for its own inbox to fill. A slot of parity par
-                // is rewritten two columns later, after every reader has taken its pivot from it (each
-                // CTA's next message follows its own pivot decision).
-                constexpr unsigned kValueBytes = Q * sizeof(T), kMessage = kValueBytes + 32;
-                static_assert(kValueBytes % 16 == 0, "16-byte stores");
-                if (lane < static_cast<unsigned>(kClusterCtas)) {
-                    const unsigned bar = remote(&inbox_bar[par], lane);
-                    auto send = [&](const T *values, unsigned slot, unsigned long long k, unsigned long long o, unsigned rw) {
-                        const unsigned *words = reinterpret_cast<const unsigned *>(values);
-                        const unsigned base = remote(&inbox[par][slot][0], lane);
+                    if (lane == 0) barrier_expect(&inbox_bar[par], (kClusterCtas + 1) * kMessage);
+                    const bool arrived = stalled ? false : barrier_wait(&inbox_bar[par], static_cast<unsigned>(j >> 1) & 1u);
+                    if (!arrived && lane == 0 && !stalled) {
+                        // a message never came: flag it, take no more waits, finish with what is here
+                        stalled = true;
+                        atomicOr(status, kStatusTimeout);
+                    }
+                    __syncwarp();
+                    // 3. the pivot, from the inbox
+                    Key k3 = 0;
+                    unsigned r3 = kNoRow;
+                    unsigned long long org = 0;
+                    if (lane < kClusterCtas) {
+                        k3 = static_cast<Key>(inbox_head[par][lane][0]);
+                        org = inbox_head[par][lane][1];
+                        r3 = static_cast<unsigned>(inbox_head[par][lane][2]);
+                    }
+                    T values[kClusterCtas];
 #pragma unroll
-                        for (unsigned m = 0; m < kValueBytes / 16; ++m)
-                            send16(base + 16 * m, words[4 * m], words[4 * m + 1], words[4 * m + 2], words[4 * m + 3], bar);
-                        const unsigned head = remote(&inbox_head[par][slot][0], lane);
-                        send16(head, static_cast<unsigned>(k), static_cast<unsigned>(k >> 32), static_cast<unsigned>(o),
-                               static_cast<unsigned>(o >> 32), bar);
-                        send16(head + 16, rw, 0u, 0u, 0u, bar);
-                    };
-                    send(warp_values[source], c, static_cast<unsigned long long>(k2), warp_origin[source], r2);
-                    if (c == 0) send(jbuf[par], kClusterCtas, 0ull, jbuf_origin[par], 0u);
-                }
-                if (lane == 0) barrier_expect(&inbox_bar[par], (kClusterCtas + 1) * kMessage);
-                const bool arrived = stalled ? false : barrier_wait(&inbox_bar[par], static_cast<unsigned>(jn >> 1) & 1u);
-                if (!arrived && lane == 0 && !stalled) {
-                    // a message never came: flag it, take no more waits, finish with what is here
-                    stalled = true;
-                    atomicOr(status, kStatusTimeout);
-                }
-                __syncwarp();
-                // the pivot, from the inbox
-                Key k3 = 0;
-                unsigned r3 = kNoRow;
-                unsigned long long org = 0;
-                if (lane < kClusterCtas) {
-                    k3 = static_cast<Key>(inbox_head[par][lane][0]);
-                    org = inbox_head[par][lane][1];
-                    r3 = static_cast<unsigned>(inbox_head[par][lane][2]);
-                }
-                T values[kClusterCtas];
+                    for (int q = 0; q < kClusterCtas; ++q) values[q] = lane < Q ? inbox[par][q][lane] : T(0);
+                    const T there = lane < Q ? inbox[par][kClusterCtas][lane] : T(0);
+                    const unsigned long long there_origin = inbox_head[par][kClusterCtas][1];
+                    best_of_warp(k3, r3);
+                    // the winner's CTA owns its row; no candidate cannot happen (row_j is one)
+                    const unsigned q = r3 == kNoRow ? 0u : r3 / kCtaRows;
+                    org = __shfl_sync(0xffffffffu, org, q);
+                    const unsigned long long prow = r3 == kNoRow ? row_j : j0 + r3;
+                    T value = values[0];
 #pragma unroll
-                for (int q = 0; q < kClusterCtas; ++q) values[q] = lane < Q ? inbox[par][q][lane] : T(0);
-                const T there = lane < Q ? inbox[par][kClusterCtas][lane] : T(0);
-                const unsigned long long there_origin = inbox_head[par][kClusterCtas][1];
-                best_of_warp(k3, r3);
-                // the winner's CTA owns its row; no candidate cannot happen (row_n is one)
-                const unsigned q = r3 == kNoRow ? 0u : r3 / kCtaRows;
-                org = __shfl_sync(0xffffffffu, org, q);
-                const unsigned long long prow = r3 == kNoRow ? row_n : j0 + r3;
-                T value = values[0];
-#pragma unroll
-                for (int s = 1; s < kClusterCtas; ++s)
-                    if (q == static_cast<unsigned>(s)) value = values[s];
-                const bool exchange = (prow - j0) / kCtaRows == c && prow != row_n;
-                if (lane < Q) {
-                    pivot_row[par][lane] = value;
-                    if (exchange) displaced[par][lane] = there;
+                    for (int s = 1; s < kClusterCtas; ++s)
+                        if (q == static_cast<unsigned>(s)) value = values[s];
+                    const bool exchange = (prow - j0) / kCtaRows == c && prow != row_j;
+                    if (lane < Q) {
+                        pivot_row[lane] = value;
+                        if (exchange) displaced[lane] = there;
+                    }
+                    if (lane == 0) {
+                        pivot_at = prow;
+                        pivot_origin = org;
+                        if (exchange) displaced_origin = there_origin;
+                        if (c == 0) exchanges[j] = static_cast<long long>(prow);
+                    }
+                } else {
+                    named_arrive(1, TH);
                 }
-                if (lane == 0) {
-                    pivot_at[par] = prow;
-                    pivot_origin[par] = org;
-                    if (exchange) displaced_origin[par] = there_origin;
-                    if (c == 0) exchanges[jn] = static_cast<long long>(prow);
-                }
-            };
-
-            // Column j with its pivot decided: the exchange, the multiplier and column j + 1 of every
-            // row below the diagonal first; then column j + 1's candidates and, on warp 0, its pivot,
-            // while the other warps finish column j's elimination (the rest of each row, the
-            // multipliers to the stage, the shift by one column). Live width: specialised on Q >=
-            // width - j, as only v[i][0, width - j) is live after j shifts.
-            auto step = [&](auto span, const int j) {
-                constexpr int Q = decltype(span)::value;
-                const int par = j & 1;
-                const unsigned long long row_j = j0 + j;
-                const unsigned long long prow = pivot_at[par];
-                const T diagonal = pivot_row[par][0];
-                T scale[R];
-                bool eliminate[R], done[R];
+                __syncthreads();
+                const unsigned long long prow = pivot_at;
 #pragma unroll
                 for (int i = 0; i < R; ++i) {
-                    done[i] = false;
                     if (r[i] == prow && prow != row_j) {
                         // this row moves to the pivot's old place: it takes the displaced row's values
 #pragma unroll
-                        for (int k = 0; k < Q; ++k) v[i][k] = displaced[par][k];
-                        origin[i] = displaced_origin[par];
+                        for (int k = 0; k < Q; ++k) v[i][k] = displaced[k];
+                        origin[i] = displaced_origin;
                     }
                     if (r[i] == row_j) {
                         // the pivot row is final: U's row j0 + j from column j0 + j on
 #pragma unroll
-                        for (int k = 0; k < Q; ++k) v[i][k] = pivot_row[par][k];
-                        origin[i] = pivot_origin[par];
+                        for (int k = 0; k < Q; ++k) v[i][k] = pivot_row[k];
+                        origin[i] = pivot_origin;
 #pragma unroll
                         for (int k = 0; k < Q; ++k)
                             if (k < width - j) a[origin[i] * n + row_j + k] = v[i][k];
                     }
-                    // eliminate below the pivot: l = a / pivot; a[k] -= l * pivot_row[k]; a zero pivot
-                    // leaves the column as it is (decompose.hpp:44-45)
-                    eliminate[i] = valid[i] && r[i] > row_j && diagonal != T(0);
-                    scale[i] = T(0);
-                    if (eliminate[i]) {
-                        scale[i] = div(v[i][0], diagonal);
-                        v[i][0] = scale[i];
-                        if constexpr (Q > 1) v[i][1] = sub(v[i][1], mul(scale[i], pivot_row[par][1]));
-                    }
-                }
-                // the rest of row i's column step
-                auto finish = [&](const int i) {
-                    if (done[i]) return;
-                    done[i] = true;
-                    if (eliminate[i]) {
-#pragma unroll
-                        for (int k = 2; k < Q; ++k) v[i][k] = sub(v[i][k], mul(scale[i], pivot_row[par][k]));
-                    }
+                    // 3. eliminate below the pivot: l = a / pivot; a[k] -= l * pivot_row[k]; a zero
+                    //    pivot leaves the column as it is (decompose.hpp:44-45)
                     if (valid[i] && r[i] > row_j) {
+                        const T diagonal = pivot_row[0];
+                        if (diagonal != T(0)) {
+                            const T l = div(v[i][0], diagonal);
+                            v[i][0] = l;
+#pragma unroll
+                            for (int k = 1; k < Q; ++k) v[i][k] = sub(v[i][k], mul(l, pivot_row[k]));
+                        }
                         if (origin[i] == r[i]) {
                             stage[j * P + static_cast<int>(r[i] - first)] = v[i][0];
                             mask[i] |= 1u << j;
@@ -450,17 +417,7 @@ namespace sci_cuda {
 #pragma unroll
                     for (int k = 0; k + 1 < Q; ++k) v[i][k] = v[i][k + 1];
                     v[i][Q - 1] = T(0);
-                };
-                if (j + 1 < width) {
-                    if constexpr (Q > 1) {
-                        propose(span, j + 1, [&](const int i) { return v[i][1]; }, finish);
-                        if (warp == 0) decide(span, j + 1);
-                        else named_arrive(1, TH);
-                    }
                 }
-#pragma unroll
-                for (int i = 0; i < R; ++i) finish(i);
-                __syncthreads();
             };
             if (t == 0) {
                 barrier_init(&inbox_bar[0], 1);
@@ -469,18 +426,13 @@ namespace sci_cuda {
                 asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
             }
             cluster_sync();  // every CTA's inbox barriers exist before the first message
-            // column 0's pivot, then the pipelined column steps
-            propose(Span<W>{}, 0, [&](const int i) { return v[i][0]; }, [](const int) {});
-            if (warp == 0) decide(Span<W>{}, 0);
-            else named_arrive(1, TH);
-            __syncthreads();
 #pragma unroll 1
             for (int j = 0; j < width; ++j) {
                 const int live = width - j;
-                if (live > 3 * W / 4) step(Span<W>{}, j);
-                else if (live > W / 2) step(Span<3 * W / 4>{}, j);
-                else if (live > W / 4) step(Span<W / 2>{}, j);
-                else step(Span<W / 4>{}, j);
+                if (live > 3 * W / 4) column(Span<W>{}, j);
+                else if (live > W / 2) column(Span<3 * W / 4>{}, j);
+                else if (live > W / 4) column(Span<W / 2>{}, j);
+                else column(Span<W / 4>{}, j);
             }
             // The staged multipliers, one row per warp store. Then every row's panel values sit at the
             // position the row started in; move the rows the exchanges displaced: all reads, a
