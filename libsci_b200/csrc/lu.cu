@@ -167,12 +167,6 @@ namespace sci_cuda {
         __device__ __forceinline__ void chain_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
         __device__ __forceinline__ void chain_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
-        __device__ __forceinline__ void named_sync(unsigned id, unsigned count) {
-            asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
-        }
-        __device__ __forceinline__ void named_arrive(unsigned id, unsigned count) {
-            asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory");
-        }
         // W values (128 bytes) from a 16-byte aligned address.
         __device__ __forceinline__ void load_row(const float *p, float *v) {
 #pragma unroll
@@ -205,13 +199,13 @@ namespace sci_cuda {
         // the end; one of a row the exchanges moved, and each pivot row of U, goes to global memory
         // at once. A final permutation moves the at most 2 W displaced rows to their positions.
         //
-        // Per column: each warp's best row is published in shared memory; warp 0 alone waits for
-        // them (a named barrier the other warps only arrive at) and pushes the CTA's candidate with
-        // its values into every CTA's inbox (st.async, counted on the receiver's mbarrier; CTA 0
-        // also pushes the row at the pivot position); warp 0 of every CTA waits for its own inbox
-        // to fill (a bounded wait), picks the pivot, and one CTA barrier hands it to every thread.
-        // Inboxes alternate by column parity; a CTA sends into one again only after its own pivot
-        // decision of the column in between, which needed every CTA's message of that column.
+        // Per column: each warp's best row is published in shared memory; after one CTA barrier,
+        // warp 0 pushes the CTA's candidate with its values into every CTA's inbox (st.async,
+        // counted on the receiver's mbarrier; CTA 0 also pushes the row at the pivot position);
+        // then every warp of every CTA waits for its own inbox to fill (a bounded wait), picks the
+        // pivot from it and eliminates, so the column takes one CTA barrier. Inboxes alternate by
+        // column parity; a CTA sends into one again only after the barrier of the column in
+        // between, which its warps reach only after reading every message of the earlier column.
         template <typename T, int CL, int ROWS>
         __global__ void __launch_bounds__(kPanelBlock, 1)
                 panel_factor(T *a, unsigned long long n, unsigned long long j0, int width, long long *piv, Movement *moved,
@@ -236,9 +230,6 @@ namespace sci_cuda {
             __shared__ bool stalled;
             __shared__ __align__(16) T jbuf[2][W];  // CTA 0: the row at the pivot position
             __shared__ unsigned long long jbuf_origin[2];
-            __shared__ __align__(16) T pivot_row[W];
-            __shared__ __align__(16) T displaced[W];
-            __shared__ unsigned long long pivot_at, pivot_origin, displaced_origin;
             __shared__ long long exchanges[W];  // CTA 0: piv[j0 + j]
 
             chain_wait();
@@ -305,27 +296,30 @@ namespace sci_cuda {
                     for (int k = 0; k < Q; ++k) jbuf[par][k] = v[0][k];
                     jbuf_origin[par] = origin[0];
                 }
+                __syncthreads();  // every warp's candidate (and CTA 0's pivot-position row) is staged
+                // 2. warp 0: the CTA's candidate; lane q sends it (and CTA 0 the pivot-position row) to
+                //    CTA q, 16 bytes per store, the message's words read from shared memory before the
+                //    first store. A slot of parity par is rewritten two columns later, after every
+                //    reader has taken its pivot from it (each CTA's next message follows its own
+                //    barrier of the column in between, which its warps reach only after reading).
+                constexpr unsigned kValueBytes = Q * sizeof(T), kMessage = kValueBytes + 32;
+                static_assert(kValueBytes % 16 == 0, "16-byte stores");
                 if (warp == 0) {
-                    named_sync(1, TH);
                     Key k2 = lane < WARPS ? warp_key[lane] : Key(0);
                     unsigned r2 = lane < WARPS ? warp_rel[lane] : kNoRow;
                     best_of_warp(k2, r2);
                     const unsigned source = r2 == kNoRow ? 0u : ((r2 - c * kCtaRows) % TH) / 32;
-                    // 2. lane q sends this CTA's candidate (and CTA 0 the pivot-position row) to CTA q,
-                    //    16 bytes per store; every CTA then waits for its own inbox to fill. A slot of
-                    //    parity par is rewritten two columns later, after every reader has taken its
-                    //    pivot from it (each CTA's next message follows its own pivot decision).
-                    constexpr unsigned kValueBytes = Q * sizeof(T), kMessage = kValueBytes + 32;
-                    static_assert(kValueBytes % 16 == 0, "16-byte stores");
                     if (lane < static_cast<unsigned>(kClusterCtas)) {
                         const unsigned bar = remote(&inbox_bar[par], lane);
                         auto send = [&](const T *values, unsigned slot, unsigned long long k, unsigned long long o, unsigned rw) {
-                            const unsigned *words = reinterpret_cast<const unsigned *>(values);
+                            uint4 words[kValueBytes / 16];
+#pragma unroll
+                            for (unsigned m = 0; m < kValueBytes / 16; ++m) words[m] = reinterpret_cast<const uint4 *>(values)[m];
                             const unsigned base = remote(&inbox[par][slot][0], lane);
+                            const unsigned head = remote(&inbox_head[par][slot][0], lane);
 #pragma unroll
                             for (unsigned m = 0; m < kValueBytes / 16; ++m)
-                                send16(base + 16 * m, words[4 * m], words[4 * m + 1], words[4 * m + 2], words[4 * m + 3], bar);
-                            const unsigned head = remote(&inbox_head[par][slot][0], lane);
+                                send16(base + 16 * m, words[m].x, words[m].y, words[m].z, words[m].w, bar);
                             send16(head, static_cast<unsigned>(k), static_cast<unsigned>(k >> 32), static_cast<unsigned>(o),
                                    static_cast<unsigned>(o >> 32), bar);
                             send16(head + 16, rw, 0u, 0u, 0u, bar);
@@ -334,70 +328,48 @@ namespace sci_cuda {
                         if (c == 0) send(jbuf[par], kClusterCtas, 0ull, jbuf_origin[par], 0u);
                     }
                     if (lane == 0) barrier_expect(&inbox_bar[par], (kClusterCtas + 1) * kMessage);
-                    const bool arrived = stalled ? false : barrier_wait(&inbox_bar[par], static_cast<unsigned>(j >> 1) & 1u);
-                    if (!arrived && lane == 0 && !stalled) {
-                        // a message never came: flag it, take no more waits, finish with what is here
-                        stalled = true;
-                        atomicOr(status, kStatusTimeout);
-                    }
-                    __syncwarp();
-                    // 3. the pivot, from the inbox
-                    Key k3 = 0;
-                    unsigned r3 = kNoRow;
-                    unsigned long long org = 0;
-                    if (lane < kClusterCtas) {
-                        k3 = static_cast<Key>(inbox_head[par][lane][0]);
-                        org = inbox_head[par][lane][1];
-                        r3 = static_cast<unsigned>(inbox_head[par][lane][2]);
-                    }
-                    T values[kClusterCtas];
-#pragma unroll
-                    for (int q = 0; q < kClusterCtas; ++q) values[q] = lane < Q ? inbox[par][q][lane] : T(0);
-                    const T there = lane < Q ? inbox[par][kClusterCtas][lane] : T(0);
-                    const unsigned long long there_origin = inbox_head[par][kClusterCtas][1];
-                    best_of_warp(k3, r3);
-                    // the winner's CTA owns its row; no candidate cannot happen (row_j is one)
-                    const unsigned q = r3 == kNoRow ? 0u : r3 / kCtaRows;
-                    org = __shfl_sync(0xffffffffu, org, q);
-                    const unsigned long long prow = r3 == kNoRow ? row_j : j0 + r3;
-                    T value = values[0];
-#pragma unroll
-                    for (int s = 1; s < kClusterCtas; ++s)
-                        if (q == static_cast<unsigned>(s)) value = values[s];
-                    const bool exchange = (prow - j0) / kCtaRows == c && prow != row_j;
-                    if (lane < Q) {
-                        pivot_row[lane] = value;
-                        if (exchange) displaced[lane] = there;
-                    }
-                    if (lane == 0) {
-                        pivot_at = prow;
-                        pivot_origin = org;
-                        if (exchange) displaced_origin = there_origin;
-                        if (c == 0) exchanges[j] = static_cast<long long>(prow);
-                    }
-                } else {
-                    named_arrive(1, TH);
                 }
-                __syncthreads();
-                const unsigned long long prow = pivot_at;
+                // 3. every warp waits for its CTA's inbox to fill (a bounded wait: one that runs out
+                //    flags the status, and no later column waits) and takes the pivot from it
+                if (!stalled && !barrier_wait(&inbox_bar[par], static_cast<unsigned>(j >> 1) & 1u) && lane == 0) {
+                    stalled = true;
+                    atomicOr(status, kStatusTimeout);
+                }
+                __syncwarp();
+                Key k3 = 0;
+                unsigned r3 = kNoRow;
+                unsigned long long org = 0;
+                if (lane < kClusterCtas) {
+                    k3 = static_cast<Key>(inbox_head[par][lane][0]);
+                    org = inbox_head[par][lane][1];
+                    r3 = static_cast<unsigned>(inbox_head[par][lane][2]);
+                }
+                best_of_warp(k3, r3);
+                // the winner's CTA owns its row; no candidate cannot happen (row_j is one)
+                const unsigned q = r3 == kNoRow ? 0u : r3 / kCtaRows;
+                org = __shfl_sync(0xffffffffu, org, q);
+                const unsigned long long prow = r3 == kNoRow ? row_j : j0 + r3;
+                const T *const pivot_row = inbox[par][q];
+                if (c == 0 && t == 0) exchanges[j] = static_cast<long long>(prow);
+                constexpr int E = 16 / sizeof(T);  // pivot-row values per 16-byte load
 #pragma unroll
                 for (int i = 0; i < R; ++i) {
                     if (r[i] == prow && prow != row_j) {
                         // this row moves to the pivot's old place: it takes the displaced row's values
 #pragma unroll
-                        for (int k = 0; k < Q; ++k) v[i][k] = displaced[k];
-                        origin[i] = displaced_origin;
+                        for (int k = 0; k < Q; k += E) load16(&inbox[par][kClusterCtas][k], &v[i][k]);
+                        origin[i] = inbox_head[par][kClusterCtas][1];
                     }
                     if (r[i] == row_j) {
                         // the pivot row is final: U's row j0 + j from column j0 + j on
 #pragma unroll
-                        for (int k = 0; k < Q; ++k) v[i][k] = pivot_row[k];
-                        origin[i] = pivot_origin;
+                        for (int k = 0; k < Q; k += E) load16(pivot_row + k, &v[i][k]);
+                        origin[i] = org;
 #pragma unroll
                         for (int k = 0; k < Q; ++k)
                             if (k < width - j) a[origin[i] * n + row_j + k] = v[i][k];
                     }
-                    // 3. eliminate below the pivot: l = a / pivot; a[k] -= l * pivot_row[k]; a zero
+                    // 4. eliminate below the pivot: l = a / pivot; a[k] -= l * pivot_row[k]; a zero
                     //    pivot leaves the column as it is (decompose.hpp:44-45)
                     if (valid[i] && r[i] > row_j) {
                         const T diagonal = pivot_row[0];
@@ -405,7 +377,13 @@ namespace sci_cuda {
                             const T l = div(v[i][0], diagonal);
                             v[i][0] = l;
 #pragma unroll
-                            for (int k = 1; k < Q; ++k) v[i][k] = sub(v[i][k], mul(l, pivot_row[k]));
+                            for (int k0 = 0; k0 < Q; k0 += E) {
+                                T p[E];
+                                load16(pivot_row + k0, p);
+#pragma unroll
+                                for (int e = 0; e < E; ++e)
+                                    if (k0 + e >= 1) v[i][k0 + e] = sub(v[i][k0 + e], mul(l, p[e]));
+                            }
                         }
                         if (origin[i] == r[i]) {
                             stage[j * P + static_cast<int>(r[i] - first)] = v[i][0];
