@@ -167,6 +167,30 @@ namespace sci_cuda {
         __device__ __forceinline__ void chain_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
         __device__ __forceinline__ void chain_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 
+        // v[k] -= l * p[k] for k in [0, Q), each product and difference rounded on its own as in
+        // the reference's column step (decompose.hpp:50-55); p is 16-byte aligned in shared memory.
+        // Float rows go two columns per instruction (mul / sub .rn.f32x2 round each lane exactly as
+        // the one-lane instructions do). Column 0 is computed too: the caller overwrites it.
+        template <int Q> __device__ __forceinline__ void eliminate_row(float *v, float l, const float *p) {
+            const Pair lp = pair(l);
+#pragma unroll
+            for (int k0 = 0; k0 < Q; k0 += 4) {
+                const float4 q = *reinterpret_cast<const float4 *>(p + k0);
+                const Pair d0 = sub(pair(v[k0], v[k0 + 1]), mul(lp, pair(q.x, q.y)));
+                const Pair d1 = sub(pair(v[k0 + 2], v[k0 + 3]), mul(lp, pair(q.z, q.w)));
+                unpair(d0, v[k0], v[k0 + 1]);
+                unpair(d1, v[k0 + 2], v[k0 + 3]);
+            }
+        }
+        template <int Q> __device__ __forceinline__ void eliminate_row(double *v, double l, const double *p) {
+#pragma unroll
+            for (int k0 = 0; k0 < Q; k0 += 2) {
+                const double2 q = *reinterpret_cast<const double2 *>(p + k0);
+                v[k0] = sub(v[k0], mul(l, q.x));
+                v[k0 + 1] = sub(v[k0 + 1], mul(l, q.y));
+            }
+        }
+
         // W values (128 bytes) from a 16-byte aligned address.
         __device__ __forceinline__ void load_row(const float *p, float *v) {
 #pragma unroll
@@ -222,10 +246,11 @@ namespace sci_cuda {
             __shared__ unsigned long long warp_origin[WARPS];
             __shared__ __align__(16) T warp_values[WARPS][W];
             // The inbox, by column parity: slot q < CL holds CTA q's candidate (its values, then a
-            // 32-byte head: key, origin, row), slot CL the row at the pivot position (from CTA 0).
+            // 16-byte head: key, then origin and row), slot CL the row at the pivot position (from
+            // CTA 0). Rows are below 2^32 (n <= kPanelRows), so origin and row take 32 bits each.
             // Senders write it with st.async; inbox_bar[parity] counts the bytes.
             __shared__ __align__(16) T inbox[2][kClusterCtas + 1][W];
-            __shared__ __align__(16) unsigned long long inbox_head[2][kClusterCtas + 1][4];
+            __shared__ __align__(16) unsigned long long inbox_head[2][kClusterCtas + 1][2];
             __shared__ __align__(8) unsigned long long inbox_bar[2];
             __shared__ bool stalled;
             __shared__ __align__(16) T jbuf[2][W];  // CTA 0: the row at the pivot position
@@ -297,37 +322,37 @@ namespace sci_cuda {
                     jbuf_origin[par] = origin[0];
                 }
                 __syncthreads();  // every warp's candidate (and CTA 0's pivot-position row) is staged
-                // 2. warp 0: the CTA's candidate; lane q sends it (and CTA 0 the pivot-position row) to
-                //    CTA q, 16 bytes per store, the message's words read from shared memory before the
-                //    first store. A slot of parity par is rewritten two columns later, after every
+                // 2. warp 0: the CTA's candidate; lane q sends it to CTA q (and lane q of CTA 0's warp 1
+                //    the pivot-position row), 16 bytes per store, the message's words read from shared
+                //    memory before the first store. A slot of parity par is rewritten two columns later, after every
                 //    reader has taken its pivot from it (each CTA's next message follows its own
                 //    barrier of the column in between, which its warps reach only after reading).
-                constexpr unsigned kValueBytes = Q * sizeof(T), kMessage = kValueBytes + 32;
+                constexpr unsigned kValueBytes = Q * sizeof(T), kMessage = kValueBytes + 16;
                 static_assert(kValueBytes % 16 == 0, "16-byte stores");
+                // One message: the values, then a 16-byte head (key; origin and row, 32 bits each).
+                auto send = [&](const T *values, unsigned slot, unsigned long long k, unsigned long long o, unsigned rw) {
+                    const unsigned bar = remote(&inbox_bar[par], lane);
+                    uint4 words[kValueBytes / 16];
+#pragma unroll
+                    for (unsigned m = 0; m < kValueBytes / 16; ++m) words[m] = reinterpret_cast<const uint4 *>(values)[m];
+                    const unsigned base = remote(&inbox[par][slot][0], lane);
+                    const unsigned head = remote(&inbox_head[par][slot][0], lane);
+#pragma unroll
+                    for (unsigned m = 0; m < kValueBytes / 16; ++m)
+                        send16(base + 16 * m, words[m].x, words[m].y, words[m].z, words[m].w, bar);
+                    send16(head, static_cast<unsigned>(k), static_cast<unsigned>(k >> 32), static_cast<unsigned>(o), rw, bar);
+                };
                 if (warp == 0) {
                     Key k2 = lane < WARPS ? warp_key[lane] : Key(0);
                     unsigned r2 = lane < WARPS ? warp_rel[lane] : kNoRow;
                     best_of_warp(k2, r2);
                     const unsigned source = r2 == kNoRow ? 0u : ((r2 - c * kCtaRows) % TH) / 32;
-                    if (lane < static_cast<unsigned>(kClusterCtas)) {
-                        const unsigned bar = remote(&inbox_bar[par], lane);
-                        auto send = [&](const T *values, unsigned slot, unsigned long long k, unsigned long long o, unsigned rw) {
-                            uint4 words[kValueBytes / 16];
-#pragma unroll
-                            for (unsigned m = 0; m < kValueBytes / 16; ++m) words[m] = reinterpret_cast<const uint4 *>(values)[m];
-                            const unsigned base = remote(&inbox[par][slot][0], lane);
-                            const unsigned head = remote(&inbox_head[par][slot][0], lane);
-#pragma unroll
-                            for (unsigned m = 0; m < kValueBytes / 16; ++m)
-                                send16(base + 16 * m, words[m].x, words[m].y, words[m].z, words[m].w, bar);
-                            send16(head, static_cast<unsigned>(k), static_cast<unsigned>(k >> 32), static_cast<unsigned>(o),
-                                   static_cast<unsigned>(o >> 32), bar);
-                            send16(head + 16, rw, 0u, 0u, 0u, bar);
-                        };
+                    if (lane < static_cast<unsigned>(kClusterCtas))
                         send(warp_values[source], c, static_cast<unsigned long long>(k2), warp_origin[source], r2);
-                        if (c == 0) send(jbuf[par], kClusterCtas, 0ull, jbuf_origin[par], 0u);
-                    }
                     if (lane == 0) barrier_expect(&inbox_bar[par], (kClusterCtas + 1) * kMessage);
+                } else if (warp == 1 && c == 0 && lane < static_cast<unsigned>(kClusterCtas)) {
+                    // CTA 0's pivot-position row, from another warp (another scheduler) at the same time
+                    send(jbuf[par], kClusterCtas, 0ull, jbuf_origin[par], 0u);
                 }
                 // 3. every warp waits for its CTA's inbox to fill (a bounded wait: one that runs out
                 //    flags the status, and no later column waits) and takes the pivot from it
@@ -341,8 +366,9 @@ namespace sci_cuda {
                 unsigned long long org = 0;
                 if (lane < kClusterCtas) {
                     k3 = static_cast<Key>(inbox_head[par][lane][0]);
-                    org = inbox_head[par][lane][1];
-                    r3 = static_cast<unsigned>(inbox_head[par][lane][2]);
+                    const unsigned long long where = inbox_head[par][lane][1];
+                    org = where & 0xFFFFFFFFull;
+                    r3 = static_cast<unsigned>(where >> 32);
                 }
                 best_of_warp(k3, r3);
                 // the winner's CTA owns its row; no candidate cannot happen (row_j is one)
@@ -358,7 +384,7 @@ namespace sci_cuda {
                         // this row moves to the pivot's old place: it takes the displaced row's values
 #pragma unroll
                         for (int k = 0; k < Q; k += E) load16(&inbox[par][kClusterCtas][k], &v[i][k]);
-                        origin[i] = inbox_head[par][kClusterCtas][1];
+                        origin[i] = inbox_head[par][kClusterCtas][1] & 0xFFFFFFFFull;
                     }
                     if (r[i] == row_j) {
                         // the pivot row is final: U's row j0 + j from column j0 + j on
@@ -375,15 +401,8 @@ namespace sci_cuda {
                         const T diagonal = pivot_row[0];
                         if (diagonal != T(0)) {
                             const T l = div(v[i][0], diagonal);
+                            eliminate_row<Q>(v[i], l, pivot_row);
                             v[i][0] = l;
-#pragma unroll
-                            for (int k0 = 0; k0 < Q; k0 += E) {
-                                T p[E];
-                                load16(pivot_row + k0, p);
-#pragma unroll
-                                for (int e = 0; e < E; ++e)
-                                    if (k0 + e >= 1) v[i][k0 + e] = sub(v[i][k0 + e], mul(l, p[e]));
-                            }
                         }
                         if (origin[i] == r[i]) {
                             stage[j * P + static_cast<int>(r[i] - first)] = v[i][0];
@@ -1038,67 +1057,133 @@ namespace sci_cuda {
                 if (c4 + j < w) c[gr * ldc + c4 + j] = sub(c[gr * ldc + c4 + j], acc[j]);
         }
 
-        // r = b - A x in FP64, the refinement's residual: 32 rows (blockIdx.x) by 16 columns of x
-        // (blockIdx.y) per CTA. A is streamed through shared memory in slices of 64 columns, coalesced,
-        // the next slice's loads issued before the current one is used; warp w sums the slice's columns
-        // [8 w, 8 w + 8) for row = lane (x's entries are then broadcasts); at the end the eight warps'
-        // sums are added in warp order. A is read once: the kernel is bound by HBM.
-        constexpr int kResidualRows = 32, kResidualSlice = 64, kResidualColumns = 16;
-        __global__ void __launch_bounds__(256, 2) residual_rows(const double *__restrict__ a, const double *__restrict__ x,
-                                                                const double *__restrict__ b, double *__restrict__ r,
-                                                                unsigned long long n, unsigned long long width) {
-            constexpr int R = kResidualRows, K = kResidualSlice, C = kResidualColumns, PA = K + 1;
-            constexpr int LA = R * K / 256, LX = K * C / 256;
-            __shared__ double as[R * PA];  // the slice of A, then the warps' sums (half the columns at a time)
-            __shared__ double xs[K * C];
-            const unsigned long long r0 = blockIdx.x * 1ull * R, c0 = blockIdx.y * 1ull * C;
-            const int t = threadIdx.x, lane = t % 32, warp = t / 32;
-            double na[LA], nx[LX];
-            auto load = [&](unsigned long long k0) {
-    #pragma unroll
-                for (int u = 0; u < LA; ++u) {
-                    const int i = t + u * 256, row = i / K, k = i % K;
-                    na[u] = (r0 + row < n && k0 + k < n) ? a[(r0 + row) * n + k0 + k] : 0.0;
+        // r = b - A x in FP64, the refinement's residual. One CTA of 512 threads per 64 rows
+        // (blockIdx.x) and 16 columns of x (blockIdx.y); A and x stream through shared memory in
+        // slices of 64 columns (cp.async, four slices in flight: 160 KB), so A is read once, from HBM,
+        // with enough bytes in flight per SM to keep it busy. Warp w of a slice takes its columns
+        // [4 w, 4 w + 4); lane (g = lane % 16, h = lane / 16) accumulates rows g, g + 16, g + 32,
+        // g + 48 against columns [8 h, 8 h + 8) of x: 32 FP64 FMAs per six 16-byte shared loads.
+        // A's slice rows are stored with their 16-byte chunks XOR-swizzled by row % 8, so the
+        // sixteen rows a load instruction reads fall on distinct banks. At the end the sixteen
+        // warps' partial sums are added in warp order: the result is deterministic.
+        constexpr int kResidualRows = 64, kResidualSlice = 64, kResidualColumns = 16, kResidualStages = 4;
+        constexpr int kResidualThreads = 512;
+        constexpr size_t kResidualShared =
+                sizeof(double) * kResidualStages * (kResidualRows * kResidualSlice + kResidualSlice * kResidualColumns);
+        static_assert(sizeof(double) * 16 * kResidualRows * kResidualColumns <= kResidualShared, "partials fit");
+
+        // cp.async of `bytes` (16, 8 or 0: the rest of the 16 / 8 bytes zero-filled)
+        __device__ __forceinline__ void residual_copy16(void *shared, const void *global, unsigned bytes) {
+            const unsigned address = static_cast<unsigned>(__cvta_generic_to_shared(shared));
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(address), "l"(global), "r"(bytes) : "memory");
+        }
+        __device__ __forceinline__ void residual_copy8(void *shared, const void *global, unsigned bytes) {
+            const unsigned address = static_cast<unsigned>(__cvta_generic_to_shared(shared));
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(address), "l"(global), "r"(bytes) : "memory");
+        }
+
+        __global__ void __launch_bounds__(kResidualThreads, 1)
+                residual_tiles(const double *__restrict__ a, const double *__restrict__ x, const double *__restrict__ b,
+                               double *__restrict__ r, unsigned long long n, unsigned long long width) {
+            constexpr int RW = kResidualRows, K = kResidualSlice, C = kResidualColumns, S = kResidualStages;
+            constexpr int CH = K / 2;  // 16-byte chunks per slice row
+            extern __shared__ __align__(16) double residual_shared[];
+            double *const as = residual_shared;             // S slices of A: [row][chunk ^ (row % 8)]
+            double *const xs = residual_shared + S * RW * K;  // S slices of x: [k][c]
+            const unsigned long long r0 = blockIdx.x * 1ull * RW, c0 = blockIdx.y * 1ull * C;
+            const int t = threadIdx.x, lane = t % 32, warp = t / 32, g = lane % 16, h = lane / 16;
+            // 16-byte copies of A when every row starts on a 16-byte boundary
+            const bool chunks = n % 2 == 0 && (reinterpret_cast<unsigned long long>(a) & 15) == 0;
+            const unsigned long long slices = (n + K - 1) / K;
+            auto issue = [&](int stage, unsigned long long k0) {
+                double *const at = as + stage * RW * K;
+#pragma unroll
+                for (int u = 0; u < RW * CH / kResidualThreads; ++u) {
+                    const int q = t + u * kResidualThreads, row = q / CH, c = q % CH;
+                    const unsigned long long gr = r0 + row, gk = k0 + 2ull * c;
+                    double *const dst = at + row * K + 2 * (c ^ (row & 7));
+                    if (chunks) {
+                        const unsigned bytes = gr < n && gk < n ? (gk + 1 < n ? 16u : 8u) : 0u;
+                        residual_copy16(dst, bytes ? a + gr * n + gk : a, bytes);
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < 2; ++e) {
+                            const bool inside = gr < n && gk + e < n;
+                            residual_copy8(dst + e, inside ? a + gr * n + gk + e : a, inside ? 8u : 0u);
+                        }
+                    }
                 }
-    #pragma unroll
-                for (int u = 0; u < LX; ++u) {
-                    const int i = t + u * 256, k = i / C, c = i % C;
-                    nx[u] = (k0 + k < n && c0 + c < width) ? x[(k0 + k) * width + c0 + c] : 0.0;
+                double *const xt = xs + stage * K * C;
+#pragma unroll
+                for (int u = 0; u < K * C / kResidualThreads; ++u) {
+                    const int q = t + u * kResidualThreads, k = q / C, c = q % C;
+                    const bool inside = k0 + k < n && c0 + c < width;
+                    residual_copy8(xt + q, inside ? x + (k0 + k) * width + c0 + c : x, inside ? 8u : 0u);
                 }
+                asm volatile("cp.async.commit_group;" ::: "memory");
             };
-            double acc[C];
-    #pragma unroll
-            for (int c = 0; c < C; ++c) acc[c] = 0.0;
-            load(0);
-            for (unsigned long long k0 = 0; k0 < n; k0 += K) {
-                __syncthreads();  // the previous slice is used up
-    #pragma unroll
-                for (int u = 0; u < LA; ++u) {
-                    const int i = t + u * 256;
-                    as[(i / K) * PA + i % K] = na[u];
-                }
-    #pragma unroll
-                for (int u = 0; u < LX; ++u) xs[t + u * 256] = nx[u];
-                __syncthreads();
-                if (k0 + K < n) load(k0 + K);
-    #pragma unroll
-                for (int k = 8 * warp; k < 8 * warp + 8; ++k) {
-                    const double av = as[lane * PA + k];
-    #pragma unroll
-                    for (int c = 0; c < C; ++c) acc[c] = fma(av, xs[k * C + c], acc[c]);
+#pragma unroll
+            for (int s = 0; s < S - 1; ++s) {
+                if (s < static_cast<long long>(slices)) issue(s, s * 1ull * K);
+                else asm volatile("cp.async.commit_group;" ::: "memory");
+            }
+            double acc[4][8];
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[p][j] = 0.0;
+            for (unsigned long long it = 0; it < slices; ++it) {
+                asm volatile("cp.async.wait_group %0;" ::"n"(S - 2) : "memory");
+                __syncthreads();  // slice `it` is in place; slice it - 1's stage is free again
+                const unsigned long long next = it + S - 1;
+                if (next < slices) issue(static_cast<int>(next % S), next * K);
+                else asm volatile("cp.async.commit_group;" ::: "memory");
+                const int stage = static_cast<int>(it % S);
+                const double *const at = as + stage * RW * K;
+                const double *const xt = xs + stage * K * C;
+#pragma unroll
+                for (int half = 0; half < 2; ++half) {
+                    const int c = 2 * warp + half;  // this warp's chunk: columns 2 c, 2 c + 1 of the slice
+                    double2 av[4];
+#pragma unroll
+                    for (int p = 0; p < 4; ++p) {
+                        const int row = g + 16 * p;
+                        av[p] = *reinterpret_cast<const double2 *>(at + row * K + 2 * (c ^ (row & 7)));
+                    }
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        double xv[8];
+                        const double2 *const xp = reinterpret_cast<const double2 *>(xt + (2 * c + e) * C + 8 * h);
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const double2 pair = xp[j];
+                            xv[2 * j] = pair.x;
+                            xv[2 * j + 1] = pair.y;
+                        }
+#pragma unroll
+                        for (int p = 0; p < 4; ++p) {
+                            const double av_e = e == 0 ? av[p].x : av[p].y;
+#pragma unroll
+                            for (int j = 0; j < 8; ++j) acc[p][j] = fma(av_e, xv[j], acc[p][j]);
+                        }
+                    }
                 }
             }
-            // r = b - (warp 0 + warp 1 + ... + warp 7), eight columns at a time through `as`
-    #pragma unroll
-            for (int half = 0; half < 2; ++half) {
-                __syncthreads();
-    #pragma unroll
-                for (int c = 0; c < C / 2; ++c) as[(warp * R + lane) * (C / 2) + c] = acc[half * (C / 2) + c];
-                __syncthreads();
-                const int row = t / (C / 2), c = half * (C / 2) + t % (C / 2);
+            // the warps' partial sums, then r = b - (warp 0 + warp 1 + ... + warp 15)
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+            __syncthreads();
+            double *const partial = residual_shared;  // [warp][row][column]
+#pragma unroll
+            for (int p = 0; p < 4; ++p)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) partial[(warp * RW + g + 16 * p) * C + 8 * h + j] = acc[p][j];
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < RW * C / kResidualThreads; ++u) {
+                const int q = t + u * kResidualThreads, row = q / C, c = q % C;
                 double sum = 0.0;
-    #pragma unroll
-                for (int w = 0; w < 8; ++w) sum += as[(w * R + row) * (C / 2) + t % (C / 2)];
+#pragma unroll
+                for (int w = 0; w < kResidualThreads / 32; ++w) sum += partial[w * RW * C + q];
                 const unsigned long long gr = r0 + row, gc = c0 + c;
                 if (gr < n && gc < width) r[gr * width + gc] = b[gr * width + gc] - sum;
             }
@@ -1392,7 +1477,6 @@ namespace sci_cuda {
         // Every CTA is resident (cooperative launch), and every wait is bounded: one that runs out
         // sets the timeout status and ends its CTA, so the CTAs after it end the same way.
         constexpr int kSweepThreads = 4 * kSolveBlock;  // four quarters of the block's 128 rows
-        constexpr int kSweepColumns = 16;
         constexpr unsigned kSweepWaitLimit = 1u << 22;
 
         __device__ __forceinline__ unsigned load_acquire(const unsigned *p) {
@@ -1413,12 +1497,12 @@ namespace sci_cuda {
             asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
         }
 
-        // acc[0..15] += a * v[0..15], two columns per packed instruction
-        __device__ __forceinline__ void axpy16(float a, const float *v, Pair *acc) {
+        // acc[0..C) += a * v[0..C), two columns per packed instruction
+        template <int C> __device__ __forceinline__ void axpy(float a, const float *v, Pair *acc) {
             const Pair pa = pair(a);
             const Pair *pv = reinterpret_cast<const Pair *>(v);
 #pragma unroll
-            for (int c = 0; c < kSweepColumns / 2; ++c) acc[c] = fma_(pa, pv[c], acc[c]);
+            for (int c = 0; c < C / 2; ++c) acc[c] = fma_(pa, pv[c], acc[c]);
         }
 
         // 16-byte asynchronous copy global -> shared through L2 only (no stale L1 line of another SM's
@@ -1433,12 +1517,13 @@ namespace sci_cuda {
             asm volatile("cp.async.wait_group %0;" ::"n"(pending) : "memory");
         }
 
-        template <bool upper>
+        template <bool upper, int C>
         __global__ void __launch_bounds__(kSweepThreads, 1)
         sweep(const float *__restrict__ lu, const float *__restrict__ inv, const float *__restrict__ couple, unsigned n,
               unsigned width, unsigned groups, const float *__restrict__ in, float *out, unsigned *flags, unsigned epoch,
               int *status) {
-            constexpr int B = kSolveBlock, C = kSweepColumns;
+            static_assert(C == 8 || C == 16, "column groups of 8 or 16");
+            constexpr int B = kSolveBlock;
             constexpr int P = C + 4;  // pitch of a staged block row: 16-byte aligned rows
             constexpr int Q = C + 1;  // pitch of a partial-sum row
             constexpr int V = B * C / kSweepThreads;  // block elements per thread in the row-major mapping
@@ -1504,15 +1589,18 @@ namespace sci_cuda {
                 return !stop;
             };
             // Starts copying block row row_of(step)'s results into `target` (row-major mapping: thread
-            // = row t / 4, columns 4 (t % 4) .. + 3), or loads them directly when rows are not 16-byte
-            // aligned (a width not a multiple of 4, or a caller's unaligned buffer).
+            // = row t / (C / 4), columns 4 (t % (C / 4)) .. + 3; B C / 4 threads copy), or loads them
+            // directly when rows are not 16-byte aligned (a width not a multiple of 4, or a caller's
+            // unaligned buffer).
             auto fetch = [&](unsigned step, float *target) {
                 const unsigned sj = row_of(step) * B;
                 if (width % 4 == 0 && (reinterpret_cast<unsigned long long>(out) & 15) == 0) {
-                    const unsigned k = t / 4, c = 4 * (t % 4);
-                    const bool inside = sj + k < n && c0 + c < width;
-                    const float *source = out + (inside ? static_cast<unsigned long long>(sj + k) * width + c0 + c : 0ull);
-                    copy16_async(target + k * P + c, source, inside);
+                    const unsigned k = t / (C / 4), c = 4 * (t % (C / 4));
+                    if (t < B * C / 4) {
+                        const bool inside = sj + k < n && c0 + c < width;
+                        const float *source = out + (inside ? static_cast<unsigned long long>(sj + k) * width + c0 + c : 0ull);
+                        copy16_async(target + k * P + c, source, inside);
+                    }
                 } else {
 #pragma unroll
                     for (int v = 0; v < V; ++v) {
@@ -1531,10 +1619,10 @@ namespace sci_cuda {
                 const float *base = source + 32 * h * P;
 #pragma unroll
                 for (int u = 0; u < 8; ++u) {
-                    axpy16(rows4[u].x, base + (4 * u + 0) * P, acc);
-                    axpy16(rows4[u].y, base + (4 * u + 1) * P, acc);
-                    axpy16(rows4[u].z, base + (4 * u + 2) * P, acc);
-                    axpy16(rows4[u].w, base + (4 * u + 3) * P, acc);
+                    axpy<C>(rows4[u].x, base + (4 * u + 0) * P, acc);
+                    axpy<C>(rows4[u].y, base + (4 * u + 1) * P, acc);
+                    axpy<C>(rows4[u].z, base + (4 * u + 2) * P, acc);
+                    axpy<C>(rows4[u].w, base + (4 * u + 3) * P, acc);
                 }
             };
             // the quarters' acc into `partial` (callers have synchronised past its last reads)
@@ -1580,10 +1668,10 @@ namespace sci_cuda {
                 const float *base = ((step & 1) ? staged1 : staged0) + 32 * h * P;
 #pragma unroll
                 for (int u = 0; u < 8; ++u) {
-                    axpy16(a[u].x, base + (4 * u + 0) * P, acc);
-                    axpy16(a[u].y, base + (4 * u + 1) * P, acc);
-                    axpy16(a[u].z, base + (4 * u + 2) * P, acc);
-                    axpy16(a[u].w, base + (4 * u + 3) * P, acc);
+                    axpy<C>(a[u].x, base + (4 * u + 0) * P, acc);
+                    axpy<C>(a[u].y, base + (4 * u + 1) * P, acc);
+                    axpy<C>(a[u].z, base + (4 * u + 2) * P, acc);
+                    axpy<C>(a[u].w, base + (4 * u + 3) * P, acc);
                 }
                 __syncthreads();  // before the buffer is refilled
             }
@@ -1667,12 +1755,14 @@ namespace sci_cuda {
         // x (n x width, the right-hand side on entry) := U^-1 L^-1 x by the two persistent sweeps, y
         // scratch; `done` stays false (and nothing is queued) when they do not apply: n not a multiple
         // of 4 (the tiles are read as 16-byte vectors), or more CTAs than can be resident at once.
+        // The right-hand sides go in column groups of 8 when that many chains fit on the GPU at once
+        // (each chain step is then half the work: 16 columns run as two chains side by side), else 16.
         int sweep_substitute(Context &ctx, const float *lu, const float *inv, unsigned long long n, float *x, float *y,
                              unsigned long long width, bool &done) {
             done = false;
             const unsigned long long blocks = (n + kSolveBlock - 1) / kSolveBlock;
-            const unsigned long long groups = (width + kSweepColumns - 1) / kSweepColumns;
             if (n % 4 != 0 || n > 0x7fffffffull || width > 0x7fffffffull) return SCI_CUDA_OK;
+            if (blocks >= 0xffff) return SCI_CUDA_OK;  // the progress marks count block rows in 16 bits
             static int cooperative = -1;
             if (cooperative < 0) {
                 int value = 0;
@@ -1680,10 +1770,24 @@ namespace sci_cuda {
                 cooperative = value;
             }
             if (!cooperative) return SCI_CUDA_OK;
-            const int resident = std::min(ctx.blocks_per_sm(reinterpret_cast<const void *>(&sweep<false>), kSweepThreads, 0),
-                                          ctx.blocks_per_sm(reinterpret_cast<const void *>(&sweep<true>), kSweepThreads, 0));
-            if (blocks * groups > static_cast<unsigned long long>(resident) * ctx.sms) return SCI_CUDA_OK;
-            if (blocks >= 0xffff) return SCI_CUDA_OK;  // the progress marks count block rows in 16 bits
+            auto capacity = [&](const void *lower, const void *upper) {
+                return static_cast<unsigned long long>(std::min(ctx.blocks_per_sm(lower, kSweepThreads, 0),
+                                                                ctx.blocks_per_sm(upper, kSweepThreads, 0))) *
+                       ctx.sms;
+            };
+            const void *kernels[2][2] = {
+                    {reinterpret_cast<const void *>(&sweep<false, 8>), reinterpret_cast<const void *>(&sweep<true, 8>)},
+                    {reinterpret_cast<const void *>(&sweep<false, 16>), reinterpret_cast<const void *>(&sweep<true, 16>)}};
+            int form = -1;
+            unsigned long long groups = 0;
+            for (int f = 0; f < 2 && form < 0; ++f) {
+                const unsigned long long columns = f == 0 ? 8 : 16, g = (width + columns - 1) / columns;
+                if (blocks * g <= capacity(kernels[f][0], kernels[f][1])) {
+                    form = f;
+                    groups = g;
+                }
+            }
+            if (form < 0) return SCI_CUDA_OK;
             if (int code = sweep_flags(ctx, groups)) return code;
             const float *couple = inv + 2ull * blocks * kSolveBlock * kSolveBlock;
             unsigned nn = static_cast<unsigned>(n), ww = static_cast<unsigned>(width), gg = static_cast<unsigned>(groups);
@@ -1693,8 +1797,7 @@ namespace sci_cuda {
                 const float *source = upper ? y : x;
                 float *target = upper ? x : y;
                 void *args[] = {&lu, &inv, &couple, &nn, &ww, &gg, &source, &target, &ctx.sweep_flags, &epoch, &ctx.status};
-                const void *kernel = upper ? reinterpret_cast<const void *>(&sweep<true>) : reinterpret_cast<const void *>(&sweep<false>);
-                if (int code = ctx.check(cudaLaunchCooperativeKernel(kernel, dim3(static_cast<unsigned>(blocks * groups)),
+                if (int code = ctx.check(cudaLaunchCooperativeKernel(kernels[form][pass], dim3(static_cast<unsigned>(blocks * groups)),
                                                                     dim3(kSweepThreads), args, 0, ctx.stream),
                                          "launching a substitution sweep"))
                     return code;
@@ -1956,9 +2059,13 @@ namespace {
     int backward_error(Context &ctx, const double *a, const double *b, const double *x, double *r, double *sums,
                        double *norms, unsigned long long n, unsigned long long width, double a_norm, const double *b_norm,
                        double &berr) {
-        residual_rows<<<dim3(static_cast<unsigned>((n + kResidualRows - 1) / kResidualRows),
-                             static_cast<unsigned>((width + kResidualColumns - 1) / kResidualColumns)),
-                        256, 0, ctx.stream>>>(a, x, b, r, n, width);
+        static const cudaError_t sized = cudaFuncSetAttribute(
+                reinterpret_cast<const void *>(&residual_tiles), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                static_cast<int>(kResidualShared));
+        if (int code = ctx.check(sized, "sizing the residual's shared memory")) return code;
+        residual_tiles<<<dim3(static_cast<unsigned>((n + kResidualRows - 1) / kResidualRows),
+                              static_cast<unsigned>((width + kResidualColumns - 1) / kResidualColumns)),
+                         kResidualThreads, kResidualShared, ctx.stream>>>(a, x, b, r, n, width);
         if (int code = ctx.check(cudaGetLastError(), "launching the residual")) return code;
         column_max<<<static_cast<unsigned>(width), 256, 0, ctx.stream>>>(r, n, width, norms);
         column_max<<<static_cast<unsigned>(width), 256, 0, ctx.stream>>>(x, n, width, norms + width);

@@ -114,3 +114,16 @@ def test_float_solve_without_refinement(device):
     x, _, _ = device.solve(device.array(a.ravel()), device.array(b.ravel()), n, 3)
     want = np.linalg.solve(a.astype(np.float64), b.astype(np.float64))
     assert np.abs(x.numpy().reshape(n, 3) - want).max() <= 1e-5 * np.abs(want).max()
+
+
+@pytest.mark.parametrize("width", [1, 8, 20, 64])
+def test_float_solve_column_groups(device, width):
+    """The substitution sweeps take the right-hand sides in column groups of 8 or 16 (a partial last
+    group zero-filled): every group's columns match FP64 at FP32 accuracy."""
+    n = 1024
+    rng = np.random.default_rng(width)
+    a = (rng.standard_normal((n, n)) + n * np.eye(n)).astype(np.float32)
+    b = rng.standard_normal((n, width)).astype(np.float32)
+    x, _, _ = device.solve(device.array(a.ravel()), device.array(b.ravel()), n, width)
+    want = np.linalg.solve(a.astype(np.float64), b.astype(np.float64))
+    assert np.abs(x.numpy().reshape(n, width) - want).max() <= 1e-5 * np.abs(want).max()
