@@ -626,9 +626,18 @@ namespace sci_cuda {
         // then all writes, so no exchange waits on another.
         template <typename T>
         __global__ void move_rows(T *a, unsigned long long n, const Movement *moved, unsigned long long c0,
-                                  unsigned long long c1, unsigned long long skip0, unsigned long long skip1) {
+                                  unsigned long long c1, unsigned long long skip0, unsigned long long skip1, unsigned *order) {
             chain_wait();
             chain_release();
+            if (order != nullptr && blockIdx.x == 0 && threadIdx.x < 32) {
+                // the same movement applied to the row order (order[i] = the original row at position
+                // i), one warp, two entries per lane: all reads, then all writes
+                const int count = static_cast<int>(moved->count), i0 = static_cast<int>(threadIdx.x), i1 = i0 + 32;
+                const unsigned v0 = i0 < count ? order[moved->src[i0]] : 0u, v1 = i1 < count ? order[moved->src[i1]] : 0u;
+                __syncwarp();
+                if (i0 < count) order[moved->rows[i0]] = v0;
+                if (i1 < count) order[moved->rows[i1]] = v1;
+            }
             const unsigned long long col = c0 + blockIdx.x * 256ull + threadIdx.x;
             if (col >= c1 || (col >= skip0 && col < skip1)) return;
             const int count = static_cast<int>(moved->count);
@@ -660,22 +669,10 @@ namespace sci_cuda {
             }
         }
 
-        // rows[] of the factorisation (the original row at each position) from the exchanges, in
-        // shared memory by one thread: the only sequential step of the permutation.
-        __global__ void order_rows(const long long *piv, unsigned *rows, unsigned long long n) {
-            extern __shared__ unsigned order[];
-            for (unsigned long long i = threadIdx.x; i < n; i += blockDim.x) order[i] = static_cast<unsigned>(i);
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                for (unsigned long long i = 0; i < n; ++i) {
-                    const unsigned long long p = static_cast<unsigned long long>(piv[i]);
-                    const unsigned x = order[i];
-                    order[i] = order[p];
-                    order[p] = x;
-                }
-            }
-            __syncthreads();
-            for (unsigned long long i = threadIdx.x; i < n; i += blockDim.x) rows[i] = order[i];
+        // order[i] = i: the row order before the first exchange.
+        __global__ void identity_rows(unsigned *order, unsigned long long n) {
+            for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < n; i += 256ull * gridDim.x)
+                order[i] = static_cast<unsigned>(i);
         }
 
         // x[i][:] = (U) b[rows[i]][:], optionally narrowing double to float: P b for the substitution.
@@ -913,21 +910,24 @@ namespace sci_cuda {
             }
         }
 
-        // The coupling blocks of the sweeps: couple[2 i] = inv(L_ii) L_i,i-1 (block rows i >= 1) and
-        // couple[2 i + 1] = inv(U_ii) U_i,i+1 (i <= blocks - 2), 128 x 128 each, rows and columns past
-        // the matrix zero. One CTA per block (blockIdx.y: 0 lower, 1 upper), 256 threads of 8 x 8
-        // outputs, k in slices of 16 staged in shared memory.
+        // The coupling blocks of the sweeps, 128 x 128 each, rows and columns past the matrix zero:
+        // couple[2 i] = inv(L_ii) L_i,i-1 (block rows i >= 1), couple[2 i + 1] = inv(U_ii) U_i,i+1
+        // (i <= blocks - 2), and two block rows apart couple[2 blocks + 2 i] = inv(L_ii) L_i,i-2,
+        // couple[2 blocks + 2 i + 1] = inv(U_ii) U_i,i+2. One CTA per block (blockIdx.y: bit 0 upper,
+        // bit 1 two rows apart), 256 threads of 8 x 8 outputs, k in slices of 16 staged in shared
+        // memory.
         __global__ void __launch_bounds__(256) couple_blocks(const float *lu, const float *inv, unsigned long long n,
                                                              float *couple) {
             constexpr int B = kSolveBlock, K = 16;
             __shared__ float left[B][K + 1];  // inv[:, k0 : k0 + 16]
             __shared__ float right[K][B];     // the tile's rows k0 .. k0 + 15
             const unsigned long long blocks = (n + B - 1) / B, i = blockIdx.x;
-            const bool upper = blockIdx.y == 1;
-            if (upper ? i + 1 >= blocks : i == 0) return;
-            const unsigned long long s = i * B, sj = upper ? s + B : s - B;
+            const bool upper = (blockIdx.y & 1) != 0;
+            const unsigned long long distance = 1 + (blockIdx.y >> 1);
+            if (upper ? i + distance >= blocks : i < distance) return;
+            const unsigned long long s = i * B, sj = upper ? s + distance * B : s - distance * B;
             const float *inverse = inv + (2 * i + (upper ? 1 : 0)) * B * B;
-            float *target = couple + (2 * i + (upper ? 1 : 0)) * B * B;
+            float *target = couple + ((distance - 1) * 2 * blocks + 2 * i + (upper ? 1 : 0)) * B * B;
             const int t = threadIdx.x, r0 = (t / 16) * 8, c0 = (t % 16) * 8;
             float acc[8][8] = {};
             for (int k0 = 0; k0 < B; k0 += K) {
@@ -1274,7 +1274,7 @@ namespace sci_cuda {
         // main stream waits for the side before it moves rows outside a block.
         template <typename T>
         int factor_device(Context &ctx, T *a, unsigned long long n, long long *piv, Movement *moved, bool tensor,
-                          bool split) {
+                          bool split, unsigned *order = nullptr) {
             constexpr int W = PanelWidth<T>::value;
             if (n > kPanelRows) return ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "factor: order %llu above %llu", n, kPanelRows);
             static const bool lookahead = [] {
@@ -1345,6 +1345,8 @@ namespace sci_cuda {
                 return simt_gemm<T>(ctx, a + t0 * n + J0, n, a + J0 * n + c0, n, a + t0 * n + c0, n, n - t0, c1 - c0, ob,
                                     true);
             };
+            // order (optional): the row order, kept up to date by each panel's row moves
+            if (order != nullptr) identity_rows<<<static_cast<unsigned>((n + 255) / 256), 256, 0, ctx.stream>>>(order, n);
             bool side_pending = false;
             for (unsigned long long J0 = 0; J0 < n; J0 += kOuter) {
                 const unsigned long long ob = std::min<unsigned long long>(kOuter, n - J0), block_end = J0 + ob;
@@ -1363,7 +1365,7 @@ namespace sci_cuda {
                     // the panel's row movement: now inside the block (everywhere without look-ahead)
                     const unsigned long long m0 = ahead ? J0 : 0, m1 = ahead ? block_end : n;
                     if (int code = ctx.check(launch_chained(move_rows<T>, dim3(static_cast<unsigned>((m1 - m0 + 255) / 256)),
-                                                            dim3(256), ctx.stream, a, n, mine, m0, m1, j0, j0 + w),
+                                                            dim3(256), ctx.stream, a, n, mine, m0, m1, j0, j0 + w, order),
                                              "launching the panel's row moves"))
                         return code;
                     // Inside the outer block only: U rows of the panel, then the rows below it. Columns
@@ -1416,9 +1418,9 @@ namespace sci_cuda {
         }
 
         // The inverses of the diagonal blocks (2 per block row) followed by the coupling blocks of the
-        // persistent sweeps (2 per block row, couple_blocks).
+        // persistent sweeps (4 per block row, couple_blocks).
         unsigned long long inverse_elements(unsigned long long n) {
-            return 4ull * ((n + kSolveBlock - 1) / kSolveBlock) * kSolveBlock * kSolveBlock;
+            return 6ull * ((n + kSolveBlock - 1) / kSolveBlock) * kSolveBlock * kSolveBlock;
         }
 
         template <typename T> int invert_diagonal(Context &ctx, const T *lu, unsigned long long n, T *inv) {
@@ -1426,7 +1428,7 @@ namespace sci_cuda {
             invert_blocks<T><<<blocks, kSolveBlock, 0, ctx.stream>>>(lu, n, inv);
             if constexpr (sizeof(T) == 4) {
                 if (blocks > 1)
-                    couple_blocks<<<dim3(blocks, 2), 256, 0, ctx.stream>>>(lu, inv, n, inv + 2ull * blocks * kSolveBlock * kSolveBlock);
+                    couple_blocks<<<dim3(blocks, 4), 256, 0, ctx.stream>>>(lu, inv, n, inv + 2ull * blocks * kSolveBlock * kSolveBlock);
             }
             return ctx.check(cudaGetLastError(), "inverting the diagonal blocks");
         }
@@ -1468,10 +1470,12 @@ namespace sci_cuda {
         // One cooperative launch solves a whole unit-lower (L) or upper (U) system in place of the
         // block-by-block launches. CTA (block row i, column group g) adds up the products of its
         // off-diagonal tiles with the other block rows' results in a fixed order, each as soon as
-        // that row has published, except the adjacent block row's; applies its
-        // diagonal block's inverse to (right-hand side - sum); and only then waits for the adjacent
-        // row, whose results enter through the coupling block inv(D_ii) D_i,adjacent. So the chain from
-        // one block row to the next is one wait, one 128 x 128 x 16 product and the write. Block rows
+        // that row has published, except the last two block rows' before it along the chain; applies
+        // its diagonal block's inverse to (right-hand side - sum); and only then takes those two rows,
+        // whose results enter through the coupling blocks inv(D_ii) D_i,j (the one two rows back as
+        // soon as it is published). So the chain from one block row to the next is one wait, one
+        // 128 x 128 x C product, one reduction and the write, and the inverse's product, which needs
+        // every earlier tile, runs while the row before is still being computed. Block rows
         // publish in chain order (written, fenced, then the group's progress mark released), so one
         // acquire of the mark shows every block row published so far.
         // Every CTA is resident (cooperative launch), and every wait is bounded: one that runs out
@@ -1484,15 +1488,16 @@ namespace sci_cuda {
             asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
             return v;
         }
-        // A polling read: relaxed, so it does not queue behind this thread's earlier loads; the caller
-        // follows the read that sees the release with fence_acquire (relaxed read + fence is an
-        // acquire pattern of the PTX memory model).
+        // A polling read: relaxed, so it does not queue behind this thread's earlier loads; the read
+        // that sees the release is followed by one acquire read of the same word (monotonic: it sees
+        // that mark or a later one, each written by a release), which orders what follows. That took
+        // 4.6-4.7 us per chain step at n = 8192 against 4.9-5.1 us with fence.acq_rel after the
+        // relaxed read instead.
         __device__ __forceinline__ unsigned load_relaxed(const unsigned *p) {
             unsigned v;
             asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
             return v;
         }
-        __device__ __forceinline__ void fence_acquire() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
         __device__ __forceinline__ void store_release(unsigned *p, unsigned v) {
             asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
         }
@@ -1541,7 +1546,7 @@ namespace sci_cuda {
             // below are broadcasts; quarter h covers the columns [32 h, 32 h + 32) of each tile
             const int t = threadIdx.x, h = t / B, r = t % B;
             const unsigned tiles = upper ? blocks - 1 - i : i;
-            const unsigned bulk = tiles > 0 ? tiles - 1 : 0;  // all tiles but the adjacent block row's
+            const unsigned bulk = tiles > 2 ? tiles - 2 : 0;  // all tiles but the last two block rows'
             if (t == 0) stop = false;
             // loaded before any wait: this block's inverse rows and its right-hand side
             float4 m[8];
@@ -1572,8 +1577,7 @@ namespace sci_cuda {
                     for (unsigned spin = 0; spin < kSweepWaitLimit; ++spin) {
                         const unsigned mark = load_relaxed(flags + g);
                         if (mark > base_mark + step) {  // marks of earlier sweeps are below base_mark
-                            fence_acquire();
-                            seen = mark - base_mark;
+                            seen = load_acquire(flags + g) - base_mark;  // the same mark or a later one
                             break;
                         }
                         __nanosleep(32);  // every waiting CTA polls the same word
@@ -1612,10 +1616,8 @@ namespace sci_cuda {
                 }
                 copies_commit();
             };
-            // acc (zeroed) := this quarter's part of rows4 times the block in `source`
-            auto multiply = [&](const float4 *rows4, const float *source) {
-#pragma unroll
-                for (int c = 0; c < C / 2; ++c) acc[c] = pair(0.0f);
+            // acc += this quarter's part of rows4 times the block in `source`
+            auto accumulate = [&](const float4 *rows4, const float *source) {
                 const float *base = source + 32 * h * P;
 #pragma unroll
                 for (int u = 0; u < 8; ++u) {
@@ -1624,6 +1626,12 @@ namespace sci_cuda {
                     axpy<C>(rows4[u].z, base + (4 * u + 2) * P, acc);
                     axpy<C>(rows4[u].w, base + (4 * u + 3) * P, acc);
                 }
+            };
+            // acc (zeroed) := the same
+            auto multiply = [&](const float4 *rows4, const float *source) {
+#pragma unroll
+                for (int c = 0; c < C / 2; ++c) acc[c] = pair(0.0f);
+                accumulate(rows4, source);
             };
             // the quarters' acc into `partial` (callers have synchronised past its last reads)
             auto publish = [&]() {
@@ -1675,11 +1683,13 @@ namespace sci_cuda {
                 }
                 __syncthreads();  // before the buffer is refilled
             }
-            // the coupling rows of the adjacent block row, in flight during what follows
+            // the coupling rows of the block row two places back along the chain, in flight during
+            // what follows
+            const float *const far = couple + 2ull * blocks * B * B;
             float4 mc[8];
 #pragma unroll
             for (int u = 0; u < 8; ++u)
-                mc[u] = tiles > 0 ? __ldg(reinterpret_cast<const float4 *>(couple + own) + u) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                mc[u] = tiles > 1 ? __ldg(reinterpret_cast<const float4 *>(far + own) + u) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             // pre = inverse (rhs - sum), kept in registers in the row-major mapping
             publish();
             __syncthreads();
@@ -1695,14 +1705,35 @@ namespace sci_cuda {
             float result[V];
 #pragma unroll
             for (int v = 0; v < V; ++v) result[v] = total(t + v * kSweepThreads);
-            // then the adjacent block row: result = pre - inv(D_ii) D_i,adjacent x_adjacent
-            if (tiles > 0) {
+            // then the last two block rows: result = pre - inv(D_ii) (D_i,far x_far + D_i,adjacent x_adjacent),
+            // the far one applied as soon as it is published, both summed before the one reduction.
+            // The adjacent row's coupling rows are loaded after the far row's wait, so that the wait's
+            // acquire does not wait for them, and they arrive while the far row is applied.
+            float4 mn[8];
+            auto adjacent_rows = [&]() {
+#pragma unroll
+                for (int u = 0; u < 8; ++u) mn[u] = __ldg(reinterpret_cast<const float4 *>(couple + own) + u);
+            };
+#pragma unroll
+            for (int c = 0; c < C / 2; ++c) acc[c] = pair(0.0f);
+            if (tiles > 1) {
                 __syncthreads();  // `partial` and staged0 are free again
+                if (!ready(tiles - 2)) return;
+                adjacent_rows();
+                fetch(tiles - 2, staged0);
+                copies_wait<0>();
+                __syncthreads();
+                accumulate(mc, staged0);
+            } else if (tiles > 0) {
+                adjacent_rows();
+            }
+            if (tiles > 0) {
+                __syncthreads();
                 if (!ready(tiles - 1)) return;
                 fetch(tiles - 1, staged0);
                 copies_wait<0>();
                 __syncthreads();
-                multiply(mc, staged0);
+                accumulate(mn, staged0);
                 publish();
                 __syncthreads();
 #pragma unroll
@@ -1953,11 +1984,6 @@ namespace sci_cuda {
             }
         }
 
-        // rows[] (device) from the exchanges of factor_device.
-        int row_order(Context &ctx, const long long *piv, unsigned *rows, unsigned long long n) {
-            order_rows<<<1, 1024, n * sizeof(unsigned), ctx.stream>>>(piv, rows, n);
-            return ctx.check(cudaGetLastError(), "ordering the rows");
-        }
 
         // x = (P b) in the element type D.
         template <typename S, typename D>
@@ -2036,11 +2062,10 @@ extern "C" int sci_cuda_decompose(sci_cuda_context *context, uint32_t precision,
                                   "copying the matrix"))
         return code;
     int code = precision == SCI_PRECISION_WIDE
-                       ? factor_device<double>(*context, static_cast<double *>(upper), order, piv, moved, false, false)
+                       ? factor_device<double>(*context, static_cast<double *>(upper), order, piv, moved, false, false, rows)
                        : factor_device<float>(*context, static_cast<float *>(upper), order, piv, moved,
-                                              mode != SCI_FACTOR_PLAIN, true);
+                                              mode != SCI_FACTOR_PLAIN, true, rows);
     if (code) return code;
-    if (int c = row_order(*context, piv, rows, order)) return c;
     const unsigned grid = static_cast<unsigned>(std::min<unsigned long long>((order * order + 255) / 256, 8ull * context->sms));
     if (precision == SCI_PRECISION_WIDE)
         split_factors<double><<<grid, 256, 0, context->stream>>>(static_cast<double *>(upper), static_cast<double *>(lower),
@@ -2158,8 +2183,7 @@ extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uin
         if (wide) {
             double *lu = carve.take<double>(n * n);
             cudaMemcpyAsync(lu, matrix, n * n * 8, cudaMemcpyDeviceToDevice, context->stream);
-            code = factor_device<double>(*context, lu, n, piv, moved, false, false);
-            if (!code) code = row_order(*context, piv, rows, n);
+            code = factor_device<double>(*context, lu, n, piv, moved, false, false, rows);
             if (!code) permute<double, double>(*context, static_cast<const double *>(right), static_cast<double *>(solution),
                                                rows, n, width);
             if (!code) code = substitute_device<double>(*context, lu, n, static_cast<double *>(solution), width);
@@ -2182,9 +2206,8 @@ extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uin
             float *inv = carve.take<float>(inverse_elements(n));
             float *y = carve.take<float>(nw);
             cudaMemcpyAsync(lu, matrix, n * n * 4, cudaMemcpyDeviceToDevice, context->stream);
-            code = factor_device<float>(*context, lu, n, piv, moved, true, true);
+            code = factor_device<float>(*context, lu, n, piv, moved, true, true, rows);
             if (!code) code = invert_diagonal<float>(*context, lu, n, inv);
-            if (!code) code = row_order(*context, piv, rows, n);
             if (!code) permute<float, float>(*context, static_cast<const float *>(right), static_cast<float *>(solution), rows,
                                              n, width);
             if (!code) code = substitute_inverse<float>(*context, lu, inv, n, static_cast<float *>(solution), y, width);
@@ -2207,9 +2230,8 @@ extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uin
     const int sms = context->sms;
 
     narrow<<<blocks_for(n * n, sms), 256, 0, context->stream>>>(a, lu, n * n);
-    if (int code = factor_device<float>(*context, lu, n, piv, moved, true, true)) return code;
+    if (int code = factor_device<float>(*context, lu, n, piv, moved, true, true, rows)) return code;
     if (int code = invert_diagonal<float>(*context, lu, n, inv)) return code;
-    if (int code = row_order(*context, piv, rows, n)) return code;
     auto correct = [&](const double *residual, double *xx) -> int {
         permute<double, float>(*context, residual, d, rows, n, width);
         if (int code = substitute_inverse<float>(*context, lu, inv, n, d, y, width)) return code;
@@ -2241,9 +2263,8 @@ namespace {
         T *z = carve.take<T>(nw);
         T *lambda = dB ? dB : carve.take<T>(nw);
         cudaMemcpyAsync(lu, a, n * n * sizeof(T), cudaMemcpyDeviceToDevice, ctx.stream);
-        if (int code = factor_device<T>(ctx, lu, n, piv, moved, sizeof(T) == 4, sizeof(T) == 4)) return code;
+        if (int code = factor_device<T>(ctx, lu, n, piv, moved, sizeof(T) == 4, sizeof(T) == 4, rows)) return code;
         if (int code = invert_diagonal<T>(ctx, lu, n, inv)) return code;
-        if (int code = row_order(ctx, piv, rows, n)) return code;
         permute<T, T>(ctx, b, x, rows, n, width);
         if constexpr (sizeof(T) == 8) {
             if (int code = substitute_device<T>(ctx, lu, n, x, width)) return code;
@@ -2324,9 +2345,8 @@ extern "C" int sci_cuda_solve_gradient(sci_cuda_context *context, uint32_t preci
     const int sms = context->sms;
 
     narrow<<<blocks_for(n * n, sms), 256, 0, context->stream>>>(a, lu, n * n);
-    if (int code = factor_device<float>(*context, lu, n, piv, moved, true, true)) return code;
+    if (int code = factor_device<float>(*context, lu, n, piv, moved, true, true, rows)) return code;
     if (int code = invert_diagonal<float>(*context, lu, n, inv)) return code;
-    if (int code = row_order(*context, piv, rows, n)) return code;
     auto forward = [&](const double *residual, double *xx) -> int {
         permute<double, float>(*context, residual, d, rows, n, width);
         if (int code = substitute_inverse<float>(*context, lu, inv, n, d, y, width)) return code;
