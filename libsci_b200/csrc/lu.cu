@@ -821,6 +821,99 @@ namespace sci_cuda {
                 if (i < w) a[(j0 + i) * n + col] = x[i];
         }
 
+        // Rows [J0, J0 + ob) of columns [c0, c1) := L11^-1 times themselves, L11 the block's unit lower
+        // triangle (ob <= kOuter): the U rows of a block over other columns. The same steps, rounded
+        // the same way, as a chain of trsm_rows (a panel's W rows in order) and rank_update (the rows
+        // below the panel minus the sum, in order, of the panel's products), in one launch: one CTA
+        // of 256 threads per strip of kStripColumns columns holds the strip's block rows in shared
+        // memory. Per panel: warp w solves columns [4 w, 4 w + 4) with eight lanes per column, lane
+        // l % 8 holding rows l % 8, + 8, ... of the panel (the owner of row k hands its value to the
+        // column's lanes, which subtract its product from their later rows); then each thread takes
+        // (row below, four columns) items with the row's W multipliers in registers.
+        constexpr int kStripColumns = 32, kStripRows = 256;
+        template <typename T> constexpr size_t strip_shared_bytes() {
+            return sizeof(T) * kStripRows * ((kStripColumns + 16 / sizeof(T)) + (PanelWidth<T>::value + 16 / sizeof(T)));
+        }
+        template <typename T> __device__ __forceinline__ void load4(const T *p, T *v) {
+            if constexpr (sizeof(T) == 4) {
+                load16(p, v);
+            } else {
+                load16(p, v);
+                load16(p + 2, v + 2);
+            }
+        }
+        template <typename T>
+        __global__ void __launch_bounds__(256) block_rows_strip(T *a, unsigned long long n, unsigned long long J0, int ob,
+                                                               unsigned long long c0, unsigned long long c1) {
+            constexpr int W = PanelWidth<T>::value, CS = kStripColumns, RW = kStripRows;
+            constexpr int XP = CS + 16 / sizeof(T), LP = W + 16 / sizeof(T);  // 16-byte aligned rows
+            constexpr int PER = W / 8;  // panel rows per lane in the solve
+            extern __shared__ __align__(16) unsigned char strip_shared[];
+            T *const x = reinterpret_cast<T *>(strip_shared);  // x[row * XP + column]: the strip's block rows
+            T *const l = x + RW * XP;                           // l[row * LP + q] = L[p0 + row][p0 + q]
+            chain_wait();
+            chain_release();
+            const int t = threadIdx.x, lane = t % 32, warp = t / 32;
+            const unsigned long long s0 = c0 + blockIdx.x * 1ull * CS;
+            // the strip's block rows; rows past ob are zero (a padded panel multiplies them by zero)
+            for (int i = t; i < RW * CS; i += 256) {
+                const int row = i / CS, col = i % CS;
+                x[row * XP + col] = (row < ob && s0 + col < c1) ? a[(J0 + row) * n + s0 + col] : T(0);
+            }
+            for (int p0 = 0; p0 < ob; p0 += W) {
+                const int w = min(W, ob - p0), rest = ob - p0;
+                __syncthreads();  // x in place; the previous panel's multipliers no longer read
+                for (int i = t; i < rest * W; i += 256) {
+                    const int row = i / W, q = i % W;
+                    l[row * LP + q] = q < w ? a[(J0 + p0 + row) * n + J0 + p0 + q] : T(0);
+                }
+                __syncthreads();
+                // the panel's rows: v[r] -= L[r][k] v[k] for k = 0, 1, ... (trsm_rows' order per row)
+                {
+                    const int col = 4 * warp + lane / 8, l8 = lane % 8;
+                    T v[PER];
+#pragma unroll
+                    for (int u = 0; u < PER; ++u) v[u] = x[(p0 + l8 + 8 * u) * XP + col];
+#pragma unroll
+                    for (int k = 0; k < W - 1; ++k) {
+                        const T vk = __shfl_sync(0xffffffffu, v[k / 8], (lane & ~7u) | (k % 8));
+#pragma unroll
+                        for (int u = 0; u < PER; ++u) {
+                            const int r = l8 + 8 * u;
+                            if (r > k) v[u] = sub(v[u], mul(l[r * LP + k], vk));
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < PER; ++u)
+                        if (l8 + 8 * u < w) x[(p0 + l8 + 8 * u) * XP + col] = v[u];
+                }
+                __syncthreads();
+                // the rows below: x[r] -= sum over q of L[r][q] x[p0 + q] (rank_update's order)
+                for (int i = t; i < (rest - w) * (CS / 4); i += 256) {
+                    const int row = w + i / (CS / 4), c4 = 4 * (i % (CS / 4));
+                    T m[W];
+#pragma unroll
+                    for (int q = 0; q < W; q += 16 / static_cast<int>(sizeof(T))) load16(l + row * LP + q, m + q);
+                    T acc[4] = {T(0), T(0), T(0), T(0)};
+#pragma unroll
+                    for (int q = 0; q < W; ++q) {
+                        T xv[4];
+                        load4(x + (p0 + q) * XP + c4, xv);
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) acc[e] = fma_(m[q], xv[e], acc[e]);
+                    }
+                    T *const target = x + (p0 + row) * XP + c4;
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) target[e] = sub(target[e], acc[e]);
+                }
+            }
+            __syncthreads();
+            for (int i = t; i < ob * CS; i += 256) {
+                const int row = i / CS, col = i % CS;
+                if (s0 + col < c1) a[(J0 + row) * n + s0 + col] = x[row * XP + col];
+            }
+        }
+
         // ---- substitution (solve.hpp:25-52), blocked ----------------------------------------------------
         // One diagonal block of `size` rows: lower (unit) or upper (divide by the diagonal) solve of
         // `width` right-hand-side columns in place. Warp w solves column (blockIdx.y * 32 + w); lane l
@@ -1303,28 +1396,17 @@ namespace sci_cuda {
             const int cluster = panel_cluster<T>();
             if (cluster == 0) return ctx.fail(SCI_CUDA_ERROR_LAUNCH, "the panel kernel's cluster cannot be scheduled");
             const unsigned move_blocks = static_cast<unsigned>((n + 255) / 256);
-            // U rows of the block (columns [c0, c1)) = L11^-1 A12, panel by panel
+            // U rows of the block (columns [c0, c1)) = L11^-1 A12: one launch, a CTA per strip of columns
+            static const cudaError_t strip_sized = cudaFuncSetAttribute(
+                    reinterpret_cast<const void *>(&block_rows_strip<T>), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                    static_cast<int>(strip_shared_bytes<T>()));
+            if (int code = ctx.check(strip_sized, "sizing the block rows' shared memory")) return code;
             auto block_rows = [&](unsigned long long J0, unsigned long long block_end, unsigned long long c0,
                                   unsigned long long c1) -> int {
                 if (c1 <= c0) return SCI_CUDA_OK;
-                // a chain of kernels, each following the one before directly on the stream: chained
-                // launches after the first (which follows an event wait or other work)
-                for (unsigned long long j0 = J0; j0 < block_end; j0 += W) {
-                    const int w = static_cast<int>(std::min<unsigned long long>(W, block_end - j0));
-                    const dim3 grid(static_cast<unsigned>((c1 - c0 + 127) / 128));
-                    if (j0 == J0) {
-                        trsm_rows<T><<<grid, 128, 0, ctx.stream>>>(a, n, j0, w, c0, c1);
-                    } else if (int code = ctx.check(launch_chained(trsm_rows<T>, grid, dim3(128), ctx.stream, a, n, j0, w, c0, c1),
-                                                    "launching the block's U rows")) {
-                        return code;
-                    }
-                    const unsigned long long below = j0 + w;
-                    if (below < block_end) {
-                        if (int code = update<T>(ctx, a + below * n + j0, n, a + j0 * n + c0, n, a + below * n + c0, n,
-                                                 block_end - below, c1 - c0, w, true))
-                            return code;
-                    }
-                }
+                const dim3 grid(static_cast<unsigned>((c1 - c0 + kStripColumns - 1) / kStripColumns));
+                block_rows_strip<T><<<grid, 256, strip_shared_bytes<T>(), ctx.stream>>>(a, n, J0, static_cast<int>(block_end - J0),
+                                                                                      c0, c1);
                 return ctx.check(cudaGetLastError(), "launching the block's U rows");
             };
             // trailing update of columns [c0, c1): A[t0:, c0:c1] -= L[t0:, J0:t0] U[J0:t0, c0:c1]
