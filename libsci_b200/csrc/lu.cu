@@ -8,17 +8,18 @@
 //
 //  for each outer block of 256 columns:
 //    for each narrow panel of W columns (W = 32 float, 16 double) inside it:
-//      1. panel_factor: one 8-CTA thread-block cluster, 1024 threads per CTA, one panel row per
-//         thread held in registers (so up to 8192 rows). Per column: a warp-shuffle argmax, a block
-//         argmax in shared memory, then one cluster barrier after which one warp per CTA reads the
-//         8 CTA candidates, the winner's row and the displaced row through distributed shared
-//         memory; then every thread eliminates its own row.
-//      2. move_rows: the panel's net row movement applied to every other column (one gather).
-//      3. trsm_rows + rank_update: U rows of the panel and the rows below it, inside the block.
-//    after the block: its U rows for the columns beyond it (trsm_rows + rank_update per panel, once
-//    the block's pivots are final), then the trailing update of everything right of and below it
-//    (GEMM, K = 256): on the tensor cores for float (three-term bf16 split, six products, about
-//    FP32 accuracy, FP32 accumulation), or plain FP32 / FP64 SIMT.
+//      1. panel_factor: one thread-block cluster (1 to 16 CTAs of 512 threads, by the rows left),
+//         one panel row per thread held in registers (so up to 8192 rows). Per column: a warp
+//         argmax, one CTA barrier, each CTA's candidate pushed into every CTA's inbox (st.async on
+//         an mbarrier), every warp picks the pivot from its inbox and eliminates its own rows.
+//      2. move_solve: the panel's net row movement applied to the block's other columns, and the
+//         panel's U rows over the block's columns right of it.
+//      3. rank_update: the rows below the panel, inside the block.
+//    after the block: its row movements applied to the other columns (move_rows_all), its U rows
+//    for the columns beyond it (block_rows_strip, once the block's pivots are final), then the
+//    trailing update of everything right of and below it (GEMM, K = 256): on the tensor cores for
+//    float (three-term bf16 split, six products, about FP32 accuracy, FP32 accumulation), or plain
+//    FP32 / FP64 SIMT.
 //
 // solve with refinement (SCI_REFINE_FP64): the matrix is factored in FP32, then
 //    x = 0, r = b;  repeat: solve LU d = P r in FP32; x += d;  r = b - A x in FP64
@@ -622,50 +623,32 @@ namespace sci_cuda {
             return chosen;
         }
 
-        // Applies a panel's net row movement to every column outside [skip0, skip1): all reads first,
-        // then all writes, so no exchange waits on another.
+        // The panels' net row movements for `count` movements in turn (a block's panels, in their
+        // order) over every column outside [skip0, skip1). One CTA of 256 threads per 32 columns: lane
+        // l takes column l of the CTA's 32 and warp g the movement's entries g, g + 8, ..., so a row's
+        // 32 columns are one coalesced 128-byte access; per movement all reads, a barrier, all
+        // writes, a barrier (each movement sees the one before it).
         template <typename T>
-        __global__ void move_rows(T *a, unsigned long long n, const Movement *moved, unsigned long long c0,
-                                  unsigned long long c1, unsigned long long skip0, unsigned long long skip1, unsigned *order) {
-            chain_wait();
-            chain_release();
-            if (order != nullptr && blockIdx.x == 0 && threadIdx.x < 32) {
-                // the same movement applied to the row order (order[i] = the original row at position
-                // i), one warp, two entries per lane: all reads, then all writes
-                const int count = static_cast<int>(moved->count), i0 = static_cast<int>(threadIdx.x), i1 = i0 + 32;
-                const unsigned v0 = i0 < count ? order[moved->src[i0]] : 0u, v1 = i1 < count ? order[moved->src[i1]] : 0u;
-                __syncwarp();
-                if (i0 < count) order[moved->rows[i0]] = v0;
-                if (i1 < count) order[moved->rows[i1]] = v1;
-            }
-            const unsigned long long col = c0 + blockIdx.x * 256ull + threadIdx.x;
-            if (col >= c1 || (col >= skip0 && col < skip1)) return;
-            const int count = static_cast<int>(moved->count);
-            T values[64];
-#pragma unroll
-            for (int i = 0; i < 64; ++i)
-                if (i < count) values[i] = a[static_cast<unsigned long long>(moved->src[i]) * n + col];
-#pragma unroll
-            for (int i = 0; i < 64; ++i)
-                if (i < count) a[static_cast<unsigned long long>(moved->rows[i]) * n + col] = values[i];
-        }
-
-        // move_rows for `count` movements in turn (a block's panels, in their order), one column per
-        // thread: the movements of one column follow each other in program order.
-        template <typename T>
-        __global__ void move_rows_all(T *a, unsigned long long n, const Movement *moved, int count,
-                                      unsigned long long skip0, unsigned long long skip1) {
-            const unsigned long long col = blockIdx.x * 256ull + threadIdx.x;
-            if (col >= n || (col >= skip0 && col < skip1)) return;
+        __global__ void __launch_bounds__(256) move_rows_all(T *a, unsigned long long n, const Movement *moved, int count,
+                                                            unsigned long long skip0, unsigned long long skip1) {
+            const int lane = static_cast<int>(threadIdx.x % 32), g = static_cast<int>(threadIdx.x / 32);
+            const unsigned long long col = blockIdx.x * 32ull + lane;
+            const bool active = col < n && !(col >= skip0 && col < skip1);
             for (int p = 0; p < count; ++p) {
                 const int rows = static_cast<int>(moved[p].count);
-                T values[64];
+                T values[8];
 #pragma unroll
-                for (int i = 0; i < 64; ++i)
-                    if (i < rows) values[i] = a[static_cast<unsigned long long>(moved[p].src[i]) * n + col];
+                for (int u = 0; u < 8; ++u) {
+                    const int e = g + 8 * u;
+                    if (active && e < rows) values[u] = a[static_cast<unsigned long long>(moved[p].src[e]) * n + col];
+                }
+                __syncthreads();
 #pragma unroll
-                for (int i = 0; i < 64; ++i)
-                    if (i < rows) a[static_cast<unsigned long long>(moved[p].rows[i]) * n + col] = values[i];
+                for (int u = 0; u < 8; ++u) {
+                    const int e = g + 8 * u;
+                    if (active && e < rows) a[static_cast<unsigned long long>(moved[p].rows[e]) * n + col] = values[u];
+                }
+                __syncthreads();
             }
         }
 
@@ -722,6 +705,17 @@ namespace sci_cuda {
                 }
             };
             fetch(0);
+            // the thread's outputs as they are, loaded with the first slice (one wait for both)
+            T old[4][TN];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const unsigned long long row = m0 + ty * 4 + i;
+#pragma unroll
+                for (int j = 0; j < TN; ++j) {
+                    const unsigned long long col = n0 + tx * TN + j;
+                    old[i][j] = (row < m && col < n) ? c[row * ldc + col] : T(0);
+                }
+            }
             for (unsigned long long k0 = 0; k0 < k; k0 += BK) {
 #pragma unroll
                 for (int u = 0; u < LA; ++u) {
@@ -756,7 +750,7 @@ namespace sci_cuda {
 #pragma unroll
                 for (int j = 0; j < TN; ++j) {
                     const unsigned long long col = n0 + tx * TN + j;
-                    if (col < n) c[row * ldc + col] = sub(c[row * ldc + col], acc[i][j]);
+                    if (col < n) c[row * ldc + col] = sub(old[i][j], acc[i][j]);
                 }
             }
         }
@@ -784,53 +778,17 @@ namespace sci_cuda {
             return ctx.check(cudaGetLastError(), "launching a rank update");
         }
 
-        // Rows [j0, j0 + w) of columns [c0, c1) := L^-1 times themselves, L the unit lower triangle
-        // of the panel's top w x w block. One thread per column, the column's w values in registers.
-        template <typename T>
-        __global__ void __launch_bounds__(128) trsm_rows(T *a, unsigned long long n, unsigned long long j0, int w, unsigned long long c0,
-                                  unsigned long long c1) {
-            constexpr int W = PanelWidth<T>::value;
-            constexpr int threads = 128, L = W * W / threads;
-            __shared__ T lower[W][W];
-            chain_wait();
-            chain_release();
-            const unsigned long long col = c0 + blockIdx.x * 1ull * threads + threadIdx.x;
-            // every global load of the thread is issued before the first shared store
-            T staged[L], x[W];
-#pragma unroll
-            for (int u = 0; u < L; ++u) {
-                const int i = threadIdx.x + u * threads, row = i / W, k = i % W;
-                staged[u] = (row < w && k < w) ? a[(j0 + row) * n + j0 + k] : T(0);
-            }
-#pragma unroll
-            for (int i = 0; i < W; ++i) x[i] = (col < c1 && i < w) ? a[(j0 + i) * n + col] : T(0);
-#pragma unroll
-            for (int u = 0; u < L; ++u) {
-                const int i = threadIdx.x + u * threads;
-                lower[i / W][i % W] = staged[u];
-            }
-            __syncthreads();
-            if (col >= c1) return;
-#pragma unroll
-            for (int i = 1; i < W; ++i) {
-#pragma unroll
-                for (int k = 0; k < i; ++k) x[i] = sub(x[i], mul(lower[i][k], x[k]));
-            }
-#pragma unroll
-            for (int i = 0; i < W; ++i)
-                if (i < w) a[(j0 + i) * n + col] = x[i];
-        }
-
         // Rows [J0, J0 + ob) of columns [c0, c1) := L11^-1 times themselves, L11 the block's unit lower
         // triangle (ob <= kOuter): the U rows of a block over other columns. The same steps, rounded
-        // the same way, as a chain of trsm_rows (a panel's W rows in order) and rank_update (the rows
-        // below the panel minus the sum, in order, of the panel's products), in one launch: one CTA
-        // of 256 threads per strip of kStripColumns columns holds the strip's block rows in shared
-        // memory. Per panel: warp w solves columns [4 w, 4 w + 4) with eight lanes per column, lane
-        // l % 8 holding rows l % 8, + 8, ... of the panel (the owner of row k hands its value to the
-        // column's lanes, which subtract its product from their later rows); then each thread takes
-        // (row below, four columns) items with the row's W multipliers in registers.
-        constexpr int kStripColumns = 32, kStripRows = 256;
+        // the same way, as a chain of move_solve's solve (a panel's W rows in order) and rank_update
+        // (the rows below the panel minus the sum, in order, of the panel's products), in one launch:
+        // one CTA of 256 threads per strip of kStripColumns columns (16: more CTAs, a shorter update
+        // per panel) holds the strip's block rows in shared memory. Per panel: warp w < 4 solves
+        // columns [4 w, 4 w + 4) with eight lanes per column, lane l % 8 holding rows l % 8, + 8, ...
+        // of the panel (the owner of row k hands its value to the column's lanes, which subtract its
+        // product from their later rows); then each thread takes (row below, four columns) items with
+        // the row's W multipliers in registers.
+        constexpr int kStripColumns = 16, kStripRows = 256;
         template <typename T> constexpr size_t strip_shared_bytes() {
             return sizeof(T) * kStripRows * ((kStripColumns + 16 / sizeof(T)) + (PanelWidth<T>::value + 16 / sizeof(T)));
         }
@@ -855,21 +813,45 @@ namespace sci_cuda {
             chain_release();
             const int t = threadIdx.x, lane = t % 32, warp = t / 32;
             const unsigned long long s0 = c0 + blockIdx.x * 1ull * CS;
-            // the strip's block rows; rows past ob are zero (a padded panel multiplies them by zero)
-            for (int i = t; i < RW * CS; i += 256) {
-                const int row = i / CS, col = i % CS;
-                x[row * XP + col] = (row < ob && s0 + col < c1) ? a[(J0 + row) * n + s0 + col] : T(0);
+            // the strip's block rows; rows past ob are zero (a padded panel multiplies them by zero).
+            // Every global load of a thread is issued before its first shared store.
+            {
+                T staged[RW * CS / 256];
+#pragma unroll
+                for (int u = 0; u < RW * CS / 256; ++u) {
+                    const int i = t + u * 256, row = i / CS, col = i % CS;
+                    staged[u] = (row < ob && s0 + col < c1) ? a[(J0 + row) * n + s0 + col] : T(0);
+                }
+#pragma unroll
+                for (int u = 0; u < RW * CS / 256; ++u) {
+                    const int i = t + u * 256;
+                    x[(i / CS) * XP + i % CS] = staged[u];
+                }
             }
+            // a panel's multipliers L[p0 + row][p0 + q] (rows below ob and columns past the panel
+            // zero), loaded into registers one panel ahead so their latency overlaps the panel before
+            T staged[RW * W / 256];
+            auto load_panel = [&](int p0) {
+                const int w = min(W, ob - p0), rest = ob - p0;
+#pragma unroll
+                for (int u = 0; u < RW * W / 256; ++u) {
+                    const int i = t + u * 256, row = i / W, q = i % W;
+                    staged[u] = (row < rest && q < w) ? a[(J0 + p0 + row) * n + J0 + p0 + q] : T(0);
+                }
+            };
+            load_panel(0);
             for (int p0 = 0; p0 < ob; p0 += W) {
                 const int w = min(W, ob - p0), rest = ob - p0;
                 __syncthreads();  // x in place; the previous panel's multipliers no longer read
-                for (int i = t; i < rest * W; i += 256) {
-                    const int row = i / W, q = i % W;
-                    l[row * LP + q] = q < w ? a[(J0 + p0 + row) * n + J0 + p0 + q] : T(0);
+#pragma unroll
+                for (int u = 0; u < RW * W / 256; ++u) {
+                    const int i = t + u * 256;
+                    l[(i / W) * LP + i % W] = staged[u];
                 }
                 __syncthreads();
-                // the panel's rows: v[r] -= L[r][k] v[k] for k = 0, 1, ... (trsm_rows' order per row)
-                {
+                if (p0 + W < ob) load_panel(p0 + W);
+                // the panel's rows: v[r] -= L[r][k] v[k] for k = 0, 1, ... (move_solve's order per row)
+                if (warp < CS / 4) {
                     const int col = 4 * warp + lane / 8, l8 = lane % 8;
                     T v[PER];
 #pragma unroll
@@ -912,6 +894,68 @@ namespace sci_cuda {
                 const int row = i / CS, col = i % CS;
                 if (s0 + col < c1) a[(J0 + row) * n + s0 + col] = x[row * XP + col];
             }
+        }
+
+        // A panel's row movement over columns [c0, c1) but its own [j0, j0 + w), and, for the block's
+        // columns right of the panel ([right, block_end)), the panel's U rows := L^-1 times themselves
+        // (L the unit lower triangle of the panel's top w x w block), in one launch. One thread per
+        // column does the column's moves and then its solve (row i minus L[i][k] times row k for
+        // k = 0, 1, ..., i - 1, each product and difference rounded, as the reference's column steps
+        // subtract them); no other thread touches the column. Block 0's first warp also moves the row order.
+        template <typename T>
+        __global__ void __launch_bounds__(128) move_solve(T *a, unsigned long long n, const Movement *moved, unsigned long long c0,
+                                                         unsigned long long c1, unsigned long long j0, int w,
+                                                         unsigned long long right, unsigned long long block_end,
+                                                         unsigned *order) {
+            constexpr int W = PanelWidth<T>::value;
+            constexpr int threads = 128, L = W * W / threads;
+            __shared__ T lower[W][W];
+            chain_wait();
+            chain_release();
+            if (order != nullptr && blockIdx.x == 0 && threadIdx.x < 32) {
+                const int count = static_cast<int>(moved->count), i0 = static_cast<int>(threadIdx.x), i1 = i0 + 32;
+                const unsigned v0 = i0 < count ? order[moved->src[i0]] : 0u, v1 = i1 < count ? order[moved->src[i1]] : 0u;
+                __syncwarp();
+                if (i0 < count) order[moved->rows[i0]] = v0;
+                if (i1 < count) order[moved->rows[i1]] = v1;
+            }
+            // the panel's top triangle (its own columns, which this kernel does not move)
+            T staged[L];
+#pragma unroll
+            for (int u = 0; u < L; ++u) {
+                const int i = threadIdx.x + u * threads, row = i / W, k = i % W;
+                staged[u] = (row < w && k < w) ? a[(j0 + row) * n + j0 + k] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < L; ++u) {
+                const int i = threadIdx.x + u * threads;
+                lower[i / W][i % W] = staged[u];
+            }
+            __syncthreads();
+            const unsigned long long col = c0 + blockIdx.x * 1ull * threads + threadIdx.x;
+            if (col >= c1 || (col >= j0 && col < j0 + w)) return;
+            {
+                const int count = static_cast<int>(moved->count);
+                T values[64];
+#pragma unroll
+                for (int i = 0; i < 64; ++i)
+                    if (i < count) values[i] = a[static_cast<unsigned long long>(moved->src[i]) * n + col];
+#pragma unroll
+                for (int i = 0; i < 64; ++i)
+                    if (i < count) a[static_cast<unsigned long long>(moved->rows[i]) * n + col] = values[i];
+            }
+            if (col < right || col >= block_end) return;
+            T x[W];
+#pragma unroll
+            for (int i = 0; i < W; ++i) x[i] = i < w ? a[(j0 + i) * n + col] : T(0);
+#pragma unroll
+            for (int i = 1; i < W; ++i) {
+#pragma unroll
+                for (int k = 0; k < i; ++k) x[i] = sub(x[i], mul(lower[i][k], x[k]));
+            }
+#pragma unroll
+            for (int i = 0; i < W; ++i)
+                if (i < w) a[(j0 + i) * n + col] = x[i];
         }
 
         // ---- substitution (solve.hpp:25-52), blocked ----------------------------------------------------
@@ -1395,7 +1439,7 @@ namespace sci_cuda {
             }
             const int cluster = panel_cluster<T>();
             if (cluster == 0) return ctx.fail(SCI_CUDA_ERROR_LAUNCH, "the panel kernel's cluster cannot be scheduled");
-            const unsigned move_blocks = static_cast<unsigned>((n + 255) / 256);
+            const unsigned move_blocks = static_cast<unsigned>((n + 31) / 32);  // move_rows_all: 32 columns per CTA
             // U rows of the block (columns [c0, c1)) = L11^-1 A12: one launch, a CTA per strip of columns
             static const cudaError_t strip_sized = cudaFuncSetAttribute(
                     reinterpret_cast<const void *>(&block_rows_strip<T>), cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1445,21 +1489,17 @@ namespace sci_cuda {
                             launch_panel_for<T>(cluster, ctx.stream, a, n, j0, w, piv, mine, ctx.status, chained);
                     if (int code = ctx.check(launched, "launching the panel factorisation")) return code;
                     // the panel's row movement: now inside the block (everywhere without look-ahead)
+                    // Inside the outer block only: U rows of the panel (with the moves, one launch),
+                    // then the rows below it. Columns beyond the block wait until the block's pivots
+                    // are all known (a later pivot of this block may still bring a row up from below).
                     const unsigned long long m0 = ahead ? J0 : 0, m1 = ahead ? block_end : n;
-                    if (int code = ctx.check(launch_chained(move_rows<T>, dim3(static_cast<unsigned>((m1 - m0 + 255) / 256)),
-                                                            dim3(256), ctx.stream, a, n, mine, m0, m1, j0, j0 + w, order),
-                                             "launching the panel's row moves"))
-                        return code;
-                    // Inside the outer block only: U rows of the panel, then the rows below it. Columns
-                    // beyond the block wait until the block's pivots are all known (a later pivot of
-                    // this block may still bring a row up from below).
                     const unsigned long long right = j0 + w;
+                    if (int code = ctx.check(launch_chained(move_solve<T>, dim3(static_cast<unsigned>((m1 - m0 + 127) / 128)),
+                                                            dim3(128), ctx.stream, a, n, mine, m0, m1, j0, w, right, block_end,
+                                                            order),
+                                             "launching the panel's row moves and U rows"))
+                        return code;
                     if (right < block_end) {
-                        if (int code = ctx.check(launch_chained(trsm_rows<T>,
-                                                                dim3(static_cast<unsigned>((block_end - right + 127) / 128)),
-                                                                dim3(128), ctx.stream, a, n, j0, w, right, block_end),
-                                                 "launching the panel's U rows"))
-                            return code;
                         if (int code = update<T>(ctx, a + right * n + j0, n, a + j0 * n + right, n, a + right * n + right, n,
                                                  n - right, block_end - right, w, true))
                             return code;
