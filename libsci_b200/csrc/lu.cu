@@ -1018,32 +1018,53 @@ namespace sci_cuda {
         // Inverses of the diagonal blocks of L (unit lower) and U, kSolveBlock x kSolveBlock each, zero
         // padded past the matrix: inv[2 b] is L's block b, inv[2 b + 1] U's. Thread c computes column c
         // of both by substitution against the identity (solve.hpp:25-52 applied to e_c), reading back
-        // only the entries it wrote itself.
+        // only the entries it wrote itself. The diagonal block is staged in shared memory first (all
+        // threads read its entries as broadcasts); for float the column being built stays there too
+        // (for double it is built in place in `inv`, which the 128 KB of the staged block leaves no
+        // room for).
+        constexpr int kInvertPitch = kSolveBlock + 1;
+        template <typename T> constexpr size_t invert_shared_bytes() {
+            return sizeof(T) * kSolveBlock * kInvertPitch * (sizeof(T) == 4 ? 2 : 1);
+        }
         template <typename T>
         __global__ void __launch_bounds__(kSolveBlock) invert_blocks(const T *lu, unsigned long long n, T *inv) {
-            constexpr int B = kSolveBlock;
+            constexpr int B = kSolveBlock, PD = kInvertPitch;
+            constexpr bool staged = sizeof(T) == 4;
+            extern __shared__ __align__(16) unsigned char invert_shared[];
+            T *const ds = reinterpret_cast<T *>(invert_shared);  // ds[i * PD + k] = d[i][k]
+            T *const work = staged ? ds + B * PD : nullptr;       // work[k * PD + c]: the column being built
             const unsigned long long s = blockIdx.x * 1ull * B;
             const int size = static_cast<int>(n - s < B ? n - s : B);
             const int c = threadIdx.x;
             T *lower = inv + 2ull * blockIdx.x * B * B;
             T *upper = lower + 1ull * B * B;
             const T *d = lu + s * n + s;
+#pragma unroll 16
+            for (int i = 0; i < B; ++i) ds[i * PD + c] = (i < size && c < size) ? d[i * n + c] : T(0);
+            __syncthreads();
+            auto at = [&](T *global, int k) -> T & { return staged ? work[k * PD + c] : global[k * B + c]; };
             for (int i = 0; i < B; ++i) {
                 T value = T(0);
                 if (c < size && i < size && i >= c) {
                     value = i == c ? T(1) : T(0);
-                    for (int k = c; k < i; ++k) value = fma_(-d[i * n + k], lower[k * B + c], value);
+                    for (int k = c; k < i; ++k) value = fma_(-ds[i * PD + k], at(lower, k), value);
                 }
-                lower[i * B + c] = value;
+                at(lower, i) = value;
+            }
+            if constexpr (staged) {
+                for (int i = 0; i < B; ++i) lower[i * B + c] = work[i * PD + c];
             }
             for (int i = B - 1; i >= 0; --i) {
                 T value = T(0);
                 if (c < size && i < size && i <= c) {
                     value = i == c ? T(1) : T(0);
-                    for (int k = i + 1; k <= c; ++k) value = fma_(-d[i * n + k], upper[k * B + c], value);
-                    value = div(value, d[i * n + i]);
+                    for (int k = i + 1; k <= c; ++k) value = fma_(-ds[i * PD + k], at(upper, k), value);
+                    value = div(value, ds[i * PD + i]);
                 }
-                upper[i * B + c] = value;
+                at(upper, i) = value;
+            }
+            if constexpr (staged) {
+                for (int i = 0; i < B; ++i) upper[i * B + c] = work[i * PD + c];
             }
         }
 
@@ -1194,6 +1215,12 @@ namespace sci_cuda {
                 if (c4 + j < w) c[gr * ldc + c4 + j] = sub(c[gr * ldc + c4 + j], acc[j]);
         }
 
+        // *target = max(*target, v) for v >= 0 or a NaN with the sign bit clear: such doubles order
+        // like their bit patterns (a NaN above +inf, so it propagates).
+        __device__ __forceinline__ void max_nonnegative(double *target, double v) {
+            atomicMax(reinterpret_cast<unsigned long long *>(target), static_cast<unsigned long long>(__double_as_longlong(v)));
+        }
+
         // r = b - A x in FP64, the refinement's residual. One CTA of 512 threads per 64 rows
         // (blockIdx.x) and 16 columns of x (blockIdx.y); A and x stream through shared memory in
         // slices of 64 columns (cp.async, four slices in flight: 160 KB), so A is read once, from HBM,
@@ -1221,7 +1248,7 @@ namespace sci_cuda {
 
         __global__ void __launch_bounds__(kResidualThreads, 1)
                 residual_tiles(const double *__restrict__ a, const double *__restrict__ x, const double *__restrict__ b,
-                               double *__restrict__ r, unsigned long long n, unsigned long long width) {
+                               double *__restrict__ r, unsigned long long n, unsigned long long width, double *r_max) {
             constexpr int RW = kResidualRows, K = kResidualSlice, C = kResidualColumns, S = kResidualStages;
             constexpr int CH = K / 2;  // 16-byte chunks per slice row
             extern __shared__ __align__(16) double residual_shared[];
@@ -1315,6 +1342,7 @@ namespace sci_cuda {
 #pragma unroll
                 for (int j = 0; j < 8; ++j) partial[(warp * RW + g + 16 * p) * C + 8 * h + j] = acc[p][j];
             __syncthreads();
+            double largest = 0.0;  // this thread's largest |r|: its outputs share column t % C
 #pragma unroll
             for (int u = 0; u < RW * C / kResidualThreads; ++u) {
                 const int q = t + u * kResidualThreads, row = q / C, c = q % C;
@@ -1322,7 +1350,24 @@ namespace sci_cuda {
 #pragma unroll
                 for (int w = 0; w < kResidualThreads / 32; ++w) sum += partial[w * RW * C + q];
                 const unsigned long long gr = r0 + row, gc = c0 + c;
-                if (gr < n && gc < width) r[gr * width + gc] = b[gr * width + gc] - sum;
+                if (gr < n && gc < width) {
+                    const double value = b[gr * width + gc] - sum;
+                    r[gr * width + gc] = value;
+                    const double m = fabs(value);
+                    largest = (m > largest || m != m) ? m : largest;
+                }
+            }
+            // each column's largest |r| over the CTA, max-ed into r_max[column] (zeroed before)
+            const double other = __shfl_xor_sync(0xffffffffu, largest, 16);  // lane ^ 16: the same column
+            largest = (other > largest || other != other) ? other : largest;
+            __syncthreads();  // the partial sums are read
+            double *const fold = residual_shared;  // fold[warp][column]
+            if (lane < C) fold[warp * C + lane] = largest;
+            __syncthreads();
+            if (t < C && c0 + t < width) {
+                double m = 0.0;
+                for (int w = 0; w < kResidualThreads / 32; ++w) m = (fold[w * C + t] > m || fold[w * C + t] != fold[w * C + t]) ? fold[w * C + t] : m;
+                max_nonnegative(&r_max[c0 + t], m);
             }
         }
 
@@ -1334,6 +1379,50 @@ namespace sci_cuda {
         __global__ void widen_add(const float *d, double *x, unsigned long long count) {
             for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < count; i += 256ull * gridDim.x)
                 x[i] += static_cast<double>(d[i]);
+        }
+        // The refinement's update x += d (n x width, width <= 256 and a divisor of 256 * gridDim.x's
+        // stride, so each thread stays in one column) and each column's largest |x|, max-ed into
+        // x_max[column] (zeroed before).
+        __global__ void __launch_bounds__(256) widen_add_max(const float *d, double *x, unsigned long long count,
+                                                            unsigned width, double *x_max) {
+            __shared__ double best[256];
+            double mine = 0.0;
+            const unsigned long long stride = 256ull * gridDim.x;
+            for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < count; i += stride) {
+                const double v = x[i] + static_cast<double>(d[i]);
+                x[i] = v;
+                const double m = fabs(v);
+                mine = (m > mine || m != m) ? m : mine;
+            }
+            best[threadIdx.x] = mine;
+            __syncthreads();
+            // thread t's elements all lie in column (blockIdx.x * 256 + t) % width: fold the threads
+            // of one column, then one atomic per column and CTA
+            if (threadIdx.x < width) {
+                const unsigned c = static_cast<unsigned>((blockIdx.x * 256ull + threadIdx.x) % width);
+                double m = 0.0;
+                for (unsigned t = threadIdx.x; t < 256; t += width) m = (best[t] > m || best[t] != best[t]) ? best[t] : m;
+                max_nonnegative(&x_max[c], m);
+            }
+        }
+        // out = (float) a for the n x n matrix, and |a|_inf (the largest row sum of |a|) max-ed into
+        // *a_norm (zeroed before): one warp per row, the row read once for both.
+        __global__ void __launch_bounds__(256) narrow_sums(const double *a, float *out, unsigned long long n, double *a_norm) {
+            const unsigned long long row = blockIdx.x * 8ull + threadIdx.x / 32;
+            if (row >= n) return;
+            const unsigned lane = threadIdx.x % 32;
+            const double *src = a + row * n;
+            float *dst = out + row * n;
+            double s = 0.0;
+#pragma unroll 4
+            for (unsigned long long k = lane; k < n; k += 32) {
+                const double v = src[k];
+                dst[k] = static_cast<float>(v);
+                s += fabs(v);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (lane == 0) max_nonnegative(a_norm, s);
         }
         // |rows of a|_1, the infinity norm's terms: one warp per row.
         template <typename T> __global__ void row_sums(const T *a, unsigned long long n, double *out) {
@@ -1547,7 +1636,11 @@ namespace sci_cuda {
 
         template <typename T> int invert_diagonal(Context &ctx, const T *lu, unsigned long long n, T *inv) {
             const unsigned blocks = static_cast<unsigned>((n + kSolveBlock - 1) / kSolveBlock);
-            invert_blocks<T><<<blocks, kSolveBlock, 0, ctx.stream>>>(lu, n, inv);
+            static const cudaError_t sized = cudaFuncSetAttribute(reinterpret_cast<const void *>(&invert_blocks<T>),
+                                                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                                  static_cast<int>(invert_shared_bytes<T>()));
+            if (int code = ctx.check(sized, "sizing the inversion's shared memory")) return code;
+            invert_blocks<T><<<blocks, kSolveBlock, invert_shared_bytes<T>(), ctx.stream>>>(lu, n, inv);
             if constexpr (sizeof(T) == 4) {
                 if (blocks > 1)
                     couple_blocks<<<dim3(blocks, 4), 256, 0, ctx.stream>>>(lu, inv, n, inv + 2ull * blocks * kSolveBlock * kSolveBlock);
@@ -2202,20 +2295,21 @@ extern "C" int sci_cuda_decompose(sci_cuda_context *context, uint32_t precision,
 namespace {
 
     // The normwise backward error max_j |b_j - A x_j|_inf / (|A|_inf |x_j|_inf + |b_j|_inf), in FP64.
-    // r is scratch (n x width), sums (n), norms (2 width); waits for the stream.
+    // r is scratch (n x width), sums (n), norms (2 width: |r_j|_inf, then |x_j|_inf); waits for the
+    // stream. x_ready: norms[width + j] already holds |x_j|_inf (the update computed it).
     int backward_error(Context &ctx, const double *a, const double *b, const double *x, double *r, double *sums,
                        double *norms, unsigned long long n, unsigned long long width, double a_norm, const double *b_norm,
-                       double &berr) {
+                       double &berr, bool x_ready = false) {
         static const cudaError_t sized = cudaFuncSetAttribute(
                 reinterpret_cast<const void *>(&residual_tiles), cudaFuncAttributeMaxDynamicSharedMemorySize,
                 static_cast<int>(kResidualShared));
         if (int code = ctx.check(sized, "sizing the residual's shared memory")) return code;
+        cudaMemsetAsync(norms, 0, width * 8, ctx.stream);
         residual_tiles<<<dim3(static_cast<unsigned>((n + kResidualRows - 1) / kResidualRows),
                               static_cast<unsigned>((width + kResidualColumns - 1) / kResidualColumns)),
-                         kResidualThreads, kResidualShared, ctx.stream>>>(a, x, b, r, n, width);
+                         kResidualThreads, kResidualShared, ctx.stream>>>(a, x, b, r, n, width, norms);
         if (int code = ctx.check(cudaGetLastError(), "launching the residual")) return code;
-        column_max<<<static_cast<unsigned>(width), 256, 0, ctx.stream>>>(r, n, width, norms);
-        column_max<<<static_cast<unsigned>(width), 256, 0, ctx.stream>>>(x, n, width, norms + width);
+        if (!x_ready) column_max<<<static_cast<unsigned>(width), 256, 0, ctx.stream>>>(x, n, width, norms + width);
         std::vector<double> host(2 * width);
         cudaMemcpyAsync(host.data(), norms, 2 * width * 8, cudaMemcpyDeviceToHost, ctx.stream);
         if (int code = ctx.drain()) return code;
@@ -2227,15 +2321,21 @@ namespace {
         return SCI_CUDA_OK;
     }
 
-    // |A|_inf and |b_j|_inf on the host.
+    // |A|_inf and |b_j|_inf on the host. a_norm_device: |A|_inf already on the device (narrow_sums
+    // computed it with the FP32 copy), else the row sums are taken here.
     int norms_of(Context &ctx, const double *a, const double *b, double *sums, double *norms, unsigned long long n,
-                 unsigned long long width, double &a_norm, std::vector<double> &b_norm) {
-        row_sums<double><<<static_cast<unsigned>((n + 7) / 8), 256, 0, ctx.stream>>>(a, n, sums);
+                 unsigned long long width, double &a_norm, std::vector<double> &b_norm,
+                 const double *a_norm_device = nullptr) {
         column_max<<<static_cast<unsigned>(width), 256, 0, ctx.stream>>>(b, n, width, norms);
-        std::vector<double> host_sums(n);
         b_norm.assign(width, 0.0);
-        cudaMemcpyAsync(host_sums.data(), sums, n * 8, cudaMemcpyDeviceToHost, ctx.stream);
         cudaMemcpyAsync(b_norm.data(), norms, width * 8, cudaMemcpyDeviceToHost, ctx.stream);
+        if (a_norm_device != nullptr) {
+            cudaMemcpyAsync(&a_norm, a_norm_device, 8, cudaMemcpyDeviceToHost, ctx.stream);
+            return ctx.drain();
+        }
+        row_sums<double><<<static_cast<unsigned>((n + 7) / 8), 256, 0, ctx.stream>>>(a, n, sums);
+        std::vector<double> host_sums(n);
+        cudaMemcpyAsync(host_sums.data(), sums, n * 8, cudaMemcpyDeviceToHost, ctx.stream);
         if (int code = ctx.drain()) return code;
         a_norm = 0.0;
         for (double v : host_sums) a_norm = std::max(a_norm, v);
@@ -2247,13 +2347,16 @@ namespace {
     // max_j |r_j|_inf / (|A|_inf |x_j|_inf + |b_j|_inf) is at most sqrt(n) eps (eps = 2^-53, the
     // stopping test of LAPACK's mixed-precision DSGESV) capped at 1e-14, or stops halving; at most
     // 30 corrections.
-    // correct(r, x) adds the FP32 correction for residual r into x.
+    // correct(r, x) adds the FP32 correction for residual r into x; with x_max_in_correct it also
+    // max-es each column's |x| into norms[width + j], which the loop zeroes before each correction.
+    // a_norm_device: |A|_inf already computed on the device (or null).
     template <class Correct>
     int refine_loop(Context &ctx, const double *a, const double *b, double *x, double *r, double *sums, double *norms,
-                    unsigned long long n, unsigned long long width, Correct correct, double &berr, int &iterations) {
+                    unsigned long long n, unsigned long long width, Correct correct, double &berr, int &iterations,
+                    const double *a_norm_device = nullptr, bool x_max_in_correct = false) {
         double a_norm = 0.0;
         std::vector<double> b_norm;
-        if (int code = norms_of(ctx, a, b, sums, norms, n, width, a_norm, b_norm)) return code;
+        if (int code = norms_of(ctx, a, b, sums, norms, n, width, a_norm, b_norm, a_norm_device)) return code;
         cudaMemsetAsync(x, 0, n * width * 8, ctx.stream);
         const double target = std::min(std::sqrt(static_cast<double>(n)) * 0x1p-53, 1e-14);
         constexpr int kMaxIterations = 30;
@@ -2262,9 +2365,11 @@ namespace {
         iterations = 0;
         const double *residual = b;  // the first correction solves for b itself
         while (iterations < kMaxIterations) {
+            if (x_max_in_correct) cudaMemsetAsync(norms + width, 0, width * 8, ctx.stream);
             if (int code = correct(residual, x)) return code;
             ++iterations;
-            if (int code = backward_error(ctx, a, b, x, r, sums, norms, n, width, a_norm, b_norm.data(), berr)) return code;
+            if (int code = backward_error(ctx, a, b, x, r, sums, norms, n, width, a_norm, b_norm.data(), berr, x_max_in_correct))
+                return code;
             residual = r;
             if (!(berr > target) || !(berr < 0.5 * previous)) break;
             previous = berr;
@@ -2348,21 +2453,31 @@ extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uin
     double *r = carve.take<double>(nw);
     float *d = carve.take<float>(nw);
     double *sums = carve.take<double>(n);
-    double *norms = carve.take<double>(2 * width);
+    double *norms = carve.take<double>(2 * width + 1);
+    double *a_norm = norms + 2 * width;
     const int sms = context->sms;
 
-    narrow<<<blocks_for(n * n, sms), 256, 0, context->stream>>>(a, lu, n * n);
+    // the FP32 copy of A and |A|_inf in one pass over A
+    cudaMemsetAsync(a_norm, 0, 8, context->stream);
+    narrow_sums<<<static_cast<unsigned>((n + 7) / 8), 256, 0, context->stream>>>(a, lu, n, a_norm);
     if (int code = factor_device<float>(*context, lu, n, piv, moved, true, true, rows)) return code;
     if (int code = invert_diagonal<float>(*context, lu, n, inv)) return code;
+    // the update also takes each column's |x|_inf when every thread of it stays in one column
+    const bool fused_max = 256 % width == 0;
     auto correct = [&](const double *residual, double *xx) -> int {
         permute<double, float>(*context, residual, d, rows, n, width);
         if (int code = substitute_inverse<float>(*context, lu, inv, n, d, y, width)) return code;
-        widen_add<<<blocks_for(nw, sms), 256, 0, context->stream>>>(d, xx, nw);
+        if (fused_max)
+            widen_add_max<<<blocks_for(nw, sms), 256, 0, context->stream>>>(d, xx, nw, static_cast<unsigned>(width),
+                                                                           norms + width);
+        else
+            widen_add<<<blocks_for(nw, sms), 256, 0, context->stream>>>(d, xx, nw);
         return SCI_CUDA_OK;
     };
     double berr = 0.0;
     int iterations = 0;
-    if (int code = refine_loop(*context, a, b, x, r, sums, norms, n, width, correct, berr, iterations)) return code;
+    if (int code = refine_loop(*context, a, b, x, r, sums, norms, n, width, correct, berr, iterations, a_norm, fused_max))
+        return code;
     if (report) {
         report->backward_error = berr;
         report->iterations = iterations;
