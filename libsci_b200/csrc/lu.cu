@@ -1695,7 +1695,8 @@ namespace sci_cuda {
         // acquire of the mark shows every block row published so far.
         // Every CTA is resident (cooperative launch), and every wait is bounded: one that runs out
         // sets the timeout status and ends its CTA, so the CTAs after it end the same way.
-        constexpr int kSweepThreads = 4 * kSolveBlock;  // four quarters of the block's 128 rows
+        constexpr int kSweepThreads = 4 * kSolveBlock;  // 8 k-groups x 64 row pairs of the block's 128 rows
+        constexpr int kSweepGroups = 8;                 // k-groups of 16 columns of a 128-column tile
         constexpr unsigned kSweepWaitLimit = 1u << 22;
 
         __device__ __forceinline__ unsigned load_acquire(const unsigned *p) {
@@ -1724,6 +1725,20 @@ namespace sci_cuda {
 #pragma unroll
             for (int c = 0; c < C / 2; ++c) acc[c] = fma_(pa, pv[c], acc[c]);
         }
+        // acc0 += a0 * v and acc1 += a1 * v: each value of v loaded once for two rows
+        template <int C> __device__ __forceinline__ void axpy2(float a0, float a1, const float *v, Pair *acc0, Pair *acc1) {
+            const Pair p0 = pair(a0), p1 = pair(a1);
+            const Pair *pv = reinterpret_cast<const Pair *>(v);
+#pragma unroll
+            for (int c = 0; c < C / 2; ++c) {
+                const Pair x = pv[c];
+                acc0[c] = fma_(p0, x, acc0[c]);
+                acc1[c] = fma_(p1, x, acc1[c]);
+            }
+        }
+        template <int C> constexpr size_t sweep_shared_bytes() {
+            return sizeof(float) * (kSolveBlock * (C + 4) + kSweepGroups * kSolveBlock * (C + 1));
+        }
 
         // 16-byte asynchronous copy global -> shared through L2 only (no stale L1 line of another SM's
         // results can be read), zero-filled when `full` is false.
@@ -1747,9 +1762,10 @@ namespace sci_cuda {
             constexpr int P = C + 4;  // pitch of a staged block row: 16-byte aligned rows
             constexpr int Q = C + 1;  // pitch of a partial-sum row
             constexpr int V = B * C / kSweepThreads;  // block elements per thread in the row-major mapping
+            constexpr int G = kSweepGroups, KG = B / G;  // k-groups and their width
             // staged[0]: a block of results (or the rhs) being applied; staged[1], the next block's
             // copy in flight, lives in the partial sums' space, which is free until the tiles are done
-            __shared__ __align__(16) float space[B * P + 4 * B * Q];
+            extern __shared__ __align__(16) float space[];  // sweep_shared_bytes<C>()
             float *const staged0 = space, *const staged1 = space + B * P;
             float (*partial)[B * Q] = reinterpret_cast<float (*)[B * Q]>(space + B * P);
             __shared__ bool stop;
@@ -1757,26 +1773,35 @@ namespace sci_cuda {
             const unsigned blocks = (n + B - 1) / B;
             const unsigned i = upper ? blocks - 1 - blockIdx.x / groups : blockIdx.x / groups;
             const unsigned g = blockIdx.x % groups, s = i * B, size = min(static_cast<unsigned>(B), n - s), c0 = g * C;
-            // thread = (quarter h, row r): a warp holds 32 rows of one quarter, so the staged reads
-            // below are broadcasts; quarter h covers the columns [32 h, 32 h + 32) of each tile
-            const int t = threadIdx.x, h = t / B, r = t % B;
+            // thread = (k-group h, row pair): rows r0 and r1 = r0 + 64, the columns [16 h, 16 h + 16)
+            // of each tile. A warp holds 32 row pairs of one k-group, so the staged reads below are
+            // broadcasts, each value used for both rows (half the shared loads of one row a thread).
+            const int t = threadIdx.x, h = t / (B / 2), r0 = t % (B / 2), r1 = r0 + B / 2;
             const unsigned tiles = upper ? blocks - 1 - i : i;
             const unsigned bulk = tiles > 2 ? tiles - 2 : 0;  // all tiles but the last two block rows'
             if (t == 0) stop = false;
+            // this thread's 16 values of rows r0 and r1 of block (2 i + upper) of `base` (the inverses
+            // and the coupling blocks share the layout)
+            const unsigned long long block_base = (2ull * i + (upper ? 1 : 0)) * B * B;
+            auto rows_of = [&](const float *base, float4 *dst) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    dst[u] = __ldg(reinterpret_cast<const float4 *>(base + block_base + r0 * B + KG * h) + u);
+                    dst[4 + u] = __ldg(reinterpret_cast<const float4 *>(base + block_base + r1 * B + KG * h) + u);
+                }
+            };
             // loaded before any wait: this block's inverse rows and its right-hand side
             float4 m[8];
-            const unsigned long long own = (2ull * i + (upper ? 1 : 0)) * B * B + r * B + 32 * h;
-#pragma unroll
-            for (int u = 0; u < 8; ++u) m[u] = __ldg(reinterpret_cast<const float4 *>(inv + own) + u);
+            rows_of(inv, m);
             float rhs[V];
 #pragma unroll
             for (int v = 0; v < V; ++v) {
                 const unsigned q = t + v * kSweepThreads, k = q / C, c = q % C;
                 rhs[v] = (s + k < n && c0 + c < width) ? in[static_cast<unsigned long long>(s + k) * width + c0 + c] : 0.0f;
             }
-            Pair acc[C / 2];
+            Pair acc[2][C / 2];  // rows r0, r1
 #pragma unroll
-            for (int c = 0; c < C / 2; ++c) acc[c] = pair(0.0f);
+            for (int c = 0; c < C / 2; ++c) acc[0][c] = acc[1][c] = pair(0.0f);
 
             // Step k of this CTA applies the block row k places along the chain (row_of(k)), which is
             // also its place in publishing order.
@@ -1831,48 +1856,58 @@ namespace sci_cuda {
                 }
                 copies_commit();
             };
-            // acc += this quarter's part of rows4 times the block in `source`
+            // acc += this k-group's part of rows4 (rows r0: [0, 4), r1: [4, 8)) times the block in `source`
             auto accumulate = [&](const float4 *rows4, const float *source) {
-                const float *base = source + 32 * h * P;
+                const float *base = source + KG * h * P;
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    axpy<C>(rows4[u].x, base + (4 * u + 0) * P, acc);
-                    axpy<C>(rows4[u].y, base + (4 * u + 1) * P, acc);
-                    axpy<C>(rows4[u].z, base + (4 * u + 2) * P, acc);
-                    axpy<C>(rows4[u].w, base + (4 * u + 3) * P, acc);
+                for (int u = 0; u < 4; ++u) {
+                    axpy2<C>(rows4[u].x, rows4[4 + u].x, base + (4 * u + 0) * P, acc[0], acc[1]);
+                    axpy2<C>(rows4[u].y, rows4[4 + u].y, base + (4 * u + 1) * P, acc[0], acc[1]);
+                    axpy2<C>(rows4[u].z, rows4[4 + u].z, base + (4 * u + 2) * P, acc[0], acc[1]);
+                    axpy2<C>(rows4[u].w, rows4[4 + u].w, base + (4 * u + 3) * P, acc[0], acc[1]);
                 }
             };
             // acc (zeroed) := the same
             auto multiply = [&](const float4 *rows4, const float *source) {
 #pragma unroll
-                for (int c = 0; c < C / 2; ++c) acc[c] = pair(0.0f);
+                for (int c = 0; c < C / 2; ++c) acc[0][c] = acc[1][c] = pair(0.0f);
                 accumulate(rows4, source);
             };
-            // the quarters' acc into `partial` (callers have synchronised past its last reads)
+            // the k-groups' acc into `partial` (callers have synchronised past its last reads)
             auto publish = [&]() {
-                float lanes[C];
 #pragma unroll
-                for (int c = 0; c < C / 2; ++c) unpair(acc[c], lanes[2 * c], lanes[2 * c + 1]);
+                for (int row = 0; row < 2; ++row) {
+                    float lanes[C];
 #pragma unroll
-                for (int c = 0; c < C; ++c) partial[h][r * Q + c] = lanes[c];
+                    for (int c = 0; c < C / 2; ++c) unpair(acc[row][c], lanes[2 * c], lanes[2 * c + 1]);
+                    const int r = row == 0 ? r0 : r1;
+#pragma unroll
+                    for (int c = 0; c < C; ++c) partial[h][r * Q + c] = lanes[c];
+                }
             };
             auto total = [&](unsigned q) {
                 const unsigned k = q / C, c = q % C;
-                return ((partial[0][k * Q + c] + partial[1][k * Q + c]) + partial[2][k * Q + c]) + partial[3][k * Q + c];
+                float sum = partial[0][k * Q + c];
+#pragma unroll
+                for (int w = 1; w < G; ++w) sum += partial[w][k * Q + c];
+                return sum;
             };
 
             // Every off-diagonal tile but the adjacent one, oldest results first, summed into acc;
             // the next block of results is copied in while the current one is applied.
-            const float *row = lu + static_cast<unsigned long long>(r < size ? s + r : s) * n;
+            const float *row0 = lu + static_cast<unsigned long long>(r0 < size ? s + r0 : s) * n;
+            const float *row1 = lu + static_cast<unsigned long long>(r1 < size ? s + r1 : s) * n;
             bool fetched = false;  // whether the current step's block is already on its way
             for (unsigned step = 0; step < bulk; ++step) {
                 const unsigned sj = row_of(step) * B;
                 float4 a[8];
 #pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const unsigned column = sj + 32 * h + 4 * u;
-                    a[u] = (r < size && column < n) ? __ldg(reinterpret_cast<const float4 *>(row + column))
-                                                    : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                for (int u = 0; u < 4; ++u) {
+                    const unsigned column = sj + KG * h + 4 * u;
+                    a[u] = (r0 < size && column < n) ? __ldg(reinterpret_cast<const float4 *>(row0 + column))
+                                                     : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    a[4 + u] = (r1 < size && column < n) ? __ldg(reinterpret_cast<const float4 *>(row1 + column))
+                                                         : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 }
                 // the next block is copied in now only if it is already known to be published (a
                 // CTA that has caught up with the chain applies the block it has, then waits)
@@ -1888,23 +1923,14 @@ namespace sci_cuda {
                     copies_wait<0>();
                 }
                 __syncthreads();  // the current block is in place for every thread
-                const float *base = ((step & 1) ? staged1 : staged0) + 32 * h * P;
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    axpy<C>(a[u].x, base + (4 * u + 0) * P, acc);
-                    axpy<C>(a[u].y, base + (4 * u + 1) * P, acc);
-                    axpy<C>(a[u].z, base + (4 * u + 2) * P, acc);
-                    axpy<C>(a[u].w, base + (4 * u + 3) * P, acc);
-                }
+                accumulate(a, (step & 1) ? staged1 : staged0);
                 __syncthreads();  // before the buffer is refilled
             }
             // the coupling rows of the block row two places back along the chain, in flight during
             // what follows
             const float *const far = couple + 2ull * blocks * B * B;
             float4 mc[8];
-#pragma unroll
-            for (int u = 0; u < 8; ++u)
-                mc[u] = tiles > 1 ? __ldg(reinterpret_cast<const float4 *>(far + own) + u) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (tiles > 1) rows_of(far, mc);
             // pre = inverse (rhs - sum), kept in registers in the row-major mapping
             publish();
             __syncthreads();
@@ -1925,12 +1951,9 @@ namespace sci_cuda {
             // The adjacent row's coupling rows are loaded after the far row's wait, so that the wait's
             // acquire does not wait for them, and they arrive while the far row is applied.
             float4 mn[8];
-            auto adjacent_rows = [&]() {
+            auto adjacent_rows = [&]() { rows_of(couple, mn); };
 #pragma unroll
-                for (int u = 0; u < 8; ++u) mn[u] = __ldg(reinterpret_cast<const float4 *>(couple + own) + u);
-            };
-#pragma unroll
-            for (int c = 0; c < C / 2; ++c) acc[c] = pair(0.0f);
+            for (int c = 0; c < C / 2; ++c) acc[0][c] = acc[1][c] = pair(0.0f);
             if (tiles > 1) {
                 __syncthreads();  // `partial` and staged0 are free again
                 if (!ready(tiles - 2)) return;
@@ -2016,19 +2039,29 @@ namespace sci_cuda {
                 cooperative = value;
             }
             if (!cooperative) return SCI_CUDA_OK;
-            auto capacity = [&](const void *lower, const void *upper) {
-                return static_cast<unsigned long long>(std::min(ctx.blocks_per_sm(lower, kSweepThreads, 0),
-                                                                ctx.blocks_per_sm(upper, kSweepThreads, 0))) *
-                       ctx.sms;
-            };
             const void *kernels[2][2] = {
                     {reinterpret_cast<const void *>(&sweep<false, 8>), reinterpret_cast<const void *>(&sweep<true, 8>)},
                     {reinterpret_cast<const void *>(&sweep<false, 16>), reinterpret_cast<const void *>(&sweep<true, 16>)}};
+            const size_t shared[2] = {sweep_shared_bytes<8>(), sweep_shared_bytes<16>()};
+            static const bool sized = [&] {
+                bool ok = true;
+                for (int f = 0; f < 2; ++f)
+                    for (int u = 0; u < 2; ++u)
+                        ok = ok && cudaFuncSetAttribute(kernels[f][u], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                        static_cast<int>(shared[f])) == cudaSuccess;
+                return ok;
+            }();
+            if (!sized) return SCI_CUDA_OK;  // the block-by-block path instead
+            auto capacity = [&](const void *lower, const void *upper, size_t bytes) {
+                return static_cast<unsigned long long>(std::min(ctx.blocks_per_sm(lower, kSweepThreads, bytes),
+                                                                ctx.blocks_per_sm(upper, kSweepThreads, bytes))) *
+                       ctx.sms;
+            };
             int form = -1;
             unsigned long long groups = 0;
             for (int f = 0; f < 2 && form < 0; ++f) {
                 const unsigned long long columns = f == 0 ? 8 : 16, g = (width + columns - 1) / columns;
-                if (blocks * g <= capacity(kernels[f][0], kernels[f][1])) {
+                if (blocks * g <= capacity(kernels[f][0], kernels[f][1], shared[f])) {
                     form = f;
                     groups = g;
                 }
@@ -2044,7 +2077,7 @@ namespace sci_cuda {
                 float *target = upper ? x : y;
                 void *args[] = {&lu, &inv, &couple, &nn, &ww, &gg, &source, &target, &ctx.sweep_flags, &epoch, &ctx.status};
                 if (int code = ctx.check(cudaLaunchCooperativeKernel(kernels[form][pass], dim3(static_cast<unsigned>(blocks * groups)),
-                                                                    dim3(kSweepThreads), args, 0, ctx.stream),
+                                                                    dim3(kSweepThreads), args, shared[form], ctx.stream),
                                          "launching a substitution sweep"))
                     return code;
             }
