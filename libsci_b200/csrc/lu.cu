@@ -1736,8 +1736,9 @@ namespace sci_cuda {
                 acc1[c] = fma_(p1, x, acc1[c]);
             }
         }
+        constexpr int kCouplePitch = kSolveBlock + 4;  // a staged coupling block's row pitch (16-byte rows)
         template <int C> constexpr size_t sweep_shared_bytes() {
-            return sizeof(float) * (kSolveBlock * (C + 4) + kSweepGroups * kSolveBlock * (C + 1));
+            return sizeof(float) * (kSolveBlock * (C + 4) + kSweepGroups * kSolveBlock * (C + 1) + 2 * kSolveBlock * kCouplePitch);
         }
 
         // 16-byte asynchronous copy global -> shared through L2 only (no stale L1 line of another SM's
@@ -1768,6 +1769,10 @@ namespace sci_cuda {
             extern __shared__ __align__(16) float space[];  // sweep_shared_bytes<C>()
             float *const staged0 = space, *const staged1 = space + B * P;
             float (*partial)[B * Q] = reinterpret_cast<float (*)[B * Q]>(space + B * P);
+            // the two coupling blocks (two rows back, adjacent), copied in at the start: loaded into
+            // registers after the tiles instead, their 128 KB held up the shared-memory reductions
+            // that follow (3 us of a 4 us step)
+            float *const couple_far = space + B * P + G * B * Q, *const couple_adjacent = couple_far + B * kCouplePitch;
             __shared__ bool stop;
             __shared__ int ready_shared;
             const unsigned blocks = (n + B - 1) / B;
@@ -1802,6 +1807,27 @@ namespace sci_cuda {
             Pair acc[2][C / 2];  // rows r0, r1
 #pragma unroll
             for (int c = 0; c < C / 2; ++c) acc[0][c] = acc[1][c] = pair(0.0f);
+            // the coupling blocks into shared memory, one group of copies committed before any other
+            // (the first wait for copies, at the latest the far block's, completes it)
+            {
+                const float *const far_block = couple + 2ull * blocks * B * B + block_base;
+                const float *const adjacent_block = couple + block_base;
+#pragma unroll 4
+                for (int u = 0; u < B * B / 4 / kSweepThreads; ++u) {
+                    const int q = t + u * kSweepThreads, row = q / (B / 4), c4 = 4 * (q % (B / 4));
+                    if (tiles > 1) copy16_async(couple_far + row * kCouplePitch + c4, far_block + row * B + c4, true);
+                    if (tiles > 0) copy16_async(couple_adjacent + row * kCouplePitch + c4, adjacent_block + row * B + c4, true);
+                }
+                copies_commit();
+            }
+            // this thread's 16 values of rows r0 and r1 of a staged coupling block
+            auto staged_rows = [&](const float *block, float4 *dst) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    dst[u] = *reinterpret_cast<const float4 *>(block + r0 * kCouplePitch + KG * h + 4 * u);
+                    dst[4 + u] = *reinterpret_cast<const float4 *>(block + r1 * kCouplePitch + KG * h + 4 * u);
+                }
+            };
 
             // Step k of this CTA applies the block row k places along the chain (row_of(k)), which is
             // also its place in publishing order.
@@ -1926,11 +1952,6 @@ namespace sci_cuda {
                 accumulate(a, (step & 1) ? staged1 : staged0);
                 __syncthreads();  // before the buffer is refilled
             }
-            // the coupling rows of the block row two places back along the chain, in flight during
-            // what follows
-            const float *const far = couple + 2ull * blocks * B * B;
-            float4 mc[8];
-            if (tiles > 1) rows_of(far, mc);
             // pre = inverse (rhs - sum), kept in registers in the row-major mapping
             publish();
             __syncthreads();
@@ -1948,22 +1969,17 @@ namespace sci_cuda {
             for (int v = 0; v < V; ++v) result[v] = total(t + v * kSweepThreads);
             // then the last two block rows: result = pre - inv(D_ii) (D_i,far x_far + D_i,adjacent x_adjacent),
             // the far one applied as soon as it is published, both summed before the one reduction.
-            // The adjacent row's coupling rows are loaded after the far row's wait, so that the wait's
-            // acquire does not wait for them, and they arrive while the far row is applied.
-            float4 mn[8];
-            auto adjacent_rows = [&]() { rows_of(couple, mn); };
 #pragma unroll
             for (int c = 0; c < C / 2; ++c) acc[0][c] = acc[1][c] = pair(0.0f);
             if (tiles > 1) {
                 __syncthreads();  // `partial` and staged0 are free again
                 if (!ready(tiles - 2)) return;
-                adjacent_rows();
                 fetch(tiles - 2, staged0);
                 copies_wait<0>();
                 __syncthreads();
-                accumulate(mc, staged0);
-            } else if (tiles > 0) {
-                adjacent_rows();
+                float4 rows4[8];
+                staged_rows(couple_far, rows4);
+                accumulate(rows4, staged0);
             }
             if (tiles > 0) {
                 __syncthreads();
@@ -1971,7 +1987,9 @@ namespace sci_cuda {
                 fetch(tiles - 1, staged0);
                 copies_wait<0>();
                 __syncthreads();
-                accumulate(mn, staged0);
+                float4 rows4[8];
+                staged_rows(couple_adjacent, rows4);
+                accumulate(rows4, staged0);
                 publish();
                 __syncthreads();
 #pragma unroll
