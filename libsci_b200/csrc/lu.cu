@@ -257,6 +257,10 @@ namespace sci_cuda {
             __shared__ __align__(16) T jbuf[2][W];  // CTA 0: the row at the pivot position
             __shared__ unsigned long long jbuf_origin[2];
             __shared__ long long exchanges[W];  // CTA 0: piv[j0 + j]
+            // CTA 0: U's rows of the panel (row j from column j0 + j on, at u_rows[j][0, width - j)) and
+            // the positions they are stored at until the final permutation, written out at the end
+            __shared__ __align__(16) T u_rows[W][W];
+            __shared__ unsigned long long u_origin[W];
 
             chain_wait();
             chain_release();
@@ -388,13 +392,14 @@ namespace sci_cuda {
                         origin[i] = inbox_head[par][kClusterCtas][1] & 0xFFFFFFFFull;
                     }
                     if (r[i] == row_j) {
-                        // the pivot row is final: U's row j0 + j from column j0 + j on
+                        // the pivot row is final: U's row j0 + j from column j0 + j on, kept for the end
+                        // (16-byte shared stores here instead of Q scalar global stores in the
+                        // column's critical warp)
 #pragma unroll
-                        for (int k = 0; k < Q; k += E) load16(pivot_row + k, &v[i][k]);
+                        for (int k = 0; k < Q; k += E)
+                            *reinterpret_cast<uint4 *>(&u_rows[j][k]) = *reinterpret_cast<const uint4 *>(pivot_row + k);
                         origin[i] = org;
-#pragma unroll
-                        for (int k = 0; k < Q; ++k)
-                            if (k < width - j) a[origin[i] * n + row_j + k] = v[i][k];
+                        u_origin[j] = org;
                     }
                     // 4. eliminate below the pivot: l = a / pivot; a[k] -= l * pivot_row[k]; a zero
                     //    pivot leaves the column as it is (decompose.hpp:44-45)
@@ -442,6 +447,11 @@ namespace sci_cuda {
                 const unsigned long long g = first + row;
                 if (g >= n) break;
                 if (lane < static_cast<unsigned>(width) && (home[row] >> lane & 1u)) a[g * n + j0 + lane] = stage[lane * P + row];
+            }
+            if (c == 0) {
+                // U's rows, at the positions the pivot rows started in (moved with them below)
+                for (int j = warp; j < width; j += WARPS)
+                    if (lane < static_cast<unsigned>(width - j)) a[u_origin[j] * n + j0 + j + lane] = u_rows[j][lane];
             }
             __threadfence();
             cluster_sync();
