@@ -73,21 +73,6 @@ namespace sci_cuda {
             asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(mapped) : "r"(address), "r"(rank));
             return mapped;
         }
-        __device__ __forceinline__ float load_remote(unsigned address, float) {
-            float v;
-            asm volatile("ld.shared::cluster.f32 %0, [%1];" : "=f"(v) : "r"(address) : "memory");
-            return v;
-        }
-        __device__ __forceinline__ double load_remote(unsigned address, double) {
-            double v;
-            asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(address) : "memory");
-            return v;
-        }
-        __device__ __forceinline__ unsigned long long load_remote_u64(unsigned address) {
-            unsigned long long v;
-            asm volatile("ld.shared::cluster.u64 %0, [%1];" : "=l"(v) : "r"(address) : "memory");
-            return v;
-        }
 
         // The panel's net row movement: after its exchanges, row rows[i] holds what row src[i] held.
         // Only rows the panel touched appear (at most twice its width).
@@ -129,15 +114,6 @@ namespace sci_cuda {
             const bool tie = hi == top_hi && lo == top_lo;
             rel = __reduce_min_sync(0xffffffffu, tie ? rel : kNoRow);
             key = (static_cast<unsigned long long>(top_hi) << 32) | top_lo;
-        }
-        __device__ __forceinline__ unsigned load_remote_u32(unsigned address) {
-            unsigned v;
-            asm volatile("ld.shared::cluster.u32 %0, [%1];" : "=r"(v) : "r"(address) : "memory");
-            return v;
-        }
-        __device__ __forceinline__ unsigned load_remote_key(unsigned address, unsigned) { return load_remote_u32(address); }
-        __device__ __forceinline__ unsigned long long load_remote_key(unsigned address, unsigned long long) {
-            return load_remote_u64(address);
         }
         template <int N> struct Span {
             static constexpr int value = N;
