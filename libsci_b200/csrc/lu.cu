@@ -1535,10 +1535,16 @@ namespace sci_cuda {
                                 unsigned long long c1, bool narrow) -> int {
                 if (t0 >= n || c1 <= c0) return SCI_CUDA_OK;
                 const unsigned long long ob = t0 - J0;
-                // narrow follows the block's U rows (a kernel) directly on the main stream: chained
-                if (narrow)
-                    return update<T>(ctx, a + t0 * n + J0, n, a + J0 * n + c0, n, a + t0 * n + c0, n, n - t0, c1 - c0, ob, true);
-                if constexpr (sizeof(T) == 4) {
+                // narrow (the next block's columns, on the main stream) in FP64 follows the block's U
+                // rows directly: the SIMT rank update, chained; in float the tensor cores take it too
+                if constexpr (sizeof(T) == 8) {
+                    if (narrow)
+                        return update<T>(ctx, a + t0 * n + J0, n, a + J0 * n + c0, n, a + t0 * n + c0, n, n - t0, c1 - c0, ob,
+                                         true);
+                } else {
+                    if (narrow && !tensor)
+                        return update<T>(ctx, a + t0 * n + J0, n, a + J0 * n + c0, n, a + t0 * n + c0, n, n - t0, c1 - c0, ob,
+                                         true);
                     if (tensor)
                         return tensor_gemm(ctx, split ? 3 : 1, a + t0 * n + J0, n, a + J0 * n + c0, n, a + t0 * n + c0, n,
                                            n - t0, c1 - c0, ob, true);
