@@ -81,6 +81,8 @@ namespace sci_cuda {
         int *status{nullptr};          // device-side error word
         double *host_result{nullptr};  // pinned
         int *host_status{nullptr};     // pinned
+        double *pinned{nullptr};       // pinned doubles for small read-backs (grown on demand)
+        size_t pinned_count{0};
 
         std::vector<Retired> retired;  // frees deferred until queued work is done
         std::map<std::tuple<const void *, int, size_t>, int> occupancy;  // (kernel, threads, smem) -> blocks/SM

@@ -308,6 +308,7 @@ int sci_cuda_close(sci_cuda_context *context) {
         }
         cudaFreeHost(context->host_result);
         cudaFreeHost(context->host_status);
+        cudaFreeHost(context->pinned);
         cudaStreamDestroy(context->stream);
     }
     delete context;

@@ -43,7 +43,9 @@ namespace sci_cuda {
 
         constexpr unsigned long long kPanelRows = 8192;  // the panel cluster holds every row in registers
         constexpr unsigned long long kOuter = 256;
-        constexpr int kMovements = static_cast<int>(kOuter / 16);  // per-panel row movements of one outer block
+        // per-panel row movements of two outer blocks (by block parity: the side stream still applies
+        // one block's while the next block's panels write theirs)
+        constexpr int kMovements = 2 * static_cast<int>(kOuter / 16);
         constexpr int kSolveBlock = 128;
 
         template <typename T> struct PanelWidth {
@@ -146,12 +148,24 @@ namespace sci_cuda {
 
         // v[k] -= l * p[k] for k in [0, Q), each product and difference rounded on its own as in
         // the reference's column step (decompose.hpp:50-55); p is 16-byte aligned in shared memory.
-        // Float rows go two columns per instruction (mul / sub .rn.f32x2 round each lane exactly as
-        // the one-lane instructions do). Column 0 is computed too: the caller overwrites it.
-        template <int Q> __device__ __forceinline__ void eliminate_row(float *v, float l, const float *p) {
+        // Split in two: eliminate_head takes columns 0 and 1 (1 is the next column, whose pivot
+        // search can then start), eliminate_tail columns [2, Q). Float rows go two columns per
+        // instruction (mul / sub .rn.f32x2 round each lane exactly as the one-lane instructions
+        // do). Column 0 is computed too: the caller overwrites it.
+        __device__ __forceinline__ void eliminate_head(float *v, float l, const float *p) {
+            const float2 q = *reinterpret_cast<const float2 *>(p);
+            const Pair d = sub(pair(v[0], v[1]), mul(pair(l), pair(q.x, q.y)));
+            unpair(d, v[0], v[1]);
+        }
+        template <int Q> __device__ __forceinline__ void eliminate_tail(float *v, float l, const float *p) {
             const Pair lp = pair(l);
+            {
+                const float2 q = *reinterpret_cast<const float2 *>(p + 2);
+                const Pair d = sub(pair(v[2], v[3]), mul(lp, pair(q.x, q.y)));
+                unpair(d, v[2], v[3]);
+            }
 #pragma unroll
-            for (int k0 = 0; k0 < Q; k0 += 4) {
+            for (int k0 = 4; k0 < Q; k0 += 4) {
                 const float4 q = *reinterpret_cast<const float4 *>(p + k0);
                 const Pair d0 = sub(pair(v[k0], v[k0 + 1]), mul(lp, pair(q.x, q.y)));
                 const Pair d1 = sub(pair(v[k0 + 2], v[k0 + 3]), mul(lp, pair(q.z, q.w)));
@@ -159,9 +173,13 @@ namespace sci_cuda {
                 unpair(d1, v[k0 + 2], v[k0 + 3]);
             }
         }
-        template <int Q> __device__ __forceinline__ void eliminate_row(double *v, double l, const double *p) {
+        __device__ __forceinline__ void eliminate_head(double *v, double l, const double *p) {
+            v[0] = sub(v[0], mul(l, p[0]));
+            v[1] = sub(v[1], mul(l, p[1]));
+        }
+        template <int Q> __device__ __forceinline__ void eliminate_tail(double *v, double l, const double *p) {
 #pragma unroll
-            for (int k0 = 0; k0 < Q; k0 += 2) {
+            for (int k0 = 2; k0 < Q; k0 += 2) {
                 const double2 q = *reinterpret_cast<const double2 *>(p + k0);
                 v[k0] = sub(v[k0], mul(l, q.x));
                 v[k0 + 1] = sub(v[k0 + 1], mul(l, q.y));
@@ -204,9 +222,13 @@ namespace sci_cuda {
         // warp 0 pushes the CTA's candidate with its values into every CTA's inbox (st.async,
         // counted on the receiver's mbarrier; CTA 0 also pushes the row at the pivot position);
         // then every warp of every CTA waits for its own inbox to fill (a bounded wait), picks the
-        // pivot from it and eliminates, so the column takes one CTA barrier. Inboxes alternate by
-        // column parity; a CTA sends into one again only after the barrier of the column in
-        // between, which its warps reach only after reading every message of the earlier column.
+        // pivot from it and eliminates, so the column takes one CTA barrier. A row's next column is
+        // eliminated first and the warp's search for the next pivot issued at once, so the search's
+        // latency overlaps the rest of the elimination. Inboxes and the published candidates
+        // alternate by column parity; a CTA sends into an inbox again only after the barrier of the
+        // column in between, which its warps reach only after reading every message of the earlier
+        // column, and warp 0 reads a parity's candidates before the barrier after which the warps
+        // publish into it again.
         template <typename T, int CL, int ROWS>
         __global__ void __launch_bounds__(kPanelBlock, 1)
                 panel_factor(T *a, unsigned long long n, unsigned long long j0, int width, long long *piv, Movement *moved,
@@ -218,10 +240,10 @@ namespace sci_cuda {
             T *stage = reinterpret_cast<T *>(panel_shared);  // stage[k * P + local row]
             __shared__ unsigned home[kCtaRows];          // bit k: stage holds column k of the row
             using Key = typename MagnitudeKey<T>::type;
-            __shared__ Key warp_key[WARPS];
-            __shared__ unsigned warp_rel[WARPS];
-            __shared__ unsigned long long warp_origin[WARPS];
-            __shared__ __align__(16) T warp_values[WARPS][W];
+            __shared__ Key warp_key[2][WARPS];
+            __shared__ unsigned warp_rel[2][WARPS];
+            __shared__ unsigned long long warp_origin[2][WARPS];
+            __shared__ __align__(16) T warp_values[2][WARPS][W];
             // The inbox, by column parity: slot q < CL holds CTA q's candidate (its values, then a
             // 16-byte head: key, then origin and row), slot CL the row at the pivot position (from
             // CTA 0). Rows are below 2^32 (n <= kPanelRows), so origin and row take 32 bits each.
@@ -261,21 +283,19 @@ namespace sci_cuda {
                 }
             }
 
-            // One column step, specialised on Q >= width - j: after j shifts only v[i][0, width - j)
-            // is live (the rest is zero), so publication, elimination and the shift stop at Q.
-            auto column = [&](auto span, const int j) {
-                constexpr int Q = decltype(span)::value;
-                const int par = j & 1;
-                const unsigned long long row_j = j0 + j;
-                // 1. candidacy; a NaN only stands at the pivot position itself, where the reference's
-                //    comparisons against it all fail (decompose.hpp:35-38).
+            // The warp's candidate for the column whose values sit at v[i][O], among rows `from` on: the
+            // best key and row, published by lane 0 at `parity`; returns the row (kNoRow: none). A NaN
+            // only stands at the pivot position itself, where the reference's comparisons against it
+            // all fail (decompose.hpp:35-38).
+            auto search = [&](auto offset, const int parity, const unsigned long long from) -> unsigned {
+                constexpr int O = decltype(offset)::value;
                 Key key = 0;
                 unsigned rel = kNoRow;
 #pragma unroll
                 for (int i = 0; i < R; ++i) {
-                    if (valid[i] && r[i] >= row_j) {
-                        const T m = fabs(v[i][0]);
-                        const bool candidate = m == m || r[i] == row_j;
+                    if (valid[i] && r[i] >= from) {
+                        const T m = fabs(v[i][O]);
+                        const bool candidate = m == m || r[i] == from;
                         const Key k = candidate ? magnitude_key(m == m ? m : T(INFINITY)) : Key(0);
                         const unsigned at = static_cast<unsigned>(r[i] - j0);
                         if (k > key || (k == key && k != 0 && at < rel)) {
@@ -286,24 +306,40 @@ namespace sci_cuda {
                 }
                 best_of_warp(key, rel);
                 if (lane == 0) {
-                    warp_key[warp] = key;
-                    warp_rel[warp] = rel;
+                    warp_key[parity][warp] = key;
+                    warp_rel[parity][warp] = rel;
                 }
+                return rel;
+            };
+            // The winning lane's values from v[i][O] on (Q of them, zero past the row's W) and origin at
+            // `parity`; in CTA 0 the thread holding row `from` (the next pivot position) stages it too.
+            auto stage_candidate = [&](auto offset, auto span, const int parity, const unsigned rel,
+                                       const unsigned long long from) {
+                constexpr int O = decltype(offset)::value, Q = decltype(span)::value;
 #pragma unroll
                 for (int i = 0; i < R; ++i) {
                     if (rel != kNoRow && r[i] - j0 == rel) {
 #pragma unroll
-                        for (int k = 0; k < Q; ++k) warp_values[warp][k] = v[i][k];
-                        warp_origin[warp] = origin[i];
+                        for (int k = 0; k < Q; ++k) warp_values[parity][warp][k] = k + O < W ? v[i][k + O] : T(0);
+                        warp_origin[parity][warp] = origin[i];
                     }
                 }
-                if (c == 0 && t == static_cast<unsigned>(j)) {  // row_j is row 0 of thread j in CTA 0
+                if (c == 0 && t == static_cast<unsigned>(from - j0)) {  // row `from` is row 0 of that thread
 #pragma unroll
-                    for (int k = 0; k < Q; ++k) jbuf[par][k] = v[0][k];
-                    jbuf_origin[par] = origin[0];
+                    for (int k = 0; k < Q; ++k) jbuf[parity][k] = k + O < W ? v[0][k + O] : T(0);
+                    jbuf_origin[parity] = origin[0];
                 }
+            };
+
+            // One column step, specialised on Q >= width - j: after j shifts only v[i][0, width - j)
+            // is live (the rest is zero), so publication, elimination and the shift stop at Q. The
+            // column's candidates were published (parity j & 1) by the step before, or before the loop.
+            auto column = [&](auto span, const int j) {
+                constexpr int Q = decltype(span)::value;
+                const int par = j & 1;
+                const unsigned long long row_j = j0 + j;
                 __syncthreads();  // every warp's candidate (and CTA 0's pivot-position row) is staged
-                // 2. warp 0: the CTA's candidate; lane q sends it to CTA q (and lane q of CTA 0's warp 1
+                // 1. warp 0: the CTA's candidate; lane q sends it to CTA q (and lane q of CTA 0's warp 1
                 //    the pivot-position row), 16 bytes per store, the message's words read from shared
                 //    memory before the first store. A slot of parity par is rewritten two columns later, after every
                 //    reader has taken its pivot from it (each CTA's next message follows its own
@@ -324,18 +360,18 @@ namespace sci_cuda {
                     send16(head, static_cast<unsigned>(k), static_cast<unsigned>(k >> 32), static_cast<unsigned>(o), rw, bar);
                 };
                 if (warp == 0) {
-                    Key k2 = lane < WARPS ? warp_key[lane] : Key(0);
-                    unsigned r2 = lane < WARPS ? warp_rel[lane] : kNoRow;
+                    Key k2 = lane < WARPS ? warp_key[par][lane] : Key(0);
+                    unsigned r2 = lane < WARPS ? warp_rel[par][lane] : kNoRow;
                     best_of_warp(k2, r2);
                     const unsigned source = r2 == kNoRow ? 0u : ((r2 - c * kCtaRows) % TH) / 32;
                     if (lane < static_cast<unsigned>(kClusterCtas))
-                        send(warp_values[source], c, static_cast<unsigned long long>(k2), warp_origin[source], r2);
+                        send(warp_values[par][source], c, static_cast<unsigned long long>(k2), warp_origin[par][source], r2);
                     if (lane == 0) barrier_expect(&inbox_bar[par], (kClusterCtas + 1) * kMessage);
                 } else if (warp == 1 && c == 0 && lane < static_cast<unsigned>(kClusterCtas)) {
                     // CTA 0's pivot-position row, from another warp (another scheduler) at the same time
                     send(jbuf[par], kClusterCtas, 0ull, jbuf_origin[par], 0u);
                 }
-                // 3. every warp waits for its CTA's inbox to fill (a bounded wait: one that runs out
+                // 2. every warp waits for its CTA's inbox to fill (a bounded wait: one that runs out
                 //    flags the status, and no later column waits) and takes the pivot from it
                 if (!stalled && !barrier_wait(&inbox_bar[par], static_cast<unsigned>(j >> 1) & 1u) && lane == 0) {
                     stalled = true;
@@ -359,6 +395,9 @@ namespace sci_cuda {
                 const T *const pivot_row = inbox[par][q];
                 if (c == 0 && t == 0) exchanges[j] = static_cast<long long>(prow);
                 constexpr int E = 16 / sizeof(T);  // pivot-row values per 16-byte load
+                const T diagonal = pivot_row[0];
+                T l[R];
+                bool below[R];
 #pragma unroll
                 for (int i = 0; i < R; ++i) {
                     if (r[i] == prow && prow != row_j) {
@@ -377,22 +416,35 @@ namespace sci_cuda {
                         origin[i] = org;
                         u_origin[j] = org;
                     }
-                    // 4. eliminate below the pivot: l = a / pivot; a[k] -= l * pivot_row[k]; a zero
-                    //    pivot leaves the column as it is (decompose.hpp:44-45)
-                    if (valid[i] && r[i] > row_j) {
-                        const T diagonal = pivot_row[0];
-                        if (diagonal != T(0)) {
-                            const T l = div(v[i][0], diagonal);
-                            eliminate_row<Q>(v[i], l, pivot_row);
-                            v[i][0] = l;
-                        }
+                    // 3. eliminate below the pivot: l = a / pivot; a[k] -= l * pivot_row[k]; a zero
+                    //    pivot leaves the column as it is (decompose.hpp:44-45). The next column
+                    //    (v[i][1]) first.
+                    below[i] = valid[i] && r[i] > row_j;
+                    l[i] = v[i][0];
+                    if (below[i] && diagonal != T(0)) {
+                        l[i] = div(v[i][0], diagonal);
+                        eliminate_head(v[i], l[i], pivot_row);
+                    }
+                }
+                // 4. the next column's search, while the rest of the elimination runs
+                const bool more = j + 1 < width;
+                const unsigned next_rel = more ? search(Span<1>{}, par ^ 1, row_j + 1) : kNoRow;
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+                    if (below[i] && diagonal != T(0)) eliminate_tail<Q>(v[i], l[i], pivot_row);
+                    if (below[i]) {
+                        v[i][0] = l[i];
                         if (origin[i] == r[i]) {
-                            stage[j * P + static_cast<int>(r[i] - first)] = v[i][0];
+                            stage[j * P + static_cast<int>(r[i] - first)] = l[i];
                             mask[i] |= 1u << j;
                         } else {
-                            a[origin[i] * n + row_j] = v[i][0];
+                            a[origin[i] * n + row_j] = l[i];
                         }
                     }
+                }
+                if (more) stage_candidate(Span<1>{}, span, par ^ 1, next_rel, row_j + 1);
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
 #pragma unroll
                     for (int k = 0; k + 1 < Q; ++k) v[i][k] = v[i][k + 1];
                     v[i][Q - 1] = T(0);
@@ -404,6 +456,8 @@ namespace sci_cuda {
                 stalled = false;
                 asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
             }
+            // column 0's candidates
+            stage_candidate(Span<0>{}, Span<W>{}, 0, search(Span<0>{}, 0, j0), j0);
             cluster_sync();  // every CTA's inbox barriers exist before the first message
 #pragma unroll 1
             for (int j = 0; j < width; ++j) {
@@ -610,16 +664,16 @@ namespace sci_cuda {
         }
 
         // The panels' net row movements for `count` movements in turn (a block's panels, in their
-        // order) over every column outside [skip0, skip1). One CTA of 256 threads per 32 columns: lane
-        // l takes column l of the CTA's 32 and warp g the movement's entries g, g + 8, ..., so a row's
-        // 32 columns are one coalesced 128-byte access; per movement all reads, a barrier, all
-        // writes, a barrier (each movement sees the one before it).
+        // order) over the columns [c0, c1). One CTA of 256 threads per 32 columns: lane l takes column
+        // l of the CTA's 32 and warp g the movement's entries g, g + 8, ..., so a row's 32 columns are
+        // one coalesced 128-byte access; per movement all reads, a barrier, all writes, a barrier
+        // (each movement sees the one before it).
         template <typename T>
         __global__ void __launch_bounds__(256) move_rows_all(T *a, unsigned long long n, const Movement *moved, int count,
-                                                            unsigned long long skip0, unsigned long long skip1) {
+                                                            unsigned long long c0, unsigned long long c1) {
             const int lane = static_cast<int>(threadIdx.x % 32), g = static_cast<int>(threadIdx.x / 32);
-            const unsigned long long col = blockIdx.x * 32ull + lane;
-            const bool active = col < n && !(col >= skip0 && col < skip1);
+            const unsigned long long col = c0 + blockIdx.x * 32ull + lane;
+            const bool active = col < c1;
             for (int p = 0; p < count; ++p) {
                 const int rows = static_cast<int>(moved[p].count);
                 T values[8];
@@ -768,15 +822,16 @@ namespace sci_cuda {
         // triangle (ob <= kOuter): the U rows of a block over other columns. The same steps, rounded
         // the same way, as a chain of move_solve's solve (a panel's W rows in order) and rank_update
         // (the rows below the panel minus the sum, in order, of the panel's products), in one launch:
-        // one CTA of 256 threads per strip of kStripColumns columns (16: more CTAs, a shorter update
-        // per panel) holds the strip's block rows in shared memory. Per panel: warp w < 4 solves
-        // columns [4 w, 4 w + 4) with eight lanes per column, lane l % 8 holding rows l % 8, + 8, ...
-        // of the panel (the owner of row k hands its value to the column's lanes, which subtract its
-        // product from their later rows); then each thread takes (row below, four columns) items with
-        // the row's W multipliers in registers.
-        constexpr int kStripColumns = 16, kStripRows = 256;
-        template <typename T> constexpr size_t strip_shared_bytes() {
-            return sizeof(T) * kStripRows * ((kStripColumns + 16 / sizeof(T)) + (PanelWidth<T>::value + 16 / sizeof(T)));
+        // one CTA of 256 threads per strip of CS columns holds the strip's block rows in shared
+        // memory: CS = 16 for the bulk of the columns (each CTA reads the whole triangle), CS = 4 for
+        // the next block's columns on the critical path (more CTAs, a quarter of the update per
+        // panel). Per panel: warp w < CS / 4 solves columns [4 w, 4 w + 4) with eight lanes per
+        // column, lane l % 8 holding rows l % 8, + 8, ... of the panel (the owner of row k hands its
+        // value to the column's lanes, which subtract its product from their later rows); then each
+        // thread takes (row below, four columns) items with the row's W multipliers in registers.
+        constexpr int kStripColumns = 16, kStripColumnsNarrow = 4, kStripRows = 256;
+        template <typename T, int CS> constexpr size_t strip_shared_bytes() {
+            return sizeof(T) * kStripRows * ((CS + 16 / sizeof(T)) + (PanelWidth<T>::value + 16 / sizeof(T)));
         }
         template <typename T> __device__ __forceinline__ void load4(const T *p, T *v) {
             if constexpr (sizeof(T) == 4) {
@@ -786,10 +841,10 @@ namespace sci_cuda {
                 load16(p + 2, v + 2);
             }
         }
-        template <typename T>
+        template <typename T, int CS>
         __global__ void __launch_bounds__(256) block_rows_strip(T *a, unsigned long long n, unsigned long long J0, int ob,
                                                                unsigned long long c0, unsigned long long c1) {
-            constexpr int W = PanelWidth<T>::value, CS = kStripColumns, RW = kStripRows;
+            constexpr int W = PanelWidth<T>::value, RW = kStripRows;
             constexpr int XP = CS + 16 / sizeof(T), LP = W + 16 / sizeof(T);  // 16-byte aligned rows
             constexpr int PER = W / 8;  // panel rows per lane in the solve
             extern __shared__ __align__(16) unsigned char strip_shared[];
@@ -1477,13 +1532,14 @@ namespace sci_cuda {
         }
 
         // A (n x n, in place) := L\U with partial pivoting, right-looking in outer blocks of kOuter
-        // columns and panels of W inside them. moved holds kMovements row movements (one per panel
-        // of a block). With look-ahead (SCI_CUDA_LOOKAHEAD unset or not 0), each block's panels
-        // move rows only inside the block's columns; the block's movements reach every other
-        // column after the previous block's bulk update is done. Then the main stream updates the
-        // next block's columns (its U rows and trailing update) and goes on to its panels, while the
-        // side stream updates the columns beyond it. The two streams touch disjoint columns, and the
-        // main stream waits for the side before it moves rows outside a block.
+        // columns and panels of W inside them. moved holds kMovements row movements: one per panel of
+        // a block, in the half of the block's parity. With look-ahead (SCI_CUDA_LOOKAHEAD unset or
+        // not 0), each block's panels move rows only inside the block's columns; the block's
+        // movements reach every other column after the previous block's bulk update is done. Then
+        // the main stream updates the next block's columns (its U rows and trailing update) and goes
+        // on to its panels, while the side stream updates the columns beyond it. The two streams
+        // touch disjoint columns (and movement halves), and the main stream waits for the side
+        // before it moves rows outside a block.
         template <typename T>
         int factor_device(Context &ctx, T *a, unsigned long long n, long long *piv, Movement *moved, bool tensor,
                           bool split, unsigned *order = nullptr) {
@@ -1514,18 +1570,38 @@ namespace sci_cuda {
             }
             const int cluster = panel_cluster<T>();
             if (cluster == 0) return ctx.fail(SCI_CUDA_ERROR_LAUNCH, "the panel kernel's cluster cannot be scheduled");
-            const unsigned move_blocks = static_cast<unsigned>((n + 31) / 32);  // move_rows_all: 32 columns per CTA
+            // a block's row movements over the columns [c0, c1) (move_rows_all: 32 columns per CTA)
+            auto move_rows = [&](const Movement *block_moves, unsigned long long c0, unsigned long long c1, int panels) {
+                if (c1 > c0)
+                    move_rows_all<T><<<static_cast<unsigned>((c1 - c0 + 31) / 32), 256, 0, ctx.stream>>>(a, n, block_moves,
+                                                                                                     panels, c0, c1);
+            };
             // U rows of the block (columns [c0, c1)) = L11^-1 A12: one launch, a CTA per strip of columns
-            static const cudaError_t strip_sized = cudaFuncSetAttribute(
-                    reinterpret_cast<const void *>(&block_rows_strip<T>), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                    static_cast<int>(strip_shared_bytes<T>()));
+            // (narrow strips for the next block's columns, on the critical path)
+            static const cudaError_t strip_sized = [] {
+                const cudaError_t wide = cudaFuncSetAttribute(
+                        reinterpret_cast<const void *>(&block_rows_strip<T, kStripColumns>),
+                        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(strip_shared_bytes<T, kStripColumns>()));
+                const cudaError_t thin = cudaFuncSetAttribute(
+                        reinterpret_cast<const void *>(&block_rows_strip<T, kStripColumnsNarrow>),
+                        cudaFuncAttributeMaxDynamicSharedMemorySize,
+                        static_cast<int>(strip_shared_bytes<T, kStripColumnsNarrow>()));
+                return wide != cudaSuccess ? wide : thin;
+            }();
             if (int code = ctx.check(strip_sized, "sizing the block rows' shared memory")) return code;
             auto block_rows = [&](unsigned long long J0, unsigned long long block_end, unsigned long long c0,
-                                  unsigned long long c1) -> int {
+                                  unsigned long long c1, bool narrow) -> int {
                 if (c1 <= c0) return SCI_CUDA_OK;
-                const dim3 grid(static_cast<unsigned>((c1 - c0 + kStripColumns - 1) / kStripColumns));
-                block_rows_strip<T><<<grid, 256, strip_shared_bytes<T>(), ctx.stream>>>(a, n, J0, static_cast<int>(block_end - J0),
-                                                                                      c0, c1);
+                const int ob = static_cast<int>(block_end - J0);
+                if (narrow) {
+                    constexpr int CS = kStripColumnsNarrow;
+                    block_rows_strip<T, CS><<<static_cast<unsigned>((c1 - c0 + CS - 1) / CS), 256, strip_shared_bytes<T, CS>(),
+                                              ctx.stream>>>(a, n, J0, ob, c0, c1);
+                } else {
+                    constexpr int CS = kStripColumns;
+                    block_rows_strip<T, CS><<<static_cast<unsigned>((c1 - c0 + CS - 1) / CS), 256, strip_shared_bytes<T, CS>(),
+                                              ctx.stream>>>(a, n, J0, ob, c0, c1);
+                }
                 return ctx.check(cudaGetLastError(), "launching the block's U rows");
             };
             // trailing update of columns [c0, c1): A[t0:, c0:c1] -= L[t0:, J0:t0] U[J0:t0, c0:c1]
@@ -1557,10 +1633,11 @@ namespace sci_cuda {
             bool side_pending = false;
             for (unsigned long long J0 = 0; J0 < n; J0 += kOuter) {
                 const unsigned long long ob = std::min<unsigned long long>(kOuter, n - J0), block_end = J0 + ob;
+                Movement *const block_moves = moved + (J0 / kOuter % 2) * (kMovements / 2);
                 int panels = 0;
                 for (unsigned long long j0 = J0; j0 < block_end; j0 += W, ++panels) {
                     const int w = static_cast<int>(std::min<unsigned long long>(W, block_end - j0));
-                    Movement *mine = moved + panels;
+                    Movement *mine = block_moves + panels;
                     // Within a block, each kernel of the chain panel -> row moves -> U rows -> rank
                     // update -> next panel follows the one before it directly on the stream, so it is
                     // launched chained (programmatic dependent launch): its launch overlaps the end of
@@ -1587,32 +1664,52 @@ namespace sci_cuda {
                     }
                     if (int code = ctx.check(cudaGetLastError(), "launching the panel updates")) return code;
                 }
-                if (ahead) {
-                    // the block's movements reach the other columns once the side stream is done with them
-                    if (side_pending) {
-                        if (int code = ctx.check(cudaStreamWaitEvent(ctx.stream, ctx.side_done, 0), "waiting for the side"))
-                            return code;
-                        side_pending = false;
-                    }
-                    move_rows_all<T><<<move_blocks, 256, 0, ctx.stream>>>(a, n, moved, panels, J0, block_end);
+                if (!ahead) {
+                    // without look-ahead every panel moved its rows everywhere; the rest of the matrix
+                    if (block_end >= n) continue;
+                    if (int code = block_rows(J0, block_end, block_end, n, false)) return code;
+                    if (int code = trailing(J0, block_end, block_end, n, false)) return code;
+                    continue;
                 }
-                if (block_end >= n) continue;
-                const unsigned long long next = ahead ? std::min<unsigned long long>(kOuter, n - block_end) : n - block_end;
-                const unsigned long long split_at = block_end + next;
-                if (split_at < n) {
-                    // the columns beyond the next block: on the side stream, from here on
+                // The block's movements reach the other columns once the side stream is done with
+                // them. The main stream moves the next block's rows, takes its U rows and trailing
+                // update and goes on to its panels; the side stream moves the rows of the columns
+                // left of the block and beyond the next one and updates the latter. With the tensor
+                // cores the side's work is short, and it starts only after the main stream's (so the
+                // critical path's small kernels find the SMs free); the SIMT update is long and
+                // bounds the factorisation, so there the side starts first.
+                if (side_pending) {
+                    if (int code = ctx.check(cudaStreamWaitEvent(ctx.stream, ctx.side_done, 0), "waiting for the side"))
+                        return code;
+                    side_pending = false;
+                }
+                const unsigned long long split_at = std::min<unsigned long long>(block_end + kOuter, n);
+                move_rows(block_moves, block_end, split_at, panels);
+                if (split_at >= n) move_rows(block_moves, 0, J0, panels);
+                auto side_work = [&]() -> int {
                     if (int code = ctx.check(cudaEventRecord(ctx.main_ready, ctx.stream), "recording the main stream"))
                         return code;
                     OnSide side(ctx);
                     if (int code = ctx.check(cudaStreamWaitEvent(ctx.stream, ctx.main_ready, 0), "side waits")) return code;
-                    if (int code = block_rows(J0, block_end, split_at, n)) return code;
+                    move_rows(block_moves, 0, J0, panels);
+                    move_rows(block_moves, split_at, n, panels);
+                    if (int code = block_rows(J0, block_end, split_at, n, false)) return code;
                     if (int code = trailing(J0, block_end, split_at, n, false)) return code;
                     if (int code = ctx.check(cudaEventRecord(ctx.side_done, ctx.stream), "recording the side")) return code;
                     side_pending = true;
+                    return SCI_CUDA_OK;
+                };
+                const bool side_late = tensor && sizeof(T) == 4;
+                if (split_at < n && !side_late) {
+                    if (int code = side_work()) return code;
                 }
-                // the next block's columns (all columns beyond without look-ahead)
-                if (int code = block_rows(J0, block_end, block_end, split_at)) return code;
-                if (int code = trailing(J0, block_end, block_end, split_at, ahead)) return code;
+                if (block_end < n) {
+                    if (int code = block_rows(J0, block_end, block_end, split_at, true)) return code;
+                    if (int code = trailing(J0, block_end, block_end, split_at, true)) return code;
+                }
+                if (split_at < n && side_late) {
+                    if (int code = side_work()) return code;
+                }
             }
             if (side_pending) {
                 if (int code = ctx.check(cudaStreamWaitEvent(ctx.stream, ctx.side_done, 0), "waiting for the side")) return code;
@@ -2337,12 +2434,29 @@ extern "C" int sci_cuda_decompose(sci_cuda_context *context, uint32_t precision,
 
 namespace {
 
+    // Pinned host doubles for the refinement's small read-backs, at least `count` of them. Growing
+    // waits for the stream first: a copy into the old buffer may still be queued.
+    double *pinned_doubles(Context &ctx, size_t count) {
+        if (count <= ctx.pinned_count) return ctx.pinned;
+        cudaStreamSynchronize(ctx.stream);
+        cudaFreeHost(ctx.pinned);
+        ctx.pinned = nullptr;
+        ctx.pinned_count = 0;
+        void *memory = nullptr;
+        if (cudaMallocHost(&memory, count * sizeof(double)) != cudaSuccess) return nullptr;
+        ctx.pinned = static_cast<double *>(memory);
+        ctx.pinned_count = count;
+        return ctx.pinned;
+    }
+
     // The normwise backward error max_j |b_j - A x_j|_inf / (|A|_inf |x_j|_inf + |b_j|_inf), in FP64.
-    // r is scratch (n x width), sums (n), norms (2 width: |r_j|_inf, then |x_j|_inf); waits for the
-    // stream. x_ready: norms[width + j] already holds |x_j|_inf (the update computed it).
-    int backward_error(Context &ctx, const double *a, const double *b, const double *x, double *r, double *sums,
-                       double *norms, unsigned long long n, unsigned long long width, double a_norm, const double *b_norm,
-                       double &berr, bool x_ready = false) {
+    // r is scratch (n x width), norms (2 width: |r_j|_inf, then |x_j|_inf); `host` is pinned memory
+    // for 2 width doubles; waits for the stream, then reads |A|_inf from *a_norm and |b_j|_inf from
+    // b_norm[j] (host memory a copy queued earlier on the stream may fill). x_ready: norms[width + j]
+    // already holds |x_j|_inf (the update computed it).
+    int backward_error(Context &ctx, const double *a, const double *b, const double *x, double *r, double *norms,
+                       unsigned long long n, unsigned long long width, const double *a_norm, const double *b_norm,
+                       double *host, double &berr, bool x_ready = false) {
         static const cudaError_t sized = cudaFuncSetAttribute(
                 reinterpret_cast<const void *>(&residual_tiles), cudaFuncAttributeMaxDynamicSharedMemorySize,
                 static_cast<int>(kResidualShared));
@@ -2353,36 +2467,30 @@ namespace {
                          kResidualThreads, kResidualShared, ctx.stream>>>(a, x, b, r, n, width, norms);
         if (int code = ctx.check(cudaGetLastError(), "launching the residual")) return code;
         if (!x_ready) column_max<<<static_cast<unsigned>(width), 256, 0, ctx.stream>>>(x, n, width, norms + width);
-        std::vector<double> host(2 * width);
-        cudaMemcpyAsync(host.data(), norms, 2 * width * 8, cudaMemcpyDeviceToHost, ctx.stream);
+        cudaMemcpyAsync(host, norms, 2 * width * 8, cudaMemcpyDeviceToHost, ctx.stream);
         if (int code = ctx.drain()) return code;
         berr = 0.0;
         for (unsigned long long j = 0; j < width; ++j) {
-            const double e = host[j] / (a_norm * host[width + j] + b_norm[j]);
+            const double e = host[j] / (*a_norm * host[width + j] + b_norm[j]);
             berr = (e > berr || e != e) ? e : berr;
         }
         return SCI_CUDA_OK;
     }
 
-    // |A|_inf and |b_j|_inf on the host. a_norm_device: |A|_inf already on the device (narrow_sums
-    // computed it with the FP32 copy), else the row sums are taken here.
-    int norms_of(Context &ctx, const double *a, const double *b, double *sums, double *norms, unsigned long long n,
-                 unsigned long long width, double &a_norm, std::vector<double> &b_norm,
-                 const double *a_norm_device = nullptr) {
+    // Queues |b_j|_inf (into norms[0, width)) and |A|_inf and their copies to host[0, width) and
+    // host[width], without waiting: the next wait for the stream makes them readable. a_norm_device:
+    // |A|_inf already computed on the device (narrow_sums takes it with the FP32 copy), else the row
+    // sums are taken here (into sums) and their maximum into norms[2 width].
+    void norms_enqueue(Context &ctx, const double *a, const double *b, double *sums, double *norms, unsigned long long n,
+                       unsigned long long width, const double *a_norm_device, double *host) {
         column_max<<<static_cast<unsigned>(width), 256, 0, ctx.stream>>>(b, n, width, norms);
-        b_norm.assign(width, 0.0);
-        cudaMemcpyAsync(b_norm.data(), norms, width * 8, cudaMemcpyDeviceToHost, ctx.stream);
-        if (a_norm_device != nullptr) {
-            cudaMemcpyAsync(&a_norm, a_norm_device, 8, cudaMemcpyDeviceToHost, ctx.stream);
-            return ctx.drain();
+        if (a_norm_device == nullptr) {
+            row_sums<double><<<static_cast<unsigned>((n + 7) / 8), 256, 0, ctx.stream>>>(a, n, sums);
+            column_max<<<1, 256, 0, ctx.stream>>>(sums, n, 1, norms + 2 * width);
+            a_norm_device = norms + 2 * width;
         }
-        row_sums<double><<<static_cast<unsigned>((n + 7) / 8), 256, 0, ctx.stream>>>(a, n, sums);
-        std::vector<double> host_sums(n);
-        cudaMemcpyAsync(host_sums.data(), sums, n * 8, cudaMemcpyDeviceToHost, ctx.stream);
-        if (int code = ctx.drain()) return code;
-        a_norm = 0.0;
-        for (double v : host_sums) a_norm = std::max(a_norm, v);
-        return SCI_CUDA_OK;
+        cudaMemcpyAsync(host, norms, width * 8, cudaMemcpyDeviceToHost, ctx.stream);
+        cudaMemcpyAsync(host + width, a_norm_device, 8, cudaMemcpyDeviceToHost, ctx.stream);
     }
 
     // The refinement loop for a x = b (a n x n, b and x n x width, double): x = 0, r = b; repeat
@@ -2392,14 +2500,19 @@ namespace {
     // 30 corrections.
     // correct(r, x) adds the FP32 correction for residual r into x; with x_max_in_correct it also
     // max-es each column's |x| into norms[width + j], which the loop zeroes before each correction.
-    // a_norm_device: |A|_inf already computed on the device (or null).
+    // a_norm_device: |A|_inf already computed on the device (or null). host: pinned memory of
+    // 3 width + 1 doubles whose first width + 1 the caller has already queued with norms_enqueue
+    // (earlier on the stream, so nothing waits for them), or null: the loop queues them itself.
     template <class Correct>
     int refine_loop(Context &ctx, const double *a, const double *b, double *x, double *r, double *sums, double *norms,
                     unsigned long long n, unsigned long long width, Correct correct, double &berr, int &iterations,
-                    const double *a_norm_device = nullptr, bool x_max_in_correct = false) {
-        double a_norm = 0.0;
-        std::vector<double> b_norm;
-        if (int code = norms_of(ctx, a, b, sums, norms, n, width, a_norm, b_norm, a_norm_device)) return code;
+                    const double *a_norm_device = nullptr, bool x_max_in_correct = false, double *host = nullptr) {
+        if (host == nullptr) {
+            host = pinned_doubles(ctx, 3 * width + 1);
+            if (host == nullptr) return ctx.fail(SCI_CUDA_ERROR_MEMORY, "pinned host memory for the refinement");
+            norms_enqueue(ctx, a, b, sums, norms, n, width, a_norm_device, host);
+        }
+        const double *b_norm = host, *a_norm = host + width;
         cudaMemsetAsync(x, 0, n * width * 8, ctx.stream);
         const double target = std::min(std::sqrt(static_cast<double>(n)) * 0x1p-53, 1e-14);
         constexpr int kMaxIterations = 30;
@@ -2411,7 +2524,8 @@ namespace {
             if (x_max_in_correct) cudaMemsetAsync(norms + width, 0, width * 8, ctx.stream);
             if (int code = correct(residual, x)) return code;
             ++iterations;
-            if (int code = backward_error(ctx, a, b, x, r, sums, norms, n, width, a_norm, b_norm.data(), berr, x_max_in_correct))
+            if (int code = backward_error(ctx, a, b, x, r, norms, n, width, a_norm, b_norm, host + width + 1, berr,
+                                          x_max_in_correct))
                 return code;
             residual = r;
             if (!(berr > target) || !(berr < 0.5 * previous)) break;
@@ -2460,15 +2574,15 @@ extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uin
             if (!code && report) {
                 double *r = carve.take<double>(nw);
                 double *sums = carve.take<double>(n);
-                double *norms = carve.take<double>(2 * width);
-                double a_norm = 0.0, berr = 0.0;
-                std::vector<double> b_norm;
-                code = norms_of(*context, static_cast<const double *>(matrix), static_cast<const double *>(right), sums,
-                                norms, n, width, a_norm, b_norm);
-                if (!code)
-                    code = backward_error(*context, static_cast<const double *>(matrix), static_cast<const double *>(right),
-                                          static_cast<const double *>(solution), r, sums, norms, n, width, a_norm,
-                                          b_norm.data(), berr);
+                double *norms = carve.take<double>(2 * width + 1);
+                double berr = 0.0;
+                double *host = pinned_doubles(*context, 3 * width + 1);
+                if (host == nullptr) return context->fail(SCI_CUDA_ERROR_MEMORY, "pinned host memory for the report");
+                norms_enqueue(*context, static_cast<const double *>(matrix), static_cast<const double *>(right), sums, norms,
+                              n, width, nullptr, host);
+                code = backward_error(*context, static_cast<const double *>(matrix), static_cast<const double *>(right),
+                                      static_cast<const double *>(solution), r, norms, n, width, host + width, host,
+                                      host + width + 1, berr);
                 if (!code) report->backward_error = berr;
             }
         } else {
@@ -2503,6 +2617,11 @@ extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uin
     // the FP32 copy of A and |A|_inf in one pass over A
     cudaMemsetAsync(a_norm, 0, 8, context->stream);
     narrow_sums<<<static_cast<unsigned>((n + 7) / 8), 256, 0, context->stream>>>(a, lu, n, a_norm);
+    // |b_j|_inf and |A|_inf on their way to the host before the factorisation: the refinement's
+    // first wait for the stream finds them there
+    double *host = pinned_doubles(*context, 3 * width + 1);
+    if (host == nullptr) return context->fail(SCI_CUDA_ERROR_MEMORY, "pinned host memory for the refinement");
+    norms_enqueue(*context, a, b, sums, norms, n, width, a_norm, host);
     if (int code = factor_device<float>(*context, lu, n, piv, moved, true, true, rows)) return code;
     if (int code = invert_diagonal<float>(*context, lu, n, inv)) return code;
     // the update also takes each column's |x|_inf when every thread of it stays in one column
@@ -2519,7 +2638,8 @@ extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uin
     };
     double berr = 0.0;
     int iterations = 0;
-    if (int code = refine_loop(*context, a, b, x, r, sums, norms, n, width, correct, berr, iterations, a_norm, fused_max))
+    if (int code = refine_loop(*context, a, b, x, r, sums, norms, n, width, correct, berr, iterations, a_norm, fused_max,
+                               host))
         return code;
     if (report) {
         report->backward_error = berr;
@@ -2621,7 +2741,7 @@ extern "C" int sci_cuda_solve_gradient(sci_cuda_context *context, uint32_t preci
     float *d = carve.take<float>(nw);
     double *r = carve.take<double>(nw);
     double *sums = carve.take<double>(n);
-    double *norms = carve.take<double>(2 * width);
+    double *norms = carve.take<double>(2 * width + 1);
     const int sms = context->sms;
 
     narrow<<<blocks_for(n * n, sms), 256, 0, context->stream>>>(a, lu, n * n);

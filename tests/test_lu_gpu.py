@@ -54,7 +54,7 @@ def test_solve_pins(device):
         assert np.all(np.abs(a @ x.numpy().reshape(b.shape) - b) < 1e-9)
 
 
-@pytest.mark.parametrize("n", [1, 2, 17, 64, 100, 257, 512])
+@pytest.mark.parametrize("n", [1, 2, 17, 64, 100, 257, 512, 1000, 1500])
 @pytest.mark.parametrize("kind", ["f64", "f32_plain"])
 def test_pivots_match_the_reference(device, reference, n, kind):
     dtype = np.float64 if kind == "f64" else np.float32
