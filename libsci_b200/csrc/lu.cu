@@ -1057,55 +1057,74 @@ namespace sci_cuda {
         }
 
         // Inverses of the diagonal blocks of L (unit lower) and U, kSolveBlock x kSolveBlock each, zero
-        // padded past the matrix: inv[2 b] is L's block b, inv[2 b + 1] U's. Thread c computes column c
-        // of both by substitution against the identity (solve.hpp:25-52 applied to e_c), reading back
-        // only the entries it wrote itself. The diagonal block is staged in shared memory first (all
-        // threads read its entries as broadcasts); for float the column being built stays there too
-        // (for double it is built in place in `inv`, which the 128 KB of the staged block leaves no
-        // room for).
+        // padded past the matrix: inv[2 b] is L's block b (blockIdx.y 0), inv[2 b + 1] U's (blockIdx.y
+        // 1). The block is staged in shared memory; warp w builds columns w, w + 32, ... of the inverse
+        // by substitution against the identity (solve.hpp:25-52 applied to e_c), lane l holding rows
+        // l, l + 32, ...: once entry k is final it is broadcast by a shuffle and every row it reaches
+        // takes its term, so the chain from one entry to the next is a shuffle and one multiply-add
+        // (the earlier form, a thread per column summing each entry's terms on its own, took 116 us
+        // for the 64 blocks of n = 8192). An entry of L's inverse takes its terms in the order of k,
+        // as the row-by-row substitution adds them; one of U's takes them from the diagonal outwards
+        // (k descending) and is then divided by the diagonal.
         constexpr int kInvertPitch = kSolveBlock + 1;
-        template <typename T> constexpr size_t invert_shared_bytes() {
-            return sizeof(T) * kSolveBlock * kInvertPitch * (sizeof(T) == 4 ? 2 : 1);
-        }
+        template <typename T> constexpr size_t invert_shared_bytes() { return sizeof(T) * kSolveBlock * kInvertPitch; }
+        constexpr int kInvertThreads = 1024;
         template <typename T>
-        __global__ void __launch_bounds__(kSolveBlock) invert_blocks(const T *lu, unsigned long long n, T *inv) {
-            constexpr int B = kSolveBlock, PD = kInvertPitch;
-            constexpr bool staged = sizeof(T) == 4;
+        __global__ void __launch_bounds__(kInvertThreads) invert_blocks(const T *lu, unsigned long long n, T *inv) {
+            constexpr int B = kSolveBlock, PD = kInvertPitch, R = B / 32;
             extern __shared__ __align__(16) unsigned char invert_shared[];
             T *const ds = reinterpret_cast<T *>(invert_shared);  // ds[i * PD + k] = d[i][k]
-            T *const work = staged ? ds + B * PD : nullptr;       // work[k * PD + c]: the column being built
             const unsigned long long s = blockIdx.x * 1ull * B;
             const int size = static_cast<int>(n - s < B ? n - s : B);
-            const int c = threadIdx.x;
-            T *lower = inv + 2ull * blockIdx.x * B * B;
-            T *upper = lower + 1ull * B * B;
+            const bool upper = blockIdx.y != 0;
+            T *const out = inv + (2ull * blockIdx.x + (upper ? 1ull : 0ull)) * B * B;
             const T *d = lu + s * n + s;
-#pragma unroll 16
-            for (int i = 0; i < B; ++i) ds[i * PD + c] = (i < size && c < size) ? d[i * n + c] : T(0);
+            for (int e = threadIdx.x; e < B * B; e += blockDim.x) {
+                const int i = e / B, k = e % B;
+                ds[i * PD + k] = (i < size && k < size) ? d[i * n + k] : T(0);
+            }
             __syncthreads();
-            auto at = [&](T *global, int k) -> T & { return staged ? work[k * PD + c] : global[k * B + c]; };
-            for (int i = 0; i < B; ++i) {
-                T value = T(0);
-                if (c < size && i < size && i >= c) {
-                    value = i == c ? T(1) : T(0);
-                    for (int k = c; k < i; ++k) value = fma_(-ds[i * PD + k], at(lower, k), value);
+            const int lane = static_cast<int>(threadIdx.x % 32);
+            for (int c = static_cast<int>(threadIdx.x / 32); c < B; c += kInvertThreads / 32) {
+                T x[R];  // x[r]: row 32 r + lane of column c
+#pragma unroll
+                for (int r = 0; r < R; ++r) x[r] = (c < size && 32 * r + lane == c) ? T(1) : T(0);
+                if (c < size && !upper) {
+                    // x_i = [i == c] - sum over k = c .. i - 1 of L_ik x_k
+#pragma unroll
+                    for (int q = 0; q < R; ++q) {
+                        if (32 * q + 31 < c) continue;
+                        for (int kk = 0; kk < 32; ++kk) {
+                            const int k = 32 * q + kk;
+                            if (k < c || k >= size) continue;
+                            const T xk = __shfl_sync(0xffffffffu, x[q], kk);
+#pragma unroll
+                            for (int r = q; r < R; ++r) {
+                                const int i = 32 * r + lane;
+                                if (i > k && i < size) x[r] = fma_(-ds[i * PD + k], xk, x[r]);
+                            }
+                        }
+                    }
+                } else if (c < size) {
+                    // x_i = ([i == c] - sum over k = c down to i + 1 of U_ik x_k) / U_ii
+#pragma unroll
+                    for (int q = R - 1; q >= 0; --q) {
+                        if (32 * q > c) continue;
+                        for (int kk = 31; kk >= 0; --kk) {
+                            const int k = 32 * q + kk;
+                            if (k > c) continue;
+                            if (lane == kk) x[q] = div(x[q], ds[k * PD + k]);
+                            const T xk = __shfl_sync(0xffffffffu, x[q], kk);
+#pragma unroll
+                            for (int r = 0; r <= q; ++r) {
+                                const int i = 32 * r + lane;
+                                if (i < k) x[r] = fma_(-ds[i * PD + k], xk, x[r]);
+                            }
+                        }
+                    }
                 }
-                at(lower, i) = value;
-            }
-            if constexpr (staged) {
-                for (int i = 0; i < B; ++i) lower[i * B + c] = work[i * PD + c];
-            }
-            for (int i = B - 1; i >= 0; --i) {
-                T value = T(0);
-                if (c < size && i < size && i <= c) {
-                    value = i == c ? T(1) : T(0);
-                    for (int k = i + 1; k <= c; ++k) value = fma_(-ds[i * PD + k], at(upper, k), value);
-                    value = div(value, ds[i * PD + i]);
-                }
-                at(upper, i) = value;
-            }
-            if constexpr (staged) {
-                for (int i = 0; i < B; ++i) upper[i * B + c] = work[i * PD + c];
+#pragma unroll
+                for (int r = 0; r < R; ++r) out[(32ull * r + lane) * B + c] = x[r];
             }
         }
 
@@ -1446,24 +1465,47 @@ namespace sci_cuda {
                 max_nonnegative(&x_max[c], m);
             }
         }
-        // out = (float) a for the n x n matrix, and |a|_inf (the largest row sum of |a|) max-ed into
-        // *a_norm (zeroed before): one warp per row, the row read once for both.
-        __global__ void __launch_bounds__(256) narrow_sums(const double *a, float *out, unsigned long long n, double *a_norm) {
+        // out = (float) a for the n x n matrix but its first `skip` columns (skip even), and |a|_inf (the
+        // largest row sum of |a|, every column) max-ed into *a_norm (zeroed before): one warp per row,
+        // the row read once for both, two elements per 16-byte load when rows are 16-byte aligned.
+        __global__ void __launch_bounds__(256) narrow_sums(const double *a, float *out, unsigned long long n, double *a_norm,
+                                                           unsigned long long skip) {
             const unsigned long long row = blockIdx.x * 8ull + threadIdx.x / 32;
             if (row >= n) return;
             const unsigned lane = threadIdx.x % 32;
             const double *src = a + row * n;
             float *dst = out + row * n;
             double s = 0.0;
+            if (n % 2 == 0) {
+                const double2 *src2 = reinterpret_cast<const double2 *>(src);
+                float2 *dst2 = reinterpret_cast<float2 *>(dst);
+                const unsigned long long pairs = n / 2, from = skip / 2;
 #pragma unroll 4
-            for (unsigned long long k = lane; k < n; k += 32) {
-                const double v = src[k];
-                dst[k] = static_cast<float>(v);
-                s += fabs(v);
+                for (unsigned long long k = lane; k < pairs; k += 32) {
+                    const double2 v = src2[k];
+                    if (k >= from) dst2[k] = make_float2(static_cast<float>(v.x), static_cast<float>(v.y));
+                    s += fabs(v.x);
+                    s += fabs(v.y);
+                }
+            } else {
+#pragma unroll 4
+                for (unsigned long long k = lane; k < n; k += 32) {
+                    const double v = src[k];
+                    if (k >= skip) dst[k] = static_cast<float>(v);
+                    s += fabs(v);
+                }
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
             if (lane == 0) max_nonnegative(a_norm, s);
+        }
+        // out = (float) a over the columns [0, columns) of every row: one warp per row.
+        __global__ void __launch_bounds__(256) narrow_columns(const double *a, float *out, unsigned long long n,
+                                                              unsigned long long columns) {
+            const unsigned long long row = blockIdx.x * 8ull + threadIdx.x / 32;
+            if (row >= n) return;
+            for (unsigned long long k = threadIdx.x % 32; k < columns; k += 32)
+                out[row * n + k] = static_cast<float>(a[row * n + k]);
         }
         // |rows of a|_1, the infinity norm's terms: one warp per row.
         template <typename T> __global__ void row_sums(const T *a, unsigned long long n, double *out) {
@@ -1517,6 +1559,16 @@ namespace sci_cuda {
             }
         };
 
+        // The factorisation's look-ahead (a second stream for the columns beyond the next block):
+        // orders above 2 kOuter, unless SCI_CUDA_LOOKAHEAD=0.
+        bool look_ahead(unsigned long long n) {
+            static const bool enabled = [] {
+                const char *setting = std::getenv("SCI_CUDA_LOOKAHEAD");
+                return !(setting && std::strcmp(setting, "0") == 0);
+            }();
+            return enabled && n > 2 * kOuter;
+        }
+
         int side_stream(Context &ctx) {
             if (ctx.side) return SCI_CUDA_OK;
             int least = 0, greatest = 0;
@@ -1540,16 +1592,16 @@ namespace sci_cuda {
         // on to its panels, while the side stream updates the columns beyond it. The two streams
         // touch disjoint columns (and movement halves), and the main stream waits for the side
         // before it moves rows outside a block.
+        //
+        // side_busy: the side stream (look_ahead(n) only) already holds work on the columns beyond the
+        // first block, with side_done recorded after it; the main stream waits for it before its
+        // first work there, as it waits for a block's side work.
         template <typename T>
         int factor_device(Context &ctx, T *a, unsigned long long n, long long *piv, Movement *moved, bool tensor,
-                          bool split, unsigned *order = nullptr) {
+                          bool split, unsigned *order = nullptr, bool side_busy = false) {
             constexpr int W = PanelWidth<T>::value;
             if (n > kPanelRows) return ctx.fail(SCI_CUDA_ERROR_UNSUPPORTED, "factor: order %llu above %llu", n, kPanelRows);
-            static const bool lookahead = [] {
-                const char *setting = std::getenv("SCI_CUDA_LOOKAHEAD");
-                return !(setting && std::strcmp(setting, "0") == 0);
-            }();
-            const bool ahead = lookahead && n > 2 * kOuter;
+            const bool ahead = look_ahead(n);
             if (ahead) {
                 if (int code = side_stream(ctx)) return code;
             }
@@ -1630,7 +1682,12 @@ namespace sci_cuda {
             };
             // order (optional): the row order, kept up to date by each panel's row moves
             if (order != nullptr) identity_rows<<<static_cast<unsigned>((n + 255) / 256), 256, 0, ctx.stream>>>(order, n);
-            bool side_pending = false;
+            bool side_pending = side_busy;
+            if (side_busy && !ahead) {
+                if (int code = ctx.check(cudaStreamWaitEvent(ctx.stream, ctx.side_done, 0), "waiting for the side"))
+                    return code;
+                side_pending = false;
+            }
             for (unsigned long long J0 = 0; J0 < n; J0 += kOuter) {
                 const unsigned long long ob = std::min<unsigned long long>(kOuter, n - J0), block_end = J0 + ob;
                 Movement *const block_moves = moved + (J0 / kOuter % 2) * (kMovements / 2);
@@ -1729,7 +1786,7 @@ namespace sci_cuda {
                                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                                   static_cast<int>(invert_shared_bytes<T>()));
             if (int code = ctx.check(sized, "sizing the inversion's shared memory")) return code;
-            invert_blocks<T><<<blocks, kSolveBlock, invert_shared_bytes<T>(), ctx.stream>>>(lu, n, inv);
+            invert_blocks<T><<<dim3(blocks, 2), kInvertThreads, invert_shared_bytes<T>(), ctx.stream>>>(lu, n, inv);
             if constexpr (sizeof(T) == 4) {
                 if (blocks > 1)
                     couple_blocks<<<dim3(blocks, 4), 256, 0, ctx.stream>>>(lu, inv, n, inv + 2ull * blocks * kSolveBlock * kSolveBlock);
@@ -2614,15 +2671,35 @@ extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uin
     double *a_norm = norms + 2 * width;
     const int sms = context->sms;
 
-    // the FP32 copy of A and |A|_inf in one pass over A
-    cudaMemsetAsync(a_norm, 0, 8, context->stream);
-    narrow_sums<<<static_cast<unsigned>((n + 7) / 8), 256, 0, context->stream>>>(a, lu, n, a_norm);
-    // |b_j|_inf and |A|_inf on their way to the host before the factorisation: the refinement's
-    // first wait for the stream finds them there
     double *host = pinned_doubles(*context, 3 * width + 1);
     if (host == nullptr) return context->fail(SCI_CUDA_ERROR_MEMORY, "pinned host memory for the refinement");
-    norms_enqueue(*context, a, b, sums, norms, n, width, a_norm, host);
-    if (int code = factor_device<float>(*context, lu, n, piv, moved, true, true, rows)) return code;
+    // The FP32 copy of A and |A|_inf in one pass over A, then |b_j|_inf and |A|_inf on their way to
+    // the host before the factorisation (the refinement's first wait for the stream finds them
+    // there). With the look-ahead, the main stream converts only the first block's columns, which
+    // are all that the first block's panels read, and starts factoring; the side stream converts
+    // the rest and takes the norms meanwhile, and the factorisation waits for it before it first
+    // touches the columns beyond the first block.
+    const bool overlap = look_ahead(n);
+    if (overlap) {
+        if (int code = side_stream(*context)) return code;
+    }
+    const unsigned long long first = overlap ? kOuter : 0;
+    cudaStream_t convert = overlap ? context->side : context->stream;
+    if (overlap)
+        narrow_columns<<<static_cast<unsigned>((n + 7) / 8), 256, 0, context->stream>>>(a, lu, n, first);
+    cudaMemsetAsync(a_norm, 0, 8, convert);
+    narrow_sums<<<static_cast<unsigned>((n + 7) / 8), 256, 0, convert>>>(a, lu, n, a_norm, first);
+    {
+        const cudaStream_t main = context->stream;
+        context->stream = convert;
+        norms_enqueue(*context, a, b, sums, norms, n, width, a_norm, host);
+        context->stream = main;
+    }
+    if (overlap) {
+        if (int code = context->check(cudaEventRecord(context->side_done, context->side), "recording the conversion"))
+            return code;
+    }
+    if (int code = factor_device<float>(*context, lu, n, piv, moved, true, true, rows, overlap)) return code;
     if (int code = invert_diagonal<float>(*context, lu, n, inv)) return code;
     // the update also takes each column's |x|_inf when every thread of it stays in one column
     const bool fused_max = 256 % width == 0;
