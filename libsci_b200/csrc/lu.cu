@@ -34,6 +34,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <cstdint>
 #include <cstring>
 #include <vector>
 
@@ -1467,16 +1468,17 @@ namespace sci_cuda {
         }
         // out = (float) a for the n x n matrix but its first `skip` columns (skip even), and |a|_inf (the
         // largest row sum of |a|, every column) max-ed into *a_norm (zeroed before): one warp per row,
-        // the row read once for both, two elements per 16-byte load when rows are 16-byte aligned.
+        // the row read once for both, two elements per 16-byte load when `paired` (n even, a 16-byte
+        // and out 8-byte aligned: every row then starts on those boundaries; narrow_paired).
         __global__ void __launch_bounds__(256) narrow_sums(const double *a, float *out, unsigned long long n, double *a_norm,
-                                                           unsigned long long skip) {
+                                                           unsigned long long skip, bool paired) {
             const unsigned long long row = blockIdx.x * 8ull + threadIdx.x / 32;
             if (row >= n) return;
             const unsigned lane = threadIdx.x % 32;
             const double *src = a + row * n;
             float *dst = out + row * n;
             double s = 0.0;
-            if (n % 2 == 0) {
+            if (paired) {
                 const double2 *src2 = reinterpret_cast<const double2 *>(src);
                 float2 *dst2 = reinterpret_cast<float2 *>(dst);
                 const unsigned long long pairs = n / 2, from = skip / 2;
@@ -1498,6 +1500,10 @@ namespace sci_cuda {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
             if (lane == 0) max_nonnegative(a_norm, s);
+        }
+        // Whether narrow_sums may read a in 16-byte pairs and write out in 8-byte pairs.
+        inline bool narrow_paired(const double *a, const float *out, unsigned long long n) {
+            return n % 2 == 0 && reinterpret_cast<uintptr_t>(a) % 16 == 0 && reinterpret_cast<uintptr_t>(out) % 8 == 0;
         }
         // out = (float) a over the columns [0, columns) of every row: one warp per row.
         __global__ void __launch_bounds__(256) narrow_columns(const double *a, float *out, unsigned long long n,
@@ -2688,7 +2694,8 @@ extern "C" int sci_cuda_solve(sci_cuda_context *context, uint32_t precision, uin
     if (overlap)
         narrow_columns<<<static_cast<unsigned>((n + 7) / 8), 256, 0, context->stream>>>(a, lu, n, first);
     cudaMemsetAsync(a_norm, 0, 8, convert);
-    narrow_sums<<<static_cast<unsigned>((n + 7) / 8), 256, 0, convert>>>(a, lu, n, a_norm, first);
+    narrow_sums<<<static_cast<unsigned>((n + 7) / 8), 256, 0, convert>>>(a, lu, n, a_norm, first,
+                                                                       narrow_paired(a, lu, n));
     {
         const cudaStream_t main = context->stream;
         context->stream = convert;

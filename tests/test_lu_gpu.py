@@ -106,6 +106,30 @@ def test_refined_solve(device, n, shift):
     assert np.abs(plain.numpy().reshape(n, 16) - x).max() <= 1e-9 * np.abs(x).max() * (1 if shift else 1e3)
 
 
+@pytest.mark.parametrize("n", [130, 600])
+def test_refined_solve_at_unaligned_addresses(device, n):
+    """Systems packed one after another in one buffer (as a caller batching them keeps them) start
+    on 8-byte boundaries only: the refined solve reads A, b and writes x at such addresses, for an
+    order without (130) and with (600) the look-ahead's second stream."""
+    from libsci_b200.native import SolveReport, check, lib
+
+    rng = np.random.default_rng(n)
+    a = rng.standard_normal((n, n)) + n * np.eye(n)
+    b = rng.standard_normal((n, 2))
+    flat_a = device.array(np.concatenate([[0.0], a.ravel()]))
+    flat_b = device.array(np.concatenate([[0.0], b.ravel()]))
+    flat_x = device.array(np.zeros(2 * n + 1))
+    assert flat_a.pointer % 16 == 0  # so A itself sits 8 bytes past a 16-byte boundary
+    report = SolveReport()
+    check(lib.sci_cuda_solve(device.handle, 1, 1, flat_a.pointer + 8, flat_b.pointer + 8, flat_x.pointer + 8, n, 2,
+                             ctypes.byref(report)), device.handle)
+    x = flat_x.numpy()[1:].reshape(n, 2)
+    assert report.backward_error <= 1e-14
+    r = b - a @ x
+    mine = np.abs(r).max(axis=0) / (np.abs(a).sum(axis=1).max() * np.abs(x).max(axis=0) + np.abs(b).max(axis=0))
+    assert mine.max() <= 2e-14
+
+
 def test_float_solve_without_refinement(device):
     n = 500
     rng = np.random.default_rng(1)
