@@ -77,15 +77,16 @@ namespace sci_cuda {
         std::string name;
 
         ReduceState *state{nullptr};   // reduction scratch (device)
-        double *result{nullptr};       // reduction result (device)
-        int *status{nullptr};          // device-side error word
-        double *host_result{nullptr};  // pinned
-        int *host_status{nullptr};     // pinned
+        double *result{nullptr};       // reduction result (device), with the status word 8 bytes on
+        int *status{nullptr};          // device-side error word (in result's allocation)
+        double *host_result{nullptr};  // pinned, with host_status 8 bytes on: one copy reads both
+        int *host_status{nullptr};     // pinned (in host_result's allocation)
         double *pinned{nullptr};       // pinned doubles for small read-backs (grown on demand)
         size_t pinned_count{0};
 
         std::vector<Retired> retired;  // frees deferred until queued work is done
         std::map<std::tuple<const void *, int, size_t>, int> occupancy;  // (kernel, threads, smem) -> blocks/SM
+        std::map<const void *, size_t> smem_raised;  // NVRTC function -> the dynamic shared memory it is allowed
         std::unique_ptr<Specializer> specializer;
         std::unique_ptr<Workspace> workspace;  // product / trailing-update operands
         std::unique_ptr<Workspace> solver;     // LU copies, pivots, residuals
@@ -133,8 +134,19 @@ namespace sci_cuda {
             return occupancy[key];
         }
 
-        // Reads and clears the device error word; waits for the stream.
-        int drain();
+        // Reads and clears the device error word; waits for the stream. status_queued: a copy of the
+        // status word into host_status is already queued on the stream.
+        int drain(bool status_queued = false);
+
+        // Lets `kernel` use `smem` bytes of dynamic shared memory, raising its limit only past the
+        // largest one set so far: for kernels no other context or entry point sets (this context's
+        // NVRTC modules).
+        template <typename Raise> void allow_smem(const void *kernel, size_t smem, Raise raise) {
+            auto found = smem_raised.find(kernel);
+            if (found != smem_raised.end() && found->second >= smem) return;
+            raise();
+            smem_raised[kernel] = smem;
+        }
     };
 
     // Block size, TMA ring depth and dynamic shared memory of a chunk launch: the widest tile whose
@@ -175,6 +187,9 @@ namespace sci_cuda {
     // Without the opt-in, static plus dynamic shared memory must stay within 48 KB; the chunk
     // kernel's static part (mbarriers, fold scratch) is under 4 KB.
     constexpr size_t kChunkSharedOptIn = 44 * 1024;
+
+    // The context's reduction result (a double) and status word (an int after it), one allocation.
+    constexpr size_t kResultBytes = 16;
 
     // The generic interpreter's kernels, compiled ahead of time (chunk_kernels_f32.cu / _f64.cu).
     const void *generic_chunk_kernel(bool wide, int mode);

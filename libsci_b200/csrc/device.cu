@@ -24,9 +24,10 @@ using namespace sci_cuda;
 
 namespace sci_cuda {
 
-    int Context::drain() {
-        int code = check(cudaMemcpyAsync(host_status, status, sizeof(int), cudaMemcpyDeviceToHost, stream),
-                         "reading the device status");
+    int Context::drain(bool status_queued) {
+        int code = status_queued ? SCI_CUDA_OK
+                                 : check(cudaMemcpyAsync(host_status, status, sizeof(int), cudaMemcpyDeviceToHost, stream),
+                                         "reading the device status");
         if (code) return code;
         code = check(cudaStreamSynchronize(stream), "synchronizing the stream");
         if (code) return code;
@@ -185,7 +186,10 @@ namespace sci_cuda {
         if (special) {
             // An NVRTC module: a driver-API function.
             CUfunction function = reinterpret_cast<CUfunction>(const_cast<void *>(special->function));
-            Driver::get().function_attribute(function, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, static_cast<int>(smem));
+            // the module is this context's own: its limit is raised past the largest use only
+            ctx.allow_smem(special->function, smem, [&] {
+                Driver::get().function_attribute(function, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, static_cast<int>(smem));
+            });
             const auto key = std::make_tuple(special->function, threads, smem);
             auto found = ctx.occupancy.find(key);
             int per_sm = 1;
@@ -202,6 +206,8 @@ namespace sci_cuda {
             if (code != CUDA_SUCCESS) return ctx.fail(SCI_CUDA_ERROR_LAUNCH, "launching a specialised chunk kernel: %d", int(code));
             return SCI_CUDA_OK;
         }
+        // Set on every launch: other contexts, and the entry point without allocations, set the same
+        // kernel's limit too (it is the process's, not this context's).
         if (smem > kChunkSharedOptIn) {
             cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         }
@@ -253,11 +259,14 @@ int sci_cuda_open(uint32_t ordinal, sci_cuda_context **context) {
     int least = 0, greatest = 0;
     cudaDeviceGetStreamPriorityRange(&least, &greatest);
     if (cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, greatest) != cudaSuccess) return SCI_CUDA_ERROR_DEVICE;
-    if (cudaMalloc(&ctx->state, sizeof(ReduceState)) != cudaSuccess || cudaMalloc(&ctx->result, sizeof(double)) != cudaSuccess ||
-        cudaMalloc(&ctx->status, sizeof(int)) != cudaSuccess || cudaMallocHost(&ctx->host_result, sizeof(double)) != cudaSuccess ||
-        cudaMallocHost(&ctx->host_status, sizeof(int)) != cudaSuccess) {
+    // the reduction's result with the status word after it (device and pinned host): a blocking
+    // reduction reads both with one copy
+    if (cudaMalloc(&ctx->state, sizeof(ReduceState)) != cudaSuccess || cudaMalloc(&ctx->result, kResultBytes) != cudaSuccess ||
+        cudaMallocHost(&ctx->host_result, kResultBytes) != cudaSuccess) {
         return SCI_CUDA_ERROR_MEMORY;
     }
+    ctx->status = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(ctx->result) + sizeof(double));
+    ctx->host_status = reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(ctx->host_result) + sizeof(double));
     cudaMemsetAsync(ctx->state, 0, sizeof(ReduceState), ctx->stream);
     cudaMemsetAsync(ctx->status, 0, sizeof(int), ctx->stream);
     *ctx->host_status = 0;
@@ -290,8 +299,7 @@ int sci_cuda_close(sci_cuda_context *context) {
         }
         context->retired.clear();
         cudaFree(context->state);
-        cudaFree(context->result);
-        cudaFree(context->status);
+        cudaFree(context->result);  // and the status word
         cudaFree(context->sweep_flags);
         if (context->side) cudaStreamDestroy(context->side);
         if (context->side_done) cudaEventDestroy(context->side_done);
@@ -306,8 +314,7 @@ int sci_cuda_close(sci_cuda_context *context) {
             cudaEventDestroy(context->downloaded);
             cudaEventDestroy(context->main_point);
         }
-        cudaFreeHost(context->host_result);
-        cudaFreeHost(context->host_status);
+        cudaFreeHost(context->host_result);  // and host_status
         cudaFreeHost(context->pinned);
         cudaStreamDestroy(context->stream);
     }
@@ -495,11 +502,12 @@ int sci_cuda_reduce(sci_cuda_context *context, const sci_chunk *chunk, uint32_t 
     }
     cudaSetDevice(context->device);
     if (int code = dispatch(*context, *chunk, kReduce, fold, count, nullptr, context->result)) return code;
-    if (int code = context->check(cudaMemcpyAsync(context->host_result, context->result, sizeof(double),
+    // the result and the status word in one copy
+    if (int code = context->check(cudaMemcpyAsync(context->host_result, context->result, kResultBytes,
                                                   cudaMemcpyDeviceToHost, context->stream),
                                   "reading the reduction"))
         return code;
-    if (int code = context->drain()) return code;
+    if (int code = context->drain(true)) return code;
     *result = *context->host_result;
     return SCI_CUDA_OK;
 }
