@@ -204,10 +204,12 @@ namespace sci_cuda {
     // and multiplies on the tensor cores; simt_gemm is the plain FP32 / FP64 form. Both queue on
     // ctx.stream. `whole_gpu`: the product has the GPU to itself, so products of 256 rows or more
     // run on the persistent CTA-pair kernel (a static split of the tiles over every SM); the LU's
-    // updates, which share the GPU with the panels, keep the one-tile-per-CTA kernel.
+    // updates, which share the GPU with the panels, keep the one-tile-per-CTA kernel. `chained`: the
+    // first launch follows the kernel before it on the stream directly, so the conversions and the
+    // product are launched with programmatic stream serialization (each waits for the one before).
     int tensor_gemm(Context &ctx, int terms, const float *a, unsigned long long lda, const float *b,
                     unsigned long long ldb, float *c, unsigned long long ldc, unsigned long long m, unsigned long long n,
-                    unsigned long long k, bool subtract, bool whole_gpu = false);
+                    unsigned long long k, bool subtract, bool whole_gpu = false, bool chained = false);
     template <typename T>
     int simt_gemm(Context &ctx, const T *a, unsigned long long lda, const T *b, unsigned long long ldb, T *c,
                   unsigned long long ldc, unsigned long long m, unsigned long long n, unsigned long long k, bool subtract);
@@ -215,7 +217,8 @@ namespace sci_cuda {
     // that B is stored n x k (pitch ldb).
     int tensor_gemm_t(Context &ctx, int terms, const float *a, unsigned long long lda, bool a_t, const float *b,
                       unsigned long long ldb, bool b_t, float *c, unsigned long long ldc, unsigned long long m,
-                      unsigned long long n, unsigned long long k, bool subtract, bool whole_gpu = false);
+                      unsigned long long n, unsigned long long k, bool subtract, bool whole_gpu = false,
+                      bool chained = false);
     template <typename T>
     int simt_gemm_t(Context &ctx, const T *a, unsigned long long lda, bool a_t, const T *b, unsigned long long ldb, bool b_t,
                     T *c, unsigned long long ldc, unsigned long long m, unsigned long long n, unsigned long long k,

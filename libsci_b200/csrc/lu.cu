@@ -610,6 +610,21 @@ namespace sci_cuda {
         // Launches `kernel` on `stream` with programmatic stream serialization, for kernels that
         // call chain_wait() before reading what the kernel before them wrote.
         template <typename... Params, typename... Args>
+        cudaError_t launch_chained_shared(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                                          Args... args) {
+            cudaLaunchConfig_t config{};
+            config.gridDim = grid;
+            config.blockDim = block;
+            config.dynamicSmemBytes = smem;
+            config.stream = stream;
+            cudaLaunchAttribute attribute[1];
+            attribute[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attribute[0].val.programmaticStreamSerializationAllowed = 1;
+            config.attrs = attribute;
+            config.numAttrs = 1;
+            return cudaLaunchKernelEx(&config, kernel, static_cast<Params>(args)...);
+        }
+        template <typename... Params, typename... Args>
         cudaError_t launch_chained(void (*kernel)(Params...), dim3 grid, dim3 block, cudaStream_t stream, Args... args) {
             cudaLaunchConfig_t config{};
             config.gridDim = grid;
@@ -1647,14 +1662,19 @@ namespace sci_cuda {
                 return wide != cudaSuccess ? wide : thin;
             }();
             if (int code = ctx.check(strip_sized, "sizing the block rows' shared memory")) return code;
+            // chained: the launch follows the kernel before it on the stream directly (narrow strips only)
             auto block_rows = [&](unsigned long long J0, unsigned long long block_end, unsigned long long c0,
-                                  unsigned long long c1, bool narrow) -> int {
+                                  unsigned long long c1, bool narrow, bool chained = false) -> int {
                 if (c1 <= c0) return SCI_CUDA_OK;
                 const int ob = static_cast<int>(block_end - J0);
                 if (narrow) {
                     constexpr int CS = kStripColumnsNarrow;
-                    block_rows_strip<T, CS><<<static_cast<unsigned>((c1 - c0 + CS - 1) / CS), 256, strip_shared_bytes<T, CS>(),
-                                              ctx.stream>>>(a, n, J0, ob, c0, c1);
+                    const dim3 grid(static_cast<unsigned>((c1 - c0 + CS - 1) / CS));
+                    if (chained)
+                        return ctx.check(launch_chained_shared(block_rows_strip<T, CS>, grid, dim3(256), strip_shared_bytes<T, CS>(),
+                                                               ctx.stream, a, n, J0, ob, c0, c1),
+                                         "launching the block's U rows");
+                    block_rows_strip<T, CS><<<grid, 256, strip_shared_bytes<T, CS>(), ctx.stream>>>(a, n, J0, ob, c0, c1);
                 } else {
                     constexpr int CS = kStripColumns;
                     block_rows_strip<T, CS><<<static_cast<unsigned>((c1 - c0 + CS - 1) / CS), 256, strip_shared_bytes<T, CS>(),
@@ -1679,9 +1699,10 @@ namespace sci_cuda {
                     if (narrow && !tensor)
                         return update<T>(ctx, a + t0 * n + J0, n, a + J0 * n + c0, n, a + t0 * n + c0, n, n - t0, c1 - c0, ob,
                                          true);
+                    // the next block's columns follow the block's U rows directly on the main stream
                     if (tensor)
                         return tensor_gemm(ctx, split ? 3 : 1, a + t0 * n + J0, n, a + J0 * n + c0, n, a + t0 * n + c0, n,
-                                           n - t0, c1 - c0, ob, true);
+                                           n - t0, c1 - c0, ob, true, false, narrow);
                 }
                 return simt_gemm<T>(ctx, a + t0 * n + J0, n, a + J0 * n + c0, n, a + t0 * n + c0, n, n - t0, c1 - c0, ob,
                                     true);
@@ -1767,7 +1788,9 @@ namespace sci_cuda {
                     if (int code = side_work()) return code;
                 }
                 if (block_end < n) {
-                    if (int code = block_rows(J0, block_end, block_end, split_at, true)) return code;
+                    // with the tensor cores the side's work comes after these, so they follow the row
+                    // moves and each other directly on the main stream (chained)
+                    if (int code = block_rows(J0, block_end, block_end, split_at, true, side_late)) return code;
                     if (int code = trailing(J0, block_end, block_end, split_at, true)) return code;
                 }
                 if (split_at < n && side_late) {

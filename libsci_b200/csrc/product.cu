@@ -67,8 +67,17 @@ namespace sci_cuda {
 
         // A (rows x k, pitch lda) into K-major terms, rows x kp: eight values per thread step, read as
         // two 16-byte vectors where the row allows it.
+        // Programmatic dependent launch: returns once the kernel before this one on the stream has
+        // finished and its writes are visible, and lets the kernel after this one launch. Both are
+        // no-ops in a kernel launched the ordinary way.
+        __device__ __forceinline__ void follow_previous() {
+            asm volatile("griddepcontrol.wait;" ::: "memory");
+            asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+        }
+
         __global__ void split_rows(const float *__restrict__ a, unsigned long long lda, Terms out, int terms,
                                    unsigned long long rows, unsigned long long k, unsigned long long kp) {
+            follow_previous();
             const unsigned long long per_row = kp / 8, total = rows * per_row;
             const bool vector = lda % 4 == 0 && reinterpret_cast<unsigned long long>(a) % 16 == 0;
             for (unsigned long long i = blockIdx.x * 256ull + threadIdx.x; i < total; i += 256ull * gridDim.x) {
@@ -96,6 +105,7 @@ namespace sci_cuda {
                                                                int terms, unsigned long long k, unsigned long long n,
                                                                unsigned long long kp) {
             __shared__ float tile[64][65];
+            follow_previous();
             const unsigned long long k0 = blockIdx.y * 64ull, n0 = blockIdx.x * 64ull;
             const bool vector = ldb % 4 == 0 && reinterpret_cast<unsigned long long>(b) % 16 == 0;
 #pragma unroll
@@ -228,6 +238,7 @@ namespace sci_cuda {
             extern __shared__ unsigned char raw[];
             __shared__ unsigned long long full[S], empty[S], done;
             __shared__ unsigned tmem_slot;
+            follow_previous();
             __shared__ int abort_flag;
             unsigned char *ring = reinterpret_cast<unsigned char *>((reinterpret_cast<unsigned long long>(raw) + 1023) & ~1023ull);
 
@@ -815,13 +826,13 @@ namespace sci_cuda {
     // transposition, so the tensor-core kernel is the same either way.
     int tensor_gemm(Context &ctx, int terms, const float *a, unsigned long long lda, const float *b,
                     unsigned long long ldb, float *c, unsigned long long ldc, unsigned long long m, unsigned long long n,
-                    unsigned long long k, bool subtract, bool whole_gpu) {
-        return tensor_gemm_t(ctx, terms, a, lda, false, b, ldb, false, c, ldc, m, n, k, subtract, whole_gpu);
+                    unsigned long long k, bool subtract, bool whole_gpu, bool chained) {
+        return tensor_gemm_t(ctx, terms, a, lda, false, b, ldb, false, c, ldc, m, n, k, subtract, whole_gpu, chained);
     }
 
     int tensor_gemm_t(Context &ctx, int terms, const float *a, unsigned long long lda, bool a_t, const float *b,
                       unsigned long long ldb, bool b_t, float *c, unsigned long long ldc, unsigned long long m,
-                      unsigned long long n, unsigned long long k, bool subtract, bool whole_gpu) {
+                      unsigned long long n, unsigned long long k, bool subtract, bool whole_gpu, bool chained) {
         if (terms < 1 || terms > 3) return ctx.fail(SCI_CUDA_ERROR_INVALID, "bf16 terms %d", terms);
         const unsigned long long kp = (k + kBK - 1) / kBK * kBK;
         if (kp > (1ull << 31) || m > (1ull << 31) || n > (1ull << 31))
@@ -835,20 +846,41 @@ namespace sci_cuda {
             at.t[q] = reinterpret_cast<__nv_bfloat16 *>(base + q * a_bytes);
             bt.t[q] = reinterpret_cast<__nv_bfloat16 *>(base + terms * a_bytes + q * b_bytes);
         }
+        // chained: launched with programmatic stream serialization (the kernels start with
+        // follow_previous), else the ordinary way
+        auto launch = [&](const void *kernel, dim3 grid, dim3 block, void **params, size_t smem) -> cudaError_t {
+            if (!chained) return cudaLaunchKernel(kernel, grid, block, params, smem, ctx.stream);
+            cudaLaunchConfig_t config{};
+            config.gridDim = grid;
+            config.blockDim = block;
+            config.dynamicSmemBytes = smem;
+            config.stream = ctx.stream;
+            cudaLaunchAttribute attribute[1];
+            attribute[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            attribute[0].val.programmaticStreamSerializationAllowed = 1;
+            config.attrs = attribute;
+            config.numAttrs = 1;
+            return cudaLaunchKernelExC(&config, kernel, params);
+        };
         auto rows_of = [&](const float *x, unsigned long long ld, Terms out, unsigned long long rows) {
             const unsigned grid =
                     static_cast<unsigned>(std::min<unsigned long long>((rows * (kp / 8) + 255) / 256, ctx.sms * 16ull));
-            split_rows<<<grid, 256, 0, ctx.stream>>>(x, ld, out, terms, rows, k, kp);
+            int count = terms;
+            unsigned long long kk = k, kpp = kp;
+            void *params[] = {&x, &ld, &out, &count, &rows, &kk, &kpp};
+            return launch(reinterpret_cast<const void *>(&split_rows), dim3(grid), dim3(256), params, 0);
         };
         auto columns_of = [&](const float *x, unsigned long long ld, Terms out, unsigned long long columns) {
             const dim3 tgrid(static_cast<unsigned>((columns + 63) / 64), static_cast<unsigned>(kp / 64));
-            split_transpose<<<tgrid, 256, 0, ctx.stream>>>(x, ld, out, terms, k, columns, kp);
+            int count = terms;
+            unsigned long long kk = k, kpp = kp;
+            void *params[] = {&x, &ld, &out, &count, &kk, &columns, &kpp};
+            return launch(reinterpret_cast<const void *>(&split_transpose), tgrid, dim3(256), params, 0);
         };
-        if (a_t) columns_of(a, lda, at, m);
-        else rows_of(a, lda, at, m);
-        if (b_t) rows_of(b, ldb, bt, n);
-        else columns_of(b, ldb, bt, n);
-        if (int code = ctx.check(cudaGetLastError(), "launching the bf16 conversion")) return code;
+        if (int code = ctx.check(a_t ? columns_of(a, lda, at, m) : rows_of(a, lda, at, m), "launching the bf16 conversion"))
+            return code;
+        if (int code = ctx.check(b_t ? rows_of(b, ldb, bt, n) : columns_of(b, ldb, bt, n), "launching the bf16 conversion"))
+            return code;
 
         ProductArgs args{c, m, n, kp, ldc, subtract ? 1 : 0, ctx.status};
         if (whole_gpu && m >= 256 && pair_kernel_enabled()) {
@@ -896,7 +928,7 @@ namespace sci_cuda {
             return code;
         void *params[] = {&maps, &args};
         const dim3 pgrid(static_cast<unsigned>((n + bn - 1) / bn), static_cast<unsigned>((m + kBM - 1) / kBM));
-        return ctx.check(cudaLaunchKernel(kernel, pgrid, dim3(192), params, smem, ctx.stream), "launching the tensor product");
+        return ctx.check(launch(kernel, pgrid, dim3(192), params, smem), "launching the tensor product");
     }
 
     // C (pitch ldc) = or -= A (pitch lda) * B (pitch ldb) with the plain SIMT kernel; a_t / b_t as for
